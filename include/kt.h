@@ -1,0 +1,121 @@
+/* kt.h -- C ABI of the B200 kmax-truss solver (libkt.so).
+ *
+ * The solver answers the question of caixiaofan/KC_CUDA: for an undirected
+ * graph given as a TSV edge list, the largest k with a non-empty k-truss and
+ * the number of edges in that k-truss (a k-truss is the largest subgraph in
+ * which every edge lies in at least k-2 triangles of the subgraph).  A graph
+ * without triangles answers kmax = 0, 0 edges, as the reference does
+ * (src/kc_cpu.cpp:703-710).
+ *
+ * The reference exposes its GPU path as C++ functions over host arrays
+ * (src/kc_gpu.h:48-69) driven by a `main -f <path>` (src/kc_gpu.cpp:209-347).
+ * This header replaces them with opaque handles and status codes; each entry
+ * point names the reference function(s) it stands in for.  All pointers in
+ * this header are HOST pointers unless the name says `_device`.  Calls on one
+ * context are serialised internally; separate contexts may be used from
+ * separate threads.
+ */
+#ifndef KT_H
+#define KT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum kt_status {
+  KT_OK = 0,
+  KT_ERR_INVALID = 1,  /* bad argument or handle */
+  KT_ERR_CUDA = 2,     /* CUDA runtime error; text in kt_last_error */
+  KT_ERR_NOMEM = 3,    /* device memory or the context's HBM budget exhausted */
+  KT_ERR_PARSE = 4,    /* a TSV line with a single number; kt_last_error names it */
+  KT_ERR_IO = 5,       /* open / mmap / read failure */
+  KT_ERR_TIMEOUT = 6,  /* a bounded device wait gave up (kernel returned early) */
+  KT_ERR_LIMIT = 7,    /* input beyond a documented size limit */
+  KT_ERR_NODEV = 8,    /* no usable CUDA device */
+  KT_ERR_BUSY = 9,     /* serving: admission refused, retry later */
+} kt_status;
+
+typedef struct kt_ctx kt_ctx;
+typedef struct kt_graph kt_graph;
+
+/* Creates a context on `device` with its own stream.  hbm_budget_bytes caps
+ * the device memory the context may hold (0 = 90% of free memory).
+ * Replaces initGPU (src/kc.cu:30-53, src/kc_gpu.h:48). */
+kt_status kt_init(int device, uint64_t hbm_budget_bytes, kt_ctx** out);
+void kt_destroy(kt_ctx* ctx);
+/* Text of the last error on this context ("" if none). */
+const char* kt_last_error(const kt_ctx* ctx);
+const char* kt_status_string(kt_status s);
+
+/* Tunables by name (see DESIGN and kt_option_names): returns KT_ERR_INVALID
+ * for an unknown name. */
+kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
+kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
+
+/* ---------------------------------------------------------------- ingest */
+
+/* Parses TSV bytes on the device and builds the cleaned graph (self-loops
+ * dropped, repeated and reverse-repeated edges merged).  The record grammar is
+ * the reference's (src/kc_gpu.cpp:243-306): a byte is a digit when, as a
+ * signed char, it is >= '0'; a line's first two digit runs are x and y; other
+ * lines are skipped; a line with one digit run is KT_ERR_PARSE.
+ * Replaces the host parse and init_graph (src/kc_gpu.cpp:221-322, 38-65). */
+kt_status kt_load_tsv(kt_ctx* ctx, const char* bytes, uint64_t len, kt_graph** out);
+/* As kt_load_tsv, from a file (mmap, pipelined host-to-device copies).
+ * Replaces MapFile + vmtouch + parse (src/mapfile.hpp:35-84,
+ * src/kc_gpu.cpp:221-240). */
+kt_status kt_load_tsv_file(kt_ctx* ctx, const char* path, kt_graph** out);
+/* Builds the cleaned graph from records x << 32 | y (host array). */
+kt_status kt_load_pairs(kt_ctx* ctx, const uint64_t* xy, uint64_t count, kt_graph** out);
+kt_status kt_graph_info(const kt_graph* g, uint64_t* num_vertices, uint64_t* num_edges);
+/* Sorted canonical edges u << 32 | v (u < v), num_edges of them. */
+kt_status kt_graph_edges(kt_ctx* ctx, const kt_graph* g, uint64_t* keys_out);
+void kt_graph_free(kt_ctx* ctx, kt_graph* g);
+
+/* ----------------------------------------------------------------- solve */
+
+/* kmax and the kmax-truss edge count.  Two phases as in the reference: a
+ * lower bound from the truss of the maximum core, then the search on the
+ * (bound-1)-core.  Replaces kmax_truss (src/kc_gpu.cpp:129-208, called twice
+ * at src/kc_gpu.cpp:336,340) with kmax_core_gpu, tricount_direct,
+ * kmax_truss_GPU and reconstruct_Graph (src/kc.cu:770, 584, 1140, 1059). */
+kt_status kt_solve(kt_ctx* ctx, kt_graph* g, uint32_t* kmax, uint64_t* edges);
+/* kt_load_tsv + kt_solve + kt_graph_free in one call (the `-f` path). */
+kt_status kt_solve_tsv(kt_ctx* ctx, const char* bytes, uint64_t len, uint32_t* kmax, uint64_t* edges);
+
+/* ------------------------------------------------------- stage outputs */
+
+/* Members of the k-core (member_out[v] = 1 if v is in it) and, in cmax_out,
+ * the largest k with a non-empty k-core.  Replaces kmax_core_gpu
+ * (src/kc.cu:770-884).  Either output may be NULL. */
+kt_status kt_kcore(kt_ctx* ctx, kt_graph* g, uint32_t k, uint8_t* member_out, uint32_t* cmax_out);
+/* Core number of every vertex (num_vertices entries). */
+kt_status kt_core_numbers(kt_ctx* ctx, kt_graph* g, uint32_t* core_out);
+/* Triangles through each edge, in kt_graph_edges order.  Replaces
+ * tricount_direct (src/kc.cu:584-651), which stores twice this value. */
+kt_status kt_edge_support(kt_ctx* ctx, kt_graph* g, uint32_t* sup_out);
+/* Trussness of each edge, in kt_graph_edges order (2 = in no triangle). */
+kt_status kt_edge_trussness(kt_ctx* ctx, kt_graph* g, uint32_t* truss_out);
+
+/* ----------------------------------------------------------- statistics */
+
+typedef struct kt_stats {
+  double ms_parse, ms_csr, ms_kcore, ms_subgraph, ms_support, ms_peel, ms_total; /* device time, last solve */
+  uint64_t kernel_launches;       /* kernels this context launched since kt_stats_reset */
+  uint64_t core_vertices, core_edges;       /* search-phase subgraph */
+  uint64_t predict_vertices, predict_edges; /* prediction-phase subgraph */
+  uint32_t cmax, kmax_lower_bound, levels, rounds;
+  uint64_t support_bytes, peel_bytes;       /* algorithmic bytes of the last solve */
+  double ms_support_kernel, ms_peel_kernel; /* summed kernel time (events) */
+  uint64_t support_launches, peel_launches;
+  uint64_t device_bytes_peak;
+} kt_stats;
+kt_status kt_get_stats(const kt_ctx* ctx, kt_stats* out);
+kt_status kt_stats_reset(kt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,478 @@
+// The C ABI (include/kt.h): handles, status codes, ingest and stage outputs.
+// Every entry point catches kt::Error and std::exception and returns a
+// status; nothing is thrown across the boundary.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "kt.h"
+#include "solve.h"
+
+struct kt_ctx {
+  kt::Ctx c;
+};
+struct kt_graph {
+  kt::Graph g;
+};
+
+namespace kt {
+
+DevWords* dev_words(Ctx* c) { return c->words.as<DevWords>(); }
+
+void reset_words(Ctx* c) {
+  KT_CUDA(cudaMemsetAsync(c->words.get(), 0, sizeof(DevWords), c->stream));
+  KT_CUDA(cudaMemsetAsync(&dev_words(c)->bad_line, 0xff, sizeof(unsigned long long), c->stream));
+}
+
+void check_words(Ctx* c, const char* stage) {
+  DevWords w;
+  copy_d2h(c, &w, c->words.get(), sizeof(DevWords));
+  if (!w.err) return;
+  char buf[256];
+  kt_status s = KT_ERR_CUDA;
+  if (w.err & kDevErrParse) {
+    std::snprintf(buf, sizeof(buf), "malformed record on line %llu: a line needs two numbers",
+                  (unsigned long long)w.bad_line + 1);
+    s = KT_ERR_PARSE;
+  } else if (w.err & (kDevErrBarrier | kDevErrWait)) {
+    std::snprintf(buf, sizeof(buf), "%s: a bounded device wait gave up (flags %u)", stage, w.err);
+    s = KT_ERR_TIMEOUT;
+  } else {
+    std::snprintf(buf, sizeof(buf), "%s: device work list overflow (flags %u)", stage, w.err);
+  }
+  reset_words(c);
+  throw Error(s, buf);
+}
+
+namespace {
+
+__global__ void k_canon_pairs(uint64_t* __restrict__ xy, uint64_t n, unsigned int* __restrict__ vmax,
+                              unsigned int* __restrict__ any) {
+  uint32_t mx = 0;
+  bool seen = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = xy[i];
+    const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+    mx = max(mx, max(x, y));
+    seen = true;
+    xy[i] = x == y ? ~0ULL : (x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x));
+  }
+  mx = warp_max(mx);
+  const unsigned s = __ballot_sync(kFull, seen);
+  if (lane_id() == 0 && s) {
+    atomicMax(vmax, mx);
+    atomicOr(any, 1u);
+  }
+}
+
+}  // namespace
+
+// Device bytes (padded) -> Graph.
+static void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g) {
+  reset_words(c);
+  DBuf block_off;
+  const uint64_t lines = parse_count_lines(c, dbuf, len, block_off);
+  DBuf keys(c, (lines ? lines : 1) * sizeof(uint64_t));
+  parse_lines(c, dbuf, len, block_off, keys.as<uint64_t>(), dev_words(c));
+  check_words(c, "parse");
+  DevWords w;
+  copy_d2h(c, &w, c->words.get(), sizeof(DevWords));
+  const uint64_t n = (w.counters[1] & 1) ? (uint64_t)(uint32_t)w.counters[0] + 1 : 0;
+  reset_words(c);
+  block_off.release();
+  build_graph(c, keys.as<uint64_t>(), lines, n, g);
+}
+
+void load_tsv(Ctx* c, const char* bytes, uint64_t len, Graph& g) {
+  DBuf dbuf(c, parse_padded_bytes(len));
+  zero(c, dbuf.get(), dbuf.bytes());
+  copy_h2d(c, dbuf.get(), bytes, len);
+  graph_from_device_bytes(c, dbuf.as<uint8_t>(), len, g);
+}
+
+void load_pairs(Ctx* c, const uint64_t* xy, uint64_t count, Graph& g) {
+  DBuf keys(c, (count ? count : 1) * sizeof(uint64_t));
+  copy_h2d(c, keys.get(), xy, count * sizeof(uint64_t));
+  DBuf mx(c, 8);
+  zero(c, mx.get(), 8);
+  if (count) {
+    k_canon_pairs<<<grid_for(count, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        keys.as<uint64_t>(), count, mx.as<unsigned int>(), mx.as<unsigned int>() + 1);
+    KT_LAUNCHED(c);
+  }
+  uint32_t h[2];
+  copy_d2h(c, h, mx.get(), 8);
+  const uint64_t n = h[1] ? (uint64_t)h[0] + 1 : 0;
+  build_graph(c, keys.as<uint64_t>(), count, n, g);
+}
+
+// File ingest: mmap, then copy through two pinned staging buffers so the
+// host-side copy of one chunk overlaps the device copy of the previous one.
+static void load_tsv_file(Ctx* c, const char* path, Graph& g) {
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) throw Error(KT_ERR_IO, std::string("open file error: ") + std::strerror(errno));
+  struct stat sb;
+  if (fstat(fd, &sb) < 0) {
+    const int e = errno;
+    close(fd);
+    throw Error(KT_ERR_IO, std::string("get file length error: ") + std::strerror(e));
+  }
+  const uint64_t len = (uint64_t)sb.st_size;
+  void* map = len ? mmap(nullptr, len, PROT_READ, MAP_SHARED, fd, 0) : MAP_FAILED;
+  if (map == MAP_FAILED) {
+    // The reference maps the file the same way and fails identically on an
+    // empty file (src/mapfile.hpp:50-54).
+    const int e = len ? errno : EINVAL;
+    close(fd);
+    throw Error(KT_ERR_IO, std::string("mmap file error: ") + std::strerror(e));
+  }
+  madvise(map, len, MADV_SEQUENTIAL);
+  struct Unmap {
+    void* p;
+    uint64_t n;
+    int fd;
+    ~Unmap() {
+      munmap(p, n);
+      close(fd);
+    }
+  } unmap{map, len, fd};
+  DBuf dbuf(c, parse_padded_bytes(len));
+  zero(c, dbuf.get(), dbuf.bytes());
+  const uint64_t chunk = (uint64_t)std::max<int64_t>(1, c->opt.parse_pipeline_mb) << 20;
+  char* stage[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  struct Pinned {
+    char** s;
+    cudaEvent_t* d;
+    ~Pinned() {
+      for (int i = 0; i < 2; ++i) {
+        if (d[i]) {
+          cudaEventSynchronize(d[i]);
+          cudaEventDestroy(d[i]);
+        }
+        if (s[i]) cudaFreeHost(s[i]);
+      }
+    }
+  } pinned{stage, done};
+  for (int i = 0; i < 2; ++i) {
+    KT_CUDA(cudaHostAlloc(&stage[i], chunk, cudaHostAllocDefault));
+    KT_CUDA(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+  }
+  const char* src = static_cast<const char*>(map);
+  int slot = 0;
+  for (uint64_t off = 0; off < len; off += chunk, slot ^= 1) {
+    const uint64_t n = std::min(chunk, len - off);
+    KT_CUDA(cudaEventSynchronize(done[slot]));
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < 16; ++t) {
+      const uint64_t a = n * t / 16, b = n * (t + 1) / 16;
+      std::memcpy(stage[slot] + a, src + off + a, b - a);
+    }
+    KT_CUDA(cudaMemcpyAsync(dbuf.as<char>() + off, stage[slot], n, cudaMemcpyHostToDevice, c->stream));
+    KT_CUDA(cudaEventRecord(done[slot], c->stream));
+  }
+  graph_from_device_bytes(c, dbuf.as<uint8_t>(), len, g);
+}
+
+}  // namespace kt
+
+using kt::Error;
+
+#define KT_API_BEGIN(ctx)                            \
+  if (!(ctx)) return KT_ERR_INVALID;                 \
+  std::lock_guard<std::recursive_mutex> lk_((ctx)->c.mu); \
+  try {                                              \
+    KT_CUDA(cudaSetDevice((ctx)->c.device));
+#define KT_API_END(ctx)                              \
+  return KT_OK;                                      \
+  }                                                  \
+  catch (const Error& e) {                           \
+    (ctx)->c.last_error = e.what();                  \
+    return e.status;                                 \
+  }                                                  \
+  catch (const std::bad_alloc&) {                    \
+    (ctx)->c.last_error = "host allocation failed";  \
+    return KT_ERR_NOMEM;                             \
+  }                                                  \
+  catch (const std::exception& e) {                  \
+    (ctx)->c.last_error = e.what();                  \
+    return KT_ERR_CUDA;                              \
+  }
+
+extern "C" {
+
+const char* kt_status_string(kt_status s) {
+  switch (s) {
+    case KT_OK: return "ok";
+    case KT_ERR_INVALID: return "invalid argument";
+    case KT_ERR_CUDA: return "CUDA error";
+    case KT_ERR_NOMEM: return "out of device memory";
+    case KT_ERR_PARSE: return "malformed input";
+    case KT_ERR_IO: return "I/O error";
+    case KT_ERR_TIMEOUT: return "device wait timed out";
+    case KT_ERR_LIMIT: return "size limit exceeded";
+    case KT_ERR_NODEV: return "no CUDA device";
+    case KT_ERR_BUSY: return "busy";
+  }
+  return "unknown status";
+}
+
+kt_status kt_init(int device, uint64_t budget, kt_ctx** out) {
+  if (!out) return KT_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return KT_ERR_NODEV;
+  }
+  if (device < 0 || device >= ndev) return KT_ERR_INVALID;
+  kt_ctx* h = new (std::nothrow) kt_ctx;
+  if (!h) return KT_ERR_NOMEM;
+  kt::Ctx& c = h->c;
+  c.device = device;
+  try {
+    KT_CUDA(cudaSetDevice(device));
+    KT_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+    KT_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    size_t fr = 0, tot = 0;
+    KT_CUDA(cudaMemGetInfo(&fr, &tot));
+    c.budget = budget ? budget : (uint64_t)(fr * 0.9);
+    // Keep freed blocks in the pool for reuse across calls.
+    cudaMemPool_t pool;
+    KT_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    KT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    KT_CUDA(cudaHostAlloc(&c.pinned, 4096, cudaHostAllocDefault));
+    for (auto& e : c.ev) KT_CUDA(cudaEventCreate(&e));
+    c.words.alloc(&c, sizeof(kt::DevWords));
+    kt::reset_words(&c);
+    kt::sync(&c);
+  } catch (const Error&) {
+    kt_destroy(h);
+    return KT_ERR_CUDA;
+  }
+  *out = h;
+  return KT_OK;
+}
+
+void kt_destroy(kt_ctx* h) {
+  if (!h) return;
+  {
+    std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+    cudaSetDevice(h->c.device);
+    h->c.words.release();
+    if (h->c.stream) cudaStreamSynchronize(h->c.stream);
+    for (auto& e : h->c.ev)
+      if (e) cudaEventDestroy(e);
+    if (h->c.pinned) cudaFreeHost(h->c.pinned);
+    if (h->c.stream) cudaStreamDestroy(h->c.stream);
+  }
+  delete h;
+}
+
+const char* kt_last_error(const kt_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
+
+static int64_t* option_slot(kt::Options& o, const char* name) {
+  if (!name) return nullptr;
+  struct {
+    const char* n;
+    int64_t* p;
+  } tab[] = {{"predict", &o.predict},
+             {"persistent", &o.persistent},
+             {"support_bitmap_max_n", &o.support_bitmap_max_n},
+             {"timeout_ms", &o.timeout_ms},
+             {"parse_pipeline_mb", &o.parse_pipeline_mb},
+             {"record_kernel_times", &o.record_kernel_times},
+             {"debug_checks", &o.debug_checks}};
+  for (auto& t : tab)
+    if (!std::strcmp(t.n, name)) return t.p;
+  return nullptr;
+}
+
+kt_status kt_set_option(kt_ctx* h, const char* name, int64_t value) {
+  if (!h) return KT_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+  int64_t* p = option_slot(h->c.opt, name);
+  if (!p) return KT_ERR_INVALID;
+  *p = value;
+  return KT_OK;
+}
+
+kt_status kt_get_option(const kt_ctx* h, const char* name, int64_t* value) {
+  if (!h || !value) return KT_ERR_INVALID;
+  int64_t* p = option_slot(const_cast<kt::Options&>(h->c.opt), name);
+  if (!p) return KT_ERR_INVALID;
+  *value = *p;
+  return KT_OK;
+}
+
+kt_status kt_load_tsv(kt_ctx* h, const char* bytes, uint64_t len, kt_graph** out) {
+  if (!out || (!bytes && len)) return KT_ERR_INVALID;
+  *out = nullptr;
+  KT_API_BEGIN(h)
+  kt_graph* g = new kt_graph;
+  try {
+    kt::load_tsv(&h->c, bytes, len, g->g);
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  *out = g;
+  KT_API_END(h)
+}
+
+kt_status kt_load_tsv_file(kt_ctx* h, const char* path, kt_graph** out) {
+  if (!out || !path) return KT_ERR_INVALID;
+  *out = nullptr;
+  KT_API_BEGIN(h)
+  kt_graph* g = new kt_graph;
+  try {
+    kt::load_tsv_file(&h->c, path, g->g);
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  *out = g;
+  KT_API_END(h)
+}
+
+kt_status kt_load_pairs(kt_ctx* h, const uint64_t* xy, uint64_t count, kt_graph** out) {
+  if (!out || (!xy && count)) return KT_ERR_INVALID;
+  *out = nullptr;
+  KT_API_BEGIN(h)
+  kt_graph* g = new kt_graph;
+  try {
+    kt::load_pairs(&h->c, xy, count, g->g);
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  *out = g;
+  KT_API_END(h)
+}
+
+kt_status kt_graph_info(const kt_graph* g, uint64_t* nv, uint64_t* ne) {
+  if (!g) return KT_ERR_INVALID;
+  if (nv) *nv = g->g.n;
+  if (ne) *ne = g->g.m;
+  return KT_OK;
+}
+
+kt_status kt_graph_edges(kt_ctx* h, const kt_graph* g, uint64_t* keys) {
+  if (!g || (!keys && g->g.m)) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::copy_d2h(&h->c, keys, g->g.edges.get(), g->g.m * sizeof(uint64_t));
+  KT_API_END(h)
+}
+
+void kt_graph_free(kt_ctx* h, kt_graph* g) {
+  if (!g) return;
+  if (h) {
+    std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+    cudaSetDevice(h->c.device);
+    delete g;
+  } else {
+    delete g;
+  }
+}
+
+kt_status kt_solve(kt_ctx* h, kt_graph* g, uint32_t* kmax, uint64_t* edges) {
+  if (!g || !kmax || !edges) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::reset_words(&h->c);
+  kt::solve_graph(&h->c, g->g, kmax, edges);
+  KT_API_END(h)
+}
+
+kt_status kt_solve_tsv(kt_ctx* h, const char* bytes, uint64_t len, uint32_t* kmax, uint64_t* edges) {
+  if (!kmax || !edges || (!bytes && len)) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Graph g;
+  kt::load_tsv(&h->c, bytes, len, g);
+  kt::solve_graph(&h->c, g, kmax, edges);
+  KT_API_END(h)
+}
+
+kt_status kt_kcore(kt_ctx* h, kt_graph* g, uint32_t k, uint8_t* member, uint32_t* cmax) {
+  if (!g) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::KCore kc;
+  kc.init(c, g->g);
+  const uint32_t cm = kc.find_max_core(c);
+  if (cmax) *cmax = cm;
+  if (member && g->g.n) {
+    kt::DBuf d(c, g->g.n);
+    if (k == 0) {
+      KT_CUDA(cudaMemsetAsync(d.get(), 1, g->g.n, c->stream));
+    } else if (k > cm) {
+      kt::zero(c, d.get(), g->g.n);
+    } else {
+      kc.restore_core(c, k);
+      kc.members(c, d.as<uint8_t>());
+    }
+    kt::copy_d2h(c, member, d.get(), g->g.n);
+  }
+  KT_API_END(h)
+}
+
+kt_status kt_core_numbers(kt_ctx* h, kt_graph* g, uint32_t* core) {
+  if (!g || (!core && g->g.n)) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::KCore kc;
+  kc.init(c, g->g);
+  kt::DBuf d(c, (g->g.n ? g->g.n : 1) * sizeof(uint32_t));
+  kc.core_numbers(c, d.as<uint32_t>());
+  kt::copy_d2h(c, core, d.get(), g->g.n * sizeof(uint32_t));
+  KT_API_END(h)
+}
+
+kt_status kt_edge_support(kt_ctx* h, kt_graph* g, uint32_t* sup) {
+  if (!g || (!sup && g->g.m)) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::DBuf d(c, (g->g.m ? g->g.m : 1) * sizeof(uint32_t));
+  kt::zero(c, d.get(), d.bytes());
+  kt::graph_support(c, g->g, d.as<uint32_t>());
+  kt::copy_d2h(c, sup, d.get(), g->g.m * sizeof(uint32_t));
+  KT_API_END(h)
+}
+
+kt_status kt_edge_trussness(kt_ctx* h, kt_graph* g, uint32_t* truss) {
+  if (!g || (!truss && g->g.m)) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::DBuf d(c, (g->g.m ? g->g.m : 1) * sizeof(uint32_t));
+  kt::zero(c, d.get(), d.bytes());
+  kt::reset_words(c);
+  kt::graph_trussness(c, g->g, d.as<uint32_t>());
+  kt::copy_d2h(c, truss, d.get(), g->g.m * sizeof(uint32_t));
+  KT_API_END(h)
+}
+
+kt_status kt_get_stats(const kt_ctx* h, kt_stats* out) {
+  if (!h || !out) return KT_ERR_INVALID;
+  *out = h->c.stats;
+  out->kernel_launches = h->c.launches;
+  out->device_bytes_peak = h->c.peak;
+  return KT_OK;
+}
+
+kt_status kt_stats_reset(kt_ctx* h) {
+  if (!h) return KT_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+  h->c.stats = kt_stats{};
+  h->c.launches = 0;
+  h->c.peak = h->c.in_use;
+  return KT_OK;
+}
+
+}  // extern "C"

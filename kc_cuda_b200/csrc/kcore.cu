@@ -1,0 +1,397 @@
+// Stage (c): k-core peeling on the full graph.
+//
+// A probe peels the current vertex set to its k-core: the vertices of degree
+// < k form the first frontier, and each round removes the frontier and
+// decrements the degrees of its surviving neighbours; a neighbour whose
+// degree steps from k to k-1 (atomicSub returns k) joins the next frontier,
+// so every vertex enters a frontier at most once.  Rows of more than
+// kBigRow entries are expanded by whole blocks, in chunks, so hub rows do
+// not serialise on one warp.
+//
+// The search for the maximum core (the reference steps k by a fixed stride
+// with host backups, src/kc.cu:770-884) ramps k geometrically from the
+// current core (each success is permanent; removed vertices keep the probe's
+// tag), then bisects; a probe that empties the graph is undone by reviving
+// its tag and recounting degrees.  The tags of successful probes increase
+// with their level, which lets any lower core be restored later without a
+// snapshot: revive the vertices whose tag is newer than the last probe at or
+// below that level, recount degrees, and probe once more.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "compact.cuh"
+#include "kcore.h"
+
+namespace kt {
+namespace {
+
+constexpr unsigned kBigRow = 2048;
+constexpr unsigned kChunkRow = 1024;
+
+struct AliveF {
+  const uint32_t* rem;
+  __device__ bool keep(uint64_t v) const { return rem[v] == kAlive; }
+  __device__ uint32_t value(uint64_t v) const { return (uint32_t)v; }
+};
+
+__global__ void k_init_state(const uint32_t* __restrict__ deg0, uint64_t n, uint32_t* __restrict__ deg,
+                             uint32_t* __restrict__ rem) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = deg0[v];
+    deg[v] = d;
+    rem[v] = d ? kAlive : 0u;  // isolated vertices leave at tag 0 (level 1)
+  }
+}
+
+// Warp-aggregated push of `want` lanes into list[cnt...].
+__device__ __forceinline__ void push_warp(bool want, uint32_t item, uint32_t* list, unsigned long long* cnt,
+                                          uint64_t cap, uint32_t* err) {
+  const unsigned b = __ballot_sync(__activemask(), want);
+  if (!b) return;
+  const unsigned leader = __ffs(b) - 1;
+  unsigned long long base = 0;
+  if (lane_id() == leader) base = atomicAdd(cnt, (unsigned long long)__popc(b));
+  base = __shfl_sync(__activemask(), base, leader);
+  if (want) {
+    const unsigned long long p = base + __popc(b & lanemask_lt());
+    if (p < cap)
+      list[p] = item;
+    else
+      atomicOr(err, kDevErrCapacity);
+  }
+}
+
+__global__ void k_frontier_init(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint32_t* __restrict__ deg,
+                                uint32_t* __restrict__ rem, uint32_t k, uint32_t tag, uint32_t* __restrict__ front,
+                                unsigned long long* fcnt, uint64_t cap, uint32_t* err) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((n_alive + 31) & ~31ULL);
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    bool want = false;
+    uint32_t v = 0;
+    if (i < n_alive) {
+      v = alive[i];
+      if (rem[v] == kAlive && deg[v] < k) {
+        rem[v] = tag;
+        want = true;
+      }
+    }
+    push_warp(want, v, front, fcnt, cap, err);
+  }
+}
+
+// Removes the frontier: warp per vertex; rows longer than kBigRow go to the
+// big list for k_expand_big.
+__global__ void k_expand(const uint32_t* __restrict__ front, uint64_t nf, const uint64_t* __restrict__ off,
+                         const uint32_t* __restrict__ adj, uint32_t* __restrict__ deg, uint32_t* __restrict__ rem,
+                         uint32_t k, uint32_t tag, uint32_t* __restrict__ next, unsigned long long* ncnt,
+                         uint32_t* __restrict__ big, unsigned long long* nbig, uint64_t cap, uint32_t* err) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t f = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); f < nf; f += warps) {
+    const uint32_t v = front[f];
+    const uint64_t b = off[v], e = off[v + 1];
+    if (e - b > kBigRow) {
+      if (lane_id() == 0) {
+        const unsigned long long p = atomicAdd(nbig, 1ULL);
+        if (p < cap)
+          big[p] = v;
+        else
+          atomicOr(err, kDevErrCapacity);
+      }
+      continue;
+    }
+    for (uint64_t j = b + lane_id(); j < ((e - b + 31) & ~31ULL) + b; j += 32) {
+      bool want = false;
+      uint32_t w = 0;
+      if (j < e) {
+        w = adj[j];
+        if (rem[w] == kAlive) {
+          const uint32_t old = atomicSub(&deg[w], 1u);
+          if (old == k) {
+            rem[w] = tag;
+            want = true;
+          }
+        }
+      }
+      push_warp(want, w, next, ncnt, cap, err);
+    }
+  }
+}
+
+// Big rows: every block takes chunks of every big row.
+__global__ void k_expand_big(const uint32_t* __restrict__ big, const unsigned long long* nbig_p,
+                             const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
+                             uint32_t* __restrict__ deg, uint32_t* __restrict__ rem, uint32_t k, uint32_t tag,
+                             uint32_t* __restrict__ next, unsigned long long* ncnt, uint64_t cap, uint32_t* err) {
+  const uint64_t nbig = *nbig_p;
+  uint64_t chunk_base = 0;
+  for (uint64_t bi = 0; bi < nbig; ++bi) {
+    const uint32_t v = big[bi];
+    const uint64_t b = off[v], e = off[v + 1];
+    const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
+    // Chunks are numbered across all big rows so blocks stay balanced.
+    for (uint64_t cidx = (blockIdx.x + gridDim.x - chunk_base % gridDim.x) % gridDim.x; cidx < chunks;
+         cidx += gridDim.x) {
+      const uint64_t cb = b + cidx * kChunkRow, ce = min(e, cb + kChunkRow);
+      for (uint64_t j = cb + threadIdx.x; j < cb + ((ce - cb + 31) & ~31ULL); j += blockDim.x) {
+        bool want = false;
+        uint32_t w = 0;
+        if (j < ce) {
+          w = adj[j];
+          if (rem[w] == kAlive) {
+            const uint32_t old = atomicSub(&deg[w], 1u);
+            if (old == k) {
+              rem[w] = tag;
+              want = true;
+            }
+          }
+        }
+        push_warp(want, w, next, ncnt, cap, err);
+      }
+    }
+    chunk_base += chunks;
+  }
+}
+
+// deg[v] = alive neighbours of v, for v in the alive list (big rows by blocks).
+__global__ void k_recount(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint64_t* __restrict__ off,
+                          const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
+                          uint32_t* __restrict__ deg, uint32_t* __restrict__ big, unsigned long long* nbig,
+                          uint64_t cap, uint32_t* err) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); i < n_alive; i += warps) {
+    const uint32_t v = alive[i];
+    const uint64_t b = off[v], e = off[v + 1];
+    if (e - b > kBigRow) {
+      if (lane_id() == 0) {
+        deg[v] = 0;
+        const unsigned long long p = atomicAdd(nbig, 1ULL);
+        if (p < cap)
+          big[p] = v;
+        else
+          atomicOr(err, kDevErrCapacity);
+      }
+      continue;
+    }
+    uint32_t c = 0;
+    for (uint64_t j = b + lane_id(); j < e; j += 32) c += rem[adj[j]] == kAlive;
+    c = warp_sum(c);
+    if (lane_id() == 0) deg[v] = c;
+  }
+}
+
+__global__ void k_recount_big(const uint32_t* __restrict__ big, const unsigned long long* nbig_p,
+                              const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
+                              const uint32_t* __restrict__ rem, uint32_t* __restrict__ deg) {
+  __shared__ uint32_t tmp[33];
+  const uint64_t nbig = *nbig_p;
+  for (uint64_t bi = 0; bi < nbig; ++bi) {
+    const uint32_t v = big[bi];
+    const uint64_t b = off[v], e = off[v + 1];
+    const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
+    uint32_t c = 0;
+    for (uint64_t cidx = blockIdx.x; cidx < chunks; cidx += gridDim.x) {
+      const uint64_t cb = b + cidx * kChunkRow, ce = min(e, cb + kChunkRow);
+      for (uint64_t j = cb + threadIdx.x; j < ce; j += blockDim.x) c += rem[adj[j]] == kAlive;
+    }
+    c = block_sum<uint32_t>(c, tmp);
+    if (threadIdx.x == 0 && c) atomicAdd(&deg[v], c);
+  }
+}
+
+__global__ void k_revive(uint32_t* __restrict__ rem, uint64_t n, uint32_t newer_than) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = rem[v];
+    if (r != kAlive && r > newer_than) rem[v] = kAlive;
+  }
+}
+
+__global__ void k_min_alive_deg(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint32_t* __restrict__ deg,
+                                const uint32_t* __restrict__ rem, uint32_t* out) {
+  uint32_t mn = 0xffffffffu;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = alive[i];
+    if (rem[v] == kAlive) mn = min(mn, deg[v]);
+  }
+  mn = warp_min(mn);
+  if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(out, mn);
+}
+
+__global__ void k_members(const uint32_t* __restrict__ rem, uint64_t n, uint8_t* __restrict__ out) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    out[v] = rem[v] == kAlive;
+}
+
+__global__ void k_core_from_tags(const uint32_t* __restrict__ rem, uint64_t n, const uint32_t* __restrict__ level,
+                                 uint32_t* __restrict__ core) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = rem[v];
+    core[v] = r == kAlive ? 0u : level[r] - 1;
+  }
+}
+
+}  // namespace
+
+void KCore::init(Ctx* c, const Graph& gr) {
+  g = &gr;
+  n = gr.n;
+  deg.ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  rem.ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  alive.ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  front[0].ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  front[1].ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  big.ensure(c, (n ? n : 1) * sizeof(uint32_t));
+  cnt.ensure(c, 8 * sizeof(unsigned long long));
+  if (n) {
+    k_init_state<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(gr.deg.as<uint32_t>(), n,
+                                                                             deg.as<uint32_t>(), rem.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
+  levels.assign(1, 1);  // tag 0 = isolated, left at level 1
+  rebuild_alive(c);
+}
+
+void KCore::rebuild_alive(Ctx* c) {
+  n_alive = compact(c, n, AliveF{rem.as<uint32_t>()}, alive.as<uint32_t>());
+}
+
+void KCore::recount(Ctx* c) {
+  if (!n_alive) return;
+  zero(c, cnt.get(), cnt.bytes());
+  unsigned long long* nbig = cnt.as<unsigned long long>() + 4;
+  k_recount<<<grid_for(n_alive * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      alive.as<uint32_t>(), n_alive, g->off.as<uint64_t>(), g->adj.as<uint32_t>(), rem.as<uint32_t>(),
+      deg.as<uint32_t>(), big.as<uint32_t>(), nbig, n, &dev_words(c)->err);
+  KT_LAUNCHED(c);
+  k_recount_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), nbig, g->off.as<uint64_t>(),
+                                                       g->adj.as<uint32_t>(), rem.as<uint32_t>(),
+                                                       deg.as<uint32_t>());
+  KT_LAUNCHED(c);
+}
+
+uint64_t KCore::probe(Ctx* c, uint32_t k) {
+  const uint32_t tag = (uint32_t)levels.size();
+  if (tag >= 0xfffffff0u) throw Error(KT_ERR_LIMIT, "k-core: too many probes");
+  levels.push_back(k);
+  if (!n_alive) return 0;
+  unsigned long long* cn = cnt.as<unsigned long long>();
+  zero(c, cnt.get(), cnt.bytes());
+  uint32_t* err = &dev_words(c)->err;
+  k_frontier_init<<<grid_for(n_alive, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), k, tag, front[0].as<uint32_t>(), cn + 0,
+      n, err);
+  KT_LAUNCHED(c);
+  uint64_t removed = 0;
+  int cur = 0;
+  uint64_t rounds_here = 0;
+  while (true) {
+    const uint64_t nf = read_word<unsigned long long>(c, cn + cur);
+    if (nf == 0) break;
+    removed += nf;
+    ++rounds_here;
+    KT_CUDA(cudaMemsetAsync(cn + (cur ^ 1), 0, sizeof(unsigned long long), c->stream));
+    KT_CUDA(cudaMemsetAsync(cn + 4, 0, sizeof(unsigned long long), c->stream));
+    k_expand<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        front[cur].as<uint32_t>(), nf, g->off.as<uint64_t>(), g->adj.as<uint32_t>(), deg.as<uint32_t>(),
+        rem.as<uint32_t>(), k, tag, front[cur ^ 1].as<uint32_t>(), cn + (cur ^ 1), big.as<uint32_t>(), cn + 4, n,
+        err);
+    KT_LAUNCHED(c);
+    k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g->off.as<uint64_t>(),
+                                                        g->adj.as<uint32_t>(), deg.as<uint32_t>(),
+                                                        rem.as<uint32_t>(), k, tag, front[cur ^ 1].as<uint32_t>(),
+                                                        cn + (cur ^ 1), n, err);
+    KT_LAUNCHED(c);
+    cur ^= 1;
+  }
+  rounds += rounds_here;
+  check_words(c, "k-core probe");
+  const uint64_t left = n_alive - removed;
+  return left;
+}
+
+uint32_t KCore::find_max_core(Ctx* c) {
+  succ.assign(1, 0);  // tag 0: isolated vertices (level 1)
+  if (!n_alive) {
+    cmax = 0;
+    return 0;
+  }
+  // Upper bound: a k-core holds >= k(k+1)/2 edges.
+  const double m = (double)g->m;
+  uint64_t ub = (uint64_t)std::floor((std::sqrt(1.0 + 8.0 * m) - 1.0) / 2.0);
+  ub = std::min<uint64_t>(ub, g->max_deg);
+  uint64_t lo = 1, hi = ub + 1;  // the 1-core (non-isolated vertices) is non-empty
+  bool ramp = true;
+  while (hi - lo > 1) {
+    uint64_t k = ramp ? std::min<uint64_t>(lo * 2, hi - 1) : lo + (hi - lo) / 2;
+    if (k <= lo) k = lo + 1;
+    const uint32_t tag = (uint32_t)levels.size();
+    const uint64_t left = probe(c, (uint32_t)k);
+    if (left) {
+      lo = k;
+      succ.push_back(tag);
+      rebuild_alive(c);
+    } else {
+      hi = k;
+      ramp = false;
+      // Undo: revive this probe's vertices and recount their degrees.
+      k_revive<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n, tag - 1);
+      KT_LAUNCHED(c);
+      levels.pop_back();
+      recount(c);
+    }
+  }
+  cmax = (uint32_t)lo;
+  return cmax;
+}
+
+void KCore::restore_core(Ctx* c, uint32_t k) {
+  // Last successful probe at or below level k; everything newer is revived.
+  uint32_t keep = 0;
+  for (uint32_t t : succ)
+    if (levels[t] <= k) keep = std::max(keep, t);
+  k_revive<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n, keep);
+  KT_LAUNCHED(c);
+  levels.resize(keep + 1);
+  std::vector<uint32_t> s2;
+  for (uint32_t t : succ)
+    if (t <= keep) s2.push_back(t);
+  succ.swap(s2);
+  rebuild_alive(c);
+  recount(c);
+  const uint32_t tag = (uint32_t)levels.size();
+  if (probe(c, k)) {
+    succ.push_back(tag);
+  }
+  rebuild_alive(c);
+}
+
+void KCore::members(Ctx* c, uint8_t* dout) {
+  if (!n) return;
+  k_members<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n, dout);
+  KT_LAUNCHED(c);
+}
+
+void KCore::core_numbers(Ctx* c, uint32_t* dcore) {
+  // Peel level by level: the alive set is always a d-core where d is its
+  // minimum degree, so the probe at d+1 removes exactly the core-d vertices.
+  DBuf mn(c, 4);
+  while (n_alive) {
+    KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));
+    k_min_alive_deg<<<grid_for(n_alive, 256, c->num_sms * 8), 256, 0, c->stream>>>(
+        alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), mn.as<uint32_t>());
+    KT_LAUNCHED(c);
+    const uint32_t d = read_word<uint32_t>(c, mn.as<uint32_t>());
+    probe(c, d + 1);
+    rebuild_alive(c);
+  }
+  DBuf lv(c, levels.size() * sizeof(uint32_t));
+  copy_h2d(c, lv.get(), levels.data(), levels.size() * sizeof(uint32_t));
+  if (n) {
+    k_core_from_tags<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n,
+                                                                                 lv.as<uint32_t>(), dcore);
+    KT_LAUNCHED(c);
+  }
+  sync(c);
+}
+
+}  // namespace kt

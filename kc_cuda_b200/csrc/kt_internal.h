@@ -1,0 +1,166 @@
+// Host-side internals shared by the solver's translation units: the context,
+// device buffers charged to the context's HBM budget, error propagation and
+// launch accounting.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kt.h"
+
+namespace kt {
+
+// Exceptions carry a status to the C boundary (api.cu), where they become
+// return codes; nothing is thrown across extern "C".
+struct Error : std::runtime_error {
+  kt_status status;
+  Error(kt_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define KT_CUDA(call)                                                   \
+  do {                                                                  \
+    cudaError_t kt_e_ = (call);                                         \
+    if (kt_e_ != cudaSuccess) ::kt::throw_cuda(kt_e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define KT_LAUNCHED(ctx)                                                   \
+  do {                                                                     \
+    cudaError_t kt_e_ = cudaGetLastError();                                \
+    if (kt_e_ != cudaSuccess) ::kt::throw_cuda(kt_e_, "kernel launch", __FILE__, __LINE__); \
+    (ctx)->launches++;                                                     \
+  } while (0)
+
+// Tunables, settable by name through kt_set_option.
+struct Options {
+  int64_t predict = 1;            // run the prediction phase (truss of the max core)
+  int64_t persistent = 1;         // peel / k-core rounds inside one cooperative launch
+  int64_t support_bitmap_max_n = 1 << 20;  // vertex-centric bitmap support up to this many vertices
+  int64_t timeout_ms = 20000;     // bound on any device-side wait
+  int64_t parse_pipeline_mb = 256;  // host->device chunk for file ingest
+  int64_t record_kernel_times = 0;  // events around support / peel kernels
+  int64_t debug_checks = 0;       // extra host-side consistency checks
+};
+
+struct Ctx;
+
+// Device buffer charged to a context's budget; freed stream-ordered.
+class DBuf {
+ public:
+  DBuf() = default;
+  DBuf(Ctx* c, size_t bytes) { alloc(c, bytes); }
+  ~DBuf() { release(); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ctx_ = o.ctx_;
+      ptr_ = o.ptr_;
+      bytes_ = o.bytes_;
+      o.ctx_ = nullptr;
+      o.ptr_ = nullptr;
+      o.bytes_ = 0;
+    }
+    return *this;
+  }
+  void alloc(Ctx* c, size_t bytes);
+  void release();
+  // Grows (discarding contents) when smaller than `bytes`.
+  void ensure(Ctx* c, size_t bytes) {
+    if (bytes > bytes_) {
+      release();
+      alloc(c, bytes);
+    }
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(ptr_); }
+  size_t bytes() const { return bytes_; }
+  void* get() const { return ptr_; }
+
+ private:
+  Ctx* ctx_ = nullptr;
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+struct Stats {
+  kt_stats s{};
+};
+
+struct Ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;
+  uint64_t in_use = 0;
+  uint64_t peak = 0;
+  uint64_t launches = 0;
+  std::string last_error;
+  Options opt;
+  kt_stats stats{};
+  std::recursive_mutex mu;
+  // Pinned host words for small device-to-host reads.
+  uint64_t* pinned = nullptr;
+  cudaEvent_t ev[8] = {};
+  // Device word block: bounded-wait error flag, barrier state, counters.
+  DBuf words;
+};
+
+// Graph held on the device: cleaned, symmetric CSR (rows unsorted) plus the
+// sorted canonical edge list.
+struct Graph {
+  uint64_t n = 0;      // vertex ids 0..n-1
+  uint64_t m = 0;      // undirected edges
+  DBuf off;            // uint64[n + 1]
+  DBuf adj;            // uint32[2m]
+  DBuf edges;          // uint64[m], sorted u << 32 | v, u < v
+  DBuf deg;            // uint32[n]
+  uint32_t max_deg = 0;
+};
+
+// Stream-ordered helpers.
+void sync(Ctx* c);
+template <typename T>
+T read_word(Ctx* c, const T* dptr) {
+  static_assert(sizeof(T) <= 8, "word");
+  KT_CUDA(cudaMemcpyAsync(c->pinned, dptr, sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  T v;
+  memcpy(&v, c->pinned, sizeof(T));
+  return v;
+}
+void copy_d2h(Ctx* c, void* dst, const void* src, size_t bytes);
+void copy_h2d(Ctx* c, void* dst, const void* src, size_t bytes);
+void zero(Ctx* c, void* dptr, size_t bytes);
+
+// Device-wide primitives (scan.cu, sort.cu).
+// Exclusive scan of n uint32 values into uint64 (out may not alias in).
+void scan_u32_to_u64(Ctx* c, const uint32_t* in, uint64_t* out, uint64_t n);
+// Exclusive scan of n uint32 values in place-safe form into uint32 (out may alias in).
+void scan_u32(Ctx* c, const uint32_t* in, uint32_t* out, uint64_t n);
+// Sum of n uint32 values (device result in *dsum, also returned).
+uint64_t reduce_u32(Ctx* c, const uint32_t* in, uint64_t n);
+// Stable LSD radix sort of keys (and optional uint32 values) over the low
+// `bits` bits.  `keys`/`vals` hold the input and receive the output.
+void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits);
+// Sorted-unique compaction of keys (drops key == ~0).  Returns new count.
+uint64_t unique_sorted_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n);
+
+// Grid sizing.
+inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap) {
+  uint64_t g = (work + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+}  // namespace kt

@@ -1,0 +1,162 @@
+// The solve driver: ingest (a, b), k-core (c), support (d), peel (e).
+//
+// Two phases, as in the reference (src/kc_gpu.cpp:336-341):
+//   1. prediction: the maximum core's kmax-truss gives a lower bound L (a
+//      subgraph's truss is a truss of the graph);
+//   2. search: the (L-1)-core contains every L-truss, so the kmax-truss is
+//      found by peeling that core from level L.
+// Shortcuts, both exact: if L = cmax + 1 the upper bound (an edge's
+// trussness is at most its ends' core number + 1) is met and phase 2 is
+// skipped; if the L-truss found in phase 2 has exactly the edges of phase
+// 1's L-truss, it is that same truss and nothing above it exists.
+#include <algorithm>
+#include <chrono>
+
+#include "solve.h"
+
+namespace kt {
+namespace {
+
+__device__ __forceinline__ uint64_t lower_bound_u64(const uint64_t* a, uint64_t n, uint64_t x) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Scatters a per-edge value of the working graph back to the graph's
+// canonical edge order.
+__global__ void k_map_back(const uint64_t* __restrict__ ends, uint64_t m, const uint32_t* __restrict__ orig,
+                           const uint64_t* __restrict__ gedges, uint64_t gm, const uint32_t* __restrict__ val,
+                           uint32_t* __restrict__ out) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = ends[e];
+    const uint32_t a = orig[(uint32_t)(k >> 32)], b = orig[(uint32_t)k];
+    const uint64_t key = a < b ? (((uint64_t)a << 32) | b) : (((uint64_t)b << 32) | a);
+    const uint64_t p = lower_bound_u64(gedges, gm, key);
+    if (p < gm && gedges[p] == key) out[p] = val[e];
+  }
+}
+
+struct Timer {
+  Ctx* c;
+  cudaEvent_t a, b;
+  explicit Timer(Ctx* cx) : c(cx) {
+    KT_CUDA(cudaEventCreate(&a));
+    KT_CUDA(cudaEventCreate(&b));
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { KT_CUDA(cudaEventRecord(a, c->stream)); }
+  double stop() {
+    KT_CUDA(cudaEventRecord(b, c->stream));
+    KT_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    KT_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+};
+
+}  // namespace
+
+void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
+  kt_stats& st = c->stats;
+  st.ms_kcore = st.ms_subgraph = st.ms_support = st.ms_peel = 0;
+  st.core_vertices = st.core_edges = st.predict_vertices = st.predict_edges = 0;
+  st.levels = 0;
+  st.rounds = 0;
+  *kmax = 0;
+  *count = 0;
+  Timer tm(c);
+  tm.start();
+  KCore kc;
+  kc.init(c, g);
+  const uint32_t cmax = kc.find_max_core(c);
+  st.cmax = cmax;
+  st.ms_kcore += tm.stop();
+  if (g.m == 0 || cmax < 2) return;  // a triangle needs three vertices of degree >= 2
+
+  uint32_t L = 0;
+  uint64_t C = 0;
+  if (c->opt.predict) {
+    tm.start();
+    Sub s1;
+    build_sub(c, g, kc, s1);
+    st.predict_vertices = s1.n;
+    st.predict_edges = s1.m;
+    st.ms_subgraph += tm.stop();
+    tm.start();
+    DBuf sup1(c, (s1.m ? s1.m : 1) * sizeof(uint32_t));
+    edge_support(c, s1, sup1.as<uint32_t>());
+    st.ms_support += tm.stop();
+    tm.start();
+    const PeelResult p1 = truss_peel(c, s1, sup1.as<uint32_t>(), 3, 0, nullptr);
+    st.ms_peel += tm.stop();
+    st.levels += p1.levels;
+    st.rounds += (uint32_t)p1.rounds;
+    L = p1.kmax;
+    C = p1.count;
+    if (L >= 3 && L == cmax + 1) {
+      *kmax = L;
+      *count = C;
+      st.kmax_lower_bound = L;
+      return;
+    }
+  }
+  st.kmax_lower_bound = L;
+  tm.start();
+  kc.restore_core(c, L >= 3 ? L - 1 : 2);
+  st.ms_kcore += tm.stop();
+  tm.start();
+  Sub s2;
+  build_sub(c, g, kc, s2);
+  st.core_vertices = s2.n;
+  st.core_edges = s2.m;
+  st.ms_subgraph += tm.stop();
+  tm.start();
+  DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
+  edge_support(c, s2, sup2.as<uint32_t>());
+  st.ms_support += tm.stop();
+  tm.start();
+  const PeelResult p2 = truss_peel(c, s2, sup2.as<uint32_t>(), std::max<uint32_t>(L, 3), L >= 3 ? C : 0, nullptr);
+  st.ms_peel += tm.stop();
+  st.levels += p2.levels;
+  st.rounds += (uint32_t)p2.rounds;
+  *kmax = p2.kmax;
+  *count = p2.count;
+}
+
+void graph_support(Ctx* c, const Graph& g, uint32_t* dout) {
+  Sub s;
+  build_sub_all(c, g, s);
+  DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
+  edge_support(c, s, sup.as<uint32_t>());
+  if (s.m) {
+    k_map_back<<<grid_for(s.m, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.ends.as<uint64_t>(), s.m, s.orig.as<uint32_t>(), g.edges.as<uint64_t>(), g.m, sup.as<uint32_t>(), dout);
+    KT_LAUNCHED(c);
+  }
+}
+
+void graph_trussness(Ctx* c, const Graph& g, uint32_t* dout) {
+  Sub s;
+  build_sub_all(c, g, s);
+  DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
+  DBuf tr(c, (s.m ? s.m : 1) * sizeof(uint32_t));
+  edge_support(c, s, sup.as<uint32_t>());
+  truss_peel(c, s, sup.as<uint32_t>(), 3, 0, tr.as<uint32_t>());
+  if (s.m) {
+    k_map_back<<<grid_for(s.m, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.ends.as<uint64_t>(), s.m, s.orig.as<uint32_t>(), g.edges.as<uint64_t>(), g.m, tr.as<uint32_t>(), dout);
+    KT_LAUNCHED(c);
+  }
+}
+
+}  // namespace kt

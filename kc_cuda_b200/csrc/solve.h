@@ -1,0 +1,15 @@
+// Solve driver and per-graph stage outputs (solve.cu).
+#pragma once
+#include "subgraph.h"
+
+namespace kt {
+
+void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count);
+void graph_support(Ctx* c, const Graph& g, uint32_t* dout);
+void graph_trussness(Ctx* c, const Graph& g, uint32_t* dout);
+
+// ingest (api.cu): host TSV bytes / records -> Graph.
+void load_tsv(Ctx* c, const char* bytes, uint64_t len, Graph& g);
+void load_pairs(Ctx* c, const uint64_t* xy, uint64_t count, Graph& g);
+
+}  // namespace kt

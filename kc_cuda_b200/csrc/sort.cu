@@ -1,0 +1,158 @@
+// Stable LSD radix sort of 64-bit keys (optionally carrying a 32-bit value),
+// 8-bit digits.
+//
+// One pass = tile histograms -> digit-major exclusive scan -> stable scatter.
+// A tile is 4096 keys: each of the 8 warps owns 512 consecutive keys, ranks
+// them with __match_any_sync against warp-private running digit counters,
+// then the block turns the per-warp counts into per-warp digit offsets.  A
+// first pass histograms all eight digit positions at once so passes whose
+// digit is the same for every key are skipped.
+#include "kt_device.cuh"
+#include "kt_internal.h"
+
+namespace kt {
+namespace {
+
+constexpr unsigned kSortThreads = 256;
+constexpr unsigned kSortWarps = kSortThreads / 32;
+constexpr unsigned kSortIpt = 16;                       // keys per lane
+constexpr unsigned kWarpKeys = 32 * kSortIpt;           // 512
+constexpr unsigned kSortTile = kSortWarps * kWarpKeys;  // 4096
+
+__global__ void __launch_bounds__(kSortThreads) k_hist_all(const uint64_t* __restrict__ keys, uint64_t n,
+                                                           int passes, unsigned long long* __restrict__ hist) {
+  __shared__ uint32_t h[8][256];
+  for (unsigned i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+  __syncthreads();
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255], 1u);
+  }
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < (unsigned)passes * 256; i += blockDim.x) {
+    const uint32_t v = (&h[0][0])[i];
+    if (v) atomicAdd(&hist[i], (unsigned long long)v);
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_tile_hist(const uint64_t* __restrict__ keys, uint64_t n, int shift,
+                                                            uint32_t ntiles, uint32_t* __restrict__ tile_hist) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (unsigned i = 0; i < kSortTile / kSortThreads; ++i) {
+    const uint64_t j = base + i * kSortThreads + threadIdx.x;
+    if (j < n) atomicAdd(&h[(keys[j] >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  tile_hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+template <bool kVals>
+__global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __restrict__ keys,
+                                                          const uint32_t* __restrict__ vals, uint64_t n, int shift,
+                                                          uint32_t ntiles, const uint32_t* __restrict__ tile_off,
+                                                          uint64_t* __restrict__ keys_out,
+                                                          uint32_t* __restrict__ vals_out) {
+  __shared__ uint32_t wrun[kSortWarps][256];
+  __shared__ uint32_t toff[256];
+  const unsigned w = warp_id(), l = lane_id();
+  toff[threadIdx.x] = tile_off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+#pragma unroll
+  for (unsigned q = 0; q < kSortWarps; ++q) wrun[q][threadIdx.x] = 0;
+  __syncthreads();
+
+  const uint64_t wbase = (uint64_t)blockIdx.x * kSortTile + (uint64_t)w * kWarpKeys;
+  uint64_t k[kSortIpt];
+  uint32_t v[kSortIpt];
+  uint32_t rank[kSortIpt];
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (unsigned j = 0; j < kSortIpt; ++j) {
+    const uint64_t idx = wbase + j * 32 + l;
+    const bool valid = idx < n;
+    k[j] = valid ? keys[idx] : 0;
+    if (kVals) v[j] = valid ? vals[idx] : 0;
+    const uint32_t d = valid ? (uint32_t)((k[j] >> shift) & 255) : 256u;
+    const unsigned peers = __match_any_sync(kFull, d);
+    const uint32_t base = valid ? wrun[w][d] : 0u;
+    __syncwarp();
+    if (valid && l == (unsigned)(__ffs(peers) - 1)) wrun[w][d] = base + __popc(peers);
+    __syncwarp();
+    rank[j] = base + __popc(peers & lt);
+  }
+  __syncthreads();
+  {
+    const unsigned d = threadIdx.x;
+    uint32_t s = 0;
+#pragma unroll
+    for (unsigned q = 0; q < kSortWarps; ++q) {
+      const uint32_t t = wrun[q][d];
+      wrun[q][d] = s;
+      s += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (unsigned j = 0; j < kSortIpt; ++j) {
+    const uint64_t idx = wbase + j * 32 + l;
+    if (idx < n) {
+      const uint32_t d = (uint32_t)((k[j] >> shift) & 255);
+      const uint32_t pos = toff[d] + wrun[w][d] + rank[j];
+      keys_out[pos] = k[j];
+      if (kVals) vals_out[pos] = v[j];
+    }
+  }
+}
+
+}  // namespace
+
+void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits) {
+  if (n < 2 || bits <= 0) return;
+  if (n >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "radix sort: more than 2^32-1 keys");
+  if (bits > 64) bits = 64;
+  const int passes = (bits + 7) / 8;
+  DBuf hist(c, 8 * 256 * sizeof(unsigned long long));
+  zero(c, hist.get(), hist.bytes());
+  k_hist_all<<<grid_for(n, kSortThreads, c->num_sms * 8), kSortThreads, 0, c->stream>>>(
+      keys, n, passes, hist.as<unsigned long long>());
+  KT_LAUNCHED(c);
+  std::vector<unsigned long long> h(8 * 256);
+  copy_d2h(c, h.data(), hist.get(), h.size() * sizeof(unsigned long long));
+
+  const uint32_t ntiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  DBuf keys_alt(c, n * sizeof(uint64_t));
+  DBuf vals_alt;
+  if (vals) vals_alt.alloc(c, n * sizeof(uint32_t));
+  DBuf th(c, (uint64_t)ntiles * 256 * sizeof(uint32_t));
+  uint64_t* ksrc = keys;
+  uint64_t* kdst = keys_alt.as<uint64_t>();
+  uint32_t* vsrc = vals;
+  uint32_t* vdst = vals ? vals_alt.as<uint32_t>() : nullptr;
+  for (int p = 0; p < passes; ++p) {
+    int distinct = 0;
+    for (int d = 0; d < 256; ++d) distinct += h[p * 256 + d] != 0;
+    if (distinct <= 1) continue;
+    const int shift = 8 * p;
+    k_tile_hist<<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, n, shift, ntiles, th.as<uint32_t>());
+    KT_LAUNCHED(c);
+    scan_u32(c, th.as<uint32_t>(), th.as<uint32_t>(), (uint64_t)ntiles * 256);
+    if (vals)
+      k_scatter<true><<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, vsrc, n, shift, ntiles, th.as<uint32_t>(), kdst,
+                                                              vdst);
+    else
+      k_scatter<false><<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, nullptr, n, shift, ntiles, th.as<uint32_t>(),
+                                                               kdst, nullptr);
+    KT_LAUNCHED(c);
+    std::swap(ksrc, kdst);
+    std::swap(vsrc, vdst);
+  }
+  if (ksrc != keys) {
+    KT_CUDA(cudaMemcpyAsync(keys, ksrc, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+    if (vals) KT_CUDA(cudaMemcpyAsync(vals, vsrc, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+  }
+}
+
+}  // namespace kt

@@ -1,0 +1,24 @@
+// Stage entry points shared between the solver's translation units.
+#pragma once
+#include "kt_device.cuh"
+#include "kt_internal.h"
+
+namespace kt {
+
+void scan_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n);
+
+// parse.cu -- stage (a)
+uint64_t parse_padded_bytes(uint64_t len);
+uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& block_off);
+void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words);
+
+// csr.cu -- stage (b): canonical keys (any order, ~0 = none) -> Graph.
+// `keys` is consumed (sorted in place).
+void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g);
+
+DevWords* dev_words(Ctx* c);
+void reset_words(Ctx* c);
+// Throws the error a kernel flagged in the device words (if any).
+void check_words(Ctx* c, const char* stage);
+
+}  // namespace kt

@@ -1,0 +1,210 @@
+// Induced subgraph of the surviving vertices, relabelled by ascending
+// (degree, id), with sorted rows and edge ids.
+//
+// The reference builds the same relabelled, oriented structure on the host
+// (construct_Graph and build_nbr_direct, src/kc_gpu.cpp:68-126,
+// src/kc.cu:1405-1580, with CPU sorts of the ranks and of every row).  Here:
+// sort (degree << 32 | id) keys for the new order; emit every surviving
+// adjacency entry as (new u << 32 | new v); one radix sort over
+// 2*ceil(log2 n') bits gives the sorted rows; edge ids follow from the
+// per-row start of the upper part (neighbours > row), found by binary
+// search, and an exclusive scan of the upper-part sizes.
+#include "compact.cuh"
+#include "subgraph.h"
+
+namespace kt {
+namespace {
+
+int bits_for(uint64_t n) {
+  int b = 0;
+  while ((1ULL << b) < n) ++b;
+  return b;
+}
+
+__global__ void k_order_keys(const uint32_t* __restrict__ alive, uint64_t na, const uint32_t* __restrict__ deg,
+                             uint64_t* __restrict__ keys) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = alive[i];
+    keys[i] = ((uint64_t)deg[v] << 32) | v;
+  }
+}
+
+__global__ void k_order_apply(const uint64_t* __restrict__ keys, uint64_t na, uint32_t* __restrict__ orig,
+                              uint32_t* __restrict__ newid, uint32_t* __restrict__ sdeg) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const uint32_t v = (uint32_t)k;
+    orig[i] = v;
+    newid[v] = (uint32_t)i;
+    sdeg[i] = (uint32_t)(k >> 32);
+  }
+}
+
+// Emits (r << 32 | newid[w]) for every alive neighbour w of orig[r], at
+// off[r] + rank.  Warp per row.
+__global__ void k_emit(const uint32_t* __restrict__ orig, uint64_t na, const uint64_t* __restrict__ goff,
+                       const uint32_t* __restrict__ gadj, const uint32_t* __restrict__ rem,
+                       const uint32_t* __restrict__ newid, const uint64_t* __restrict__ soff,
+                       uint64_t* __restrict__ keys) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); r < na; r += warps) {
+    const uint32_t v = orig[r];
+    const uint64_t b = goff[v], e = goff[v + 1];
+    uint64_t pos = soff[r];
+    const uint64_t row_end = soff[r + 1];  // a degree mismatch must not spill into the next row
+    for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
+      bool keep = false;
+      uint32_t w = 0;
+      if (j < e) {
+        w = gadj[j];
+        keep = rem == nullptr || rem[w] == kAlive;
+      }
+      const unsigned bal = __ballot_sync(kFull, keep);
+      const uint64_t p = pos + __popc(bal & lanemask_lt());
+      if (keep && p < row_end) keys[p] = ((uint64_t)r << 32) | newid[w];
+      pos += __popc(bal);
+    }
+  }
+}
+
+__global__ void k_rows_from_keys(const uint64_t* __restrict__ keys, uint64_t n2, uint32_t* __restrict__ adj) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (uint64_t)gridDim.x * blockDim.x)
+    adj[i] = (uint32_t)keys[i];
+}
+
+// up[r] = first position in row r holding a neighbour > r.
+__global__ void k_upper_start(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj, uint64_t n,
+                              uint64_t* __restrict__ up, uint32_t* __restrict__ upcnt) {
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = off[r], hi = off[r + 1];
+    const uint64_t end = hi;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (adj[mid] <= (uint32_t)r)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    up[r] = lo;
+    upcnt[r] = (uint32_t)(end - lo);
+  }
+}
+
+// Edge ids: upper entries number themselves; a lower entry (r, c < r) finds
+// r in the upper part of row c.  Warp per row.
+__global__ void k_edge_ids(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj, uint64_t n,
+                           const uint64_t* __restrict__ up, const uint64_t* __restrict__ eoff,
+                           uint32_t* __restrict__ eid, uint64_t* __restrict__ ends) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); r < n; r += warps) {
+    const uint64_t b = off[r], e = off[r + 1], u0 = up[r];
+    for (uint64_t j = b + lane_id(); j < e; j += 32) {
+      const uint32_t col = adj[j];
+      if (j >= u0) {
+        const uint64_t id = eoff[r] + (j - u0);
+        eid[j] = (uint32_t)id;
+        ends[id] = (r << 32) | col;
+      } else {
+        uint64_t lo = up[col], hi = off[col + 1];
+        while (lo < hi) {
+          const uint64_t mid = (lo + hi) >> 1;
+          if (adj[mid] < (uint32_t)r)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        eid[j] = (uint32_t)(eoff[col] + (lo - up[col]));
+      }
+    }
+  }
+}
+
+struct DegPositive {
+  const uint32_t* deg;
+  __device__ bool keep(uint64_t v) const { return deg[v] > 0; }
+  __device__ uint32_t value(uint64_t v) const { return (uint32_t)v; }
+};
+
+void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
+                     const uint32_t* rem, Sub& s) {
+  if (na >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "subgraph: too many vertices");
+  s.n = (uint32_t)na;
+  s.orig.alloc(c, (na ? na : 1) * sizeof(uint32_t));
+  s.off.alloc(c, (na + 1) * sizeof(uint64_t));
+  s.up.alloc(c, (na ? na : 1) * sizeof(uint64_t));
+  if (na == 0) {
+    zero(c, s.off.get(), sizeof(uint64_t));
+    s.m = 0;
+    s.adj.alloc(c, 4);
+    s.eid.alloc(c, 4);
+    s.ends.alloc(c, 8);
+    return;
+  }
+  // New order.
+  DBuf okeys(c, na * sizeof(uint64_t));
+  k_order_keys<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(alive, na, deg, okeys.as<uint64_t>());
+  KT_LAUNCHED(c);
+  radix_sort_u64(c, okeys.as<uint64_t>(), nullptr, na, 64);
+  DBuf newid(c, (g.n ? g.n : 1) * sizeof(uint32_t));
+  DBuf sdeg(c, (na + 1) * sizeof(uint32_t));
+  zero(c, sdeg.get(), (na + 1) * sizeof(uint32_t));
+  k_order_apply<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>());
+  KT_LAUNCHED(c);
+  okeys.release();
+  scan_u32_to_u64(c, sdeg.as<uint32_t>(), s.off.as<uint64_t>(), na + 1);
+  const uint64_t n2 = read_word<uint64_t>(c, s.off.as<uint64_t>() + na);
+  if (n2 & 1) throw Error(KT_ERR_CUDA, "subgraph: odd adjacency size (inconsistent degrees)");
+  s.m = n2 / 2;
+  if (s.m >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "subgraph: more than 2^32-1 edges");
+  // Entries, sorted.
+  DBuf keys(c, (n2 ? n2 : 1) * sizeof(uint64_t));
+  k_emit<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.orig.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem, newid.as<uint32_t>(),
+      s.off.as<uint64_t>(), keys.as<uint64_t>());
+  KT_LAUNCHED(c);
+  newid.release();
+  const int vb = bits_for(na);
+  // Row in bits 32.., column in bits 0..vb-1: constant digits are skipped.
+  radix_sort_u64(c, keys.as<uint64_t>(), nullptr, n2, 64);
+  s.adj.alloc(c, (n2 ? n2 : 1) * sizeof(uint32_t));
+  if (n2) {
+    k_rows_from_keys<<<grid_for(n2, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys.as<uint64_t>(), n2,
+                                                                                  s.adj.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
+  keys.release();
+  (void)vb;
+  // Edge ids.
+  DBuf upcnt(c, (na + 1) * sizeof(uint32_t));
+  zero(c, upcnt.get(), (na + 1) * sizeof(uint32_t));
+  k_upper_start<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.off.as<uint64_t>(), s.adj.as<uint32_t>(), na, s.up.as<uint64_t>(), upcnt.as<uint32_t>());
+  KT_LAUNCHED(c);
+  DBuf eoff(c, (na + 1) * sizeof(uint64_t));
+  scan_u32_to_u64(c, upcnt.as<uint32_t>(), eoff.as<uint64_t>(), na + 1);
+  s.eid.alloc(c, (n2 ? n2 : 1) * sizeof(uint32_t));
+  s.ends.alloc(c, (s.m ? s.m : 1) * sizeof(uint64_t));
+  k_edge_ids<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.off.as<uint64_t>(), s.adj.as<uint32_t>(), na, s.up.as<uint64_t>(), eoff.as<uint64_t>(),
+      s.eid.as<uint32_t>(), s.ends.as<uint64_t>());
+  KT_LAUNCHED(c);
+  // Maximum degree (the last vertex in ascending-degree order).
+  uint32_t md = 0;
+  copy_d2h(c, &md, sdeg.as<uint32_t>() + (na - 1), sizeof(uint32_t));
+  s.max_deg = md;
+}
+
+}  // namespace
+
+void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s) {
+  build_from_list(c, g, kc.alive.as<uint32_t>(), kc.n_alive, kc.deg.as<uint32_t>(), kc.rem.as<uint32_t>(), s);
+}
+
+void build_sub_all(Ctx* c, const Graph& g, Sub& s) {
+  DBuf list(c, (g.n ? g.n : 1) * sizeof(uint32_t));
+  const uint64_t na = compact(c, g.n, DegPositive{g.deg.as<uint32_t>()}, list.as<uint32_t>());
+  build_from_list(c, g, list.as<uint32_t>(), na, g.deg.as<uint32_t>(), nullptr, s);
+}
+
+}  // namespace kt

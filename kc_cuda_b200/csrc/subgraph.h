@@ -1,0 +1,42 @@
+// The working graph of the truss stages: an induced subgraph relabelled by
+// ascending (degree, id), with sorted rows and an id per undirected edge.
+#pragma once
+#include "kcore.h"
+#include "stages.h"
+
+namespace kt {
+
+struct Sub {
+  uint32_t n = 0;   // vertices (new ids 0..n-1, ascending degree)
+  uint64_t m = 0;   // undirected edges (ids 0..m-1, sorted by (u, v), u < v)
+  DBuf orig;        // uint32[n]   original id of each new id
+  DBuf off;         // uint64[n+1] row offsets
+  DBuf adj;         // uint32[2m]  neighbours, ascending per row
+  DBuf eid;         // uint32[2m]  edge id of each entry
+  DBuf up;          // uint64[n]   first entry of each row with neighbour > row
+  DBuf ends;        // uint64[m]   u << 32 | v of each edge (new ids, u < v)
+  uint32_t max_deg = 0;
+};
+
+// Builds the subgraph induced by the k-core state's alive vertices.
+void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s);
+// Builds the whole graph as a subgraph (every vertex of degree > 0).
+void build_sub_all(Ctx* c, const Graph& g, Sub& s);
+
+// support.cu: sup[e] = triangles through edge e (all edges of s).
+void edge_support(Ctx* c, const Sub& s, uint32_t* sup);
+
+// peel.cu
+struct PeelResult {
+  uint32_t kmax = 0;
+  uint64_t count = 0;
+  uint32_t levels = 0;
+  uint64_t rounds = 0;
+  bool stopped_early = false;
+};
+// Peels from truss level t0 upwards until no edge is left.  stop_count: if
+// nonzero and the t0-truss has exactly that many edges, stop there.
+// truss (optional, device uint32[m]) receives each edge's trussness.
+PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss);
+
+}  // namespace kt

@@ -1,0 +1,137 @@
+// Stage (d): support (triangles through each edge) of the working graph.
+//
+// Vertex-centric, no atomics on the counts: a block owns a vertex v at a
+// time, marks N(v) in a shared-memory bitmap over the subgraph's vertex ids,
+// and for every lower neighbour u (new id < v, so deg(u) <= deg(v)) a warp
+// scans N(u) against the bitmap; the popcount is |N(u) n N(v)|, written to
+// the edge (u, v).  Each edge is counted once, from its higher-degree end,
+// scanning the shorter list.  Blocks are persistent and take vertices from
+// the highest degree down through an atomic cursor.
+//
+// The reference counts triangles on the degree-oriented graph with a
+// warp-per-vertex merge and scatters 2 per triangle to all three edges with
+// atomics (tricount_direct, src/kc.cu:505-651); its support is twice this.
+//
+// Graphs whose vertex count exceeds the bitmap limit use k_support_search:
+// warp per edge, lanes binary-search the shorter row in the longer one.
+#include "subgraph.h"
+
+namespace kt {
+namespace {
+
+constexpr unsigned kSupThreads = 256;
+
+__global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, const uint64_t* __restrict__ off,
+                                                                const uint32_t* __restrict__ adj,
+                                                                const uint32_t* __restrict__ eid,
+                                                                const uint64_t* __restrict__ up,
+                                                                uint32_t* __restrict__ sup,
+                                                                unsigned long long* cursor) {
+  extern __shared__ uint32_t bits[];
+  __shared__ uint32_t s_v;
+  const uint32_t words = (n + 31) / 32;
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0;
+  __syncthreads();
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned long long t = atomicAdd(cursor, 1ULL);
+      s_v = t < n ? (uint32_t)(n - 1 - t) : 0xffffffffu;
+    }
+    __syncthreads();
+    const uint32_t v = s_v;
+    if (v == 0xffffffffu) break;
+    const uint64_t vb = off[v], ve = off[v + 1], vu = up[v];
+    for (uint64_t j = vb + threadIdx.x; j < ve; j += blockDim.x) {
+      const uint32_t w = adj[j];
+      atomicOr(&bits[w >> 5], 1u << (w & 31));
+    }
+    __syncthreads();
+    // Lower neighbours u of v: entries [vb, vu).
+    for (uint64_t j = vb + warp_id(); j < vu; j += blockDim.x >> 5) {
+      const uint32_t u = adj[j];
+      const uint64_t ub = off[u], ue = off[u + 1];
+      uint32_t cnt = 0;
+      for (uint64_t q = ub + lane_id(); q < ue; q += 32) {
+        const uint32_t w = adj[q];
+        cnt += (bits[w >> 5] >> (w & 31)) & 1u;
+      }
+      cnt = warp_sum(cnt);
+      if (lane_id() == 0) sup[eid[j]] = cnt;
+    }
+    __syncthreads();
+    for (uint64_t j = vb + threadIdx.x; j < ve; j += blockDim.x) {
+      const uint32_t w = adj[j];
+      bits[w >> 5] = 0;
+    }
+    __syncthreads();
+  }
+}
+
+// Position of x in sorted a[lo, hi), or hi.
+__device__ __forceinline__ uint64_t find_sorted(const uint32_t* a, uint64_t lo, uint64_t hi, uint32_t x) {
+  const uint64_t end = hi;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < end && a[lo] == x) ? lo : end;
+}
+
+__global__ void k_support_search(uint64_t m, const uint64_t* __restrict__ ends, const uint64_t* __restrict__ off,
+                                 const uint32_t* __restrict__ adj, uint32_t* __restrict__ sup) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t e = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); e < m; e += warps) {
+    const uint64_t k = ends[e];
+    uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
+    if (off[a + 1] - off[a] > off[b + 1] - off[b]) {
+      const uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    const uint64_t ab = off[a], ae = off[a + 1], bb = off[b], be = off[b + 1];
+    uint32_t cnt = 0;
+    for (uint64_t q = ab + lane_id(); q < ae; q += 32) cnt += find_sorted(adj, bb, be, adj[q]) != be;
+    cnt = warp_sum(cnt);
+    if (lane_id() == 0) sup[e] = cnt;
+  }
+}
+
+}  // namespace
+
+void edge_support(Ctx* c, const Sub& s, uint32_t* sup) {
+  if (s.m == 0) return;
+  cudaEvent_t e0 = c->ev[0], e1 = c->ev[1];
+  if (c->opt.record_kernel_times) KT_CUDA(cudaEventRecord(e0, c->stream));
+  if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
+    const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
+    if (smem > 48 * 1024)
+      KT_CUDA(cudaFuncSetAttribute(k_support_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_support_bitmap, kSupThreads, smem));
+    if (per_sm < 1) throw Error(KT_ERR_LIMIT, "support: bitmap does not fit in shared memory");
+    DBuf cur(c, 8);
+    zero(c, cur.get(), 8);
+    const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * c->num_sms, s.n);
+    k_support_bitmap<<<grid, kSupThreads, smem, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
+                                                             s.eid.as<uint32_t>(), s.up.as<uint64_t>(), sup,
+                                                             cur.as<unsigned long long>());
+    KT_LAUNCHED(c);
+  } else {
+    k_support_search<<<grid_for(s.m * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.m, s.ends.as<uint64_t>(), s.off.as<uint64_t>(), s.adj.as<uint32_t>(), sup);
+    KT_LAUNCHED(c);
+  }
+  c->stats.support_launches++;
+  if (c->opt.record_kernel_times) {
+    KT_CUDA(cudaEventRecord(e1, c->stream));
+    KT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    KT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    c->stats.ms_support_kernel += ms;
+  }
+}
+
+}  // namespace kt

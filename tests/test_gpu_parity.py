@@ -1,0 +1,173 @@
+"""GPU parity: the CUDA solver through the C ABI against the reference's
+answers (golden fixtures from kc_cpu) and against the CPU oracle's stage
+outputs, bit for bit."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import kt_oracle as O
+from conftest import ROOT, golden_bytes
+from kc_cuda_b200 import gen
+import kc_cuda_b200 as K
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = K.Context(0)
+    yield c
+    c.close()
+
+
+def spec_graphs(golden):
+    for name, e in golden.items():
+        if "spec" in e and "file" not in e:
+            yield name, e, gen.Graph(gen.GraphSpec(**e["spec"]))
+
+
+def test_golden_fixtures_tsv(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e:
+            continue
+        data = golden_bytes(e)
+        if "error" in e:
+            continue
+        assert ctx.solve_tsv(data) == (e["kmax"], e["edges"]), name
+
+
+def test_golden_fixtures_file_path(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e:
+            continue
+        path = os.path.join(ROOT, "tests", "golden", e["file"])
+        if "error" in e:
+            with pytest.raises(K.KtError) as ei:
+                ctx.load_tsv_file(path)
+            assert ei.value.status == 5 and "mmap file error" in ei.value.message
+            continue
+        g = ctx.load_tsv_file(path)
+        assert g.kmax_truss() == (e["kmax"], e["edges"]), name
+
+
+def test_golden_generated_specs(ctx, golden):
+    for name, e, g in spec_graphs(golden):
+        assert ctx.solve_tsv(g.tsv_bytes()) == (e["kmax"], e["edges"]), name
+
+
+def test_messy_input_same_answer(ctx, golden):
+    for name, e in golden.items():
+        if "spec" not in e or "file" not in e:
+            continue
+        g = gen.Graph(gen.GraphSpec(**e["spec"]))
+        assert ctx.solve_tsv(g.tsv_bytes(messy=True, mess_seed=11)) == (e["kmax"], e["edges"]), name
+
+
+def test_csr_matches_oracle_clean(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e or "error" in e:
+            continue
+        data = golden_bytes(e)
+        want = O.clean(O.parse(data))
+        g = ctx.load_tsv(data)
+        assert np.array_equal(g.edges(), want), name
+
+
+def test_csr_large_random_pairs(ctx):
+    rng = np.random.default_rng(5)
+    n = 1 << 18
+    x = rng.integers(0, n, 3_000_000, dtype=np.uint64)
+    y = (x + rng.integers(0, 64, x.size, dtype=np.uint64)) % np.uint64(n)  # repeats and self-loops
+    xy = (x << np.uint64(32)) | y
+    g = ctx.load_pairs(xy)
+    assert np.array_equal(g.edges(), O.clean(xy))
+
+
+def test_support_matches_oracle(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e or "error" in e:
+            continue
+        g = ctx.load_tsv(golden_bytes(e))
+        edges = g.edges()
+        assert np.array_equal(g.tricount(), O.support(edges)), name
+
+
+def test_trussness_matches_oracle(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e or "error" in e:
+            continue
+        g = ctx.load_tsv(golden_bytes(e))
+        edges = g.edges()
+        t = g.trussness()
+        assert np.array_equal(t, O.trussness(edges)), name
+        if len(edges):
+            assert O.kmax_from_truss(t) == (e["kmax"], e["edges"]), name
+
+
+def test_core_numbers_and_kcore(ctx, golden):
+    for name, e in golden.items():
+        if "file" not in e or "error" in e:
+            continue
+        g = ctx.load_tsv(golden_bytes(e))
+        n = g.num_vertices
+        core = O.core_numbers(g.edges(), n)
+        assert np.array_equal(g.core_numbers(), core), name
+        cmax = int(core.max()) if n else 0
+        for k in sorted({1, 2, max(1, cmax // 2), cmax, cmax + 1}):
+            mem, cm = g.kmax_core(k)
+            assert cm == cmax, name
+            assert np.array_equal(mem, core >= k), (name, k)
+
+
+def test_config1_rmat_s16(ctx, golden):
+    e = golden["rmat_s16_ef16_k30"]
+    g = gen.Graph(gen.GraphSpec(**e["spec"]))
+    assert ctx.solve_tsv(g.tsv_bytes()) == (e["kmax"], e["edges"]) == (114, 8958)
+    st = ctx.stats()
+    assert st["cmax"] > 0 and st["core_edges"] > 0
+
+
+def test_without_prediction_same_answer(ctx, golden):
+    ctx.set_option("predict", 0)
+    try:
+        for name, e, g in spec_graphs(golden):
+            assert ctx.solve_tsv(g.tsv_bytes()) == (e["kmax"], e["edges"]), name
+    finally:
+        ctx.set_option("predict", 1)
+
+
+def test_search_fallback_support_kernel(ctx, golden):
+    """The binary-search support kernel (used above the bitmap size limit)."""
+    ctx.set_option("support_bitmap_max_n", 0)
+    try:
+        for name, e in golden.items():
+            if "file" not in e or "error" in e:
+                continue
+            g = ctx.load_tsv(golden_bytes(e))
+            assert np.array_equal(g.tricount(), O.support(g.edges())), name
+            assert g.kmax_truss() == (e["kmax"], e["edges"]), name
+    finally:
+        ctx.set_option("support_bitmap_max_n", 1 << 20)
+
+
+def test_parse_error_reports_line(ctx):
+    with pytest.raises(K.KtError) as ei:
+        ctx.solve_tsv(b"1\t2\n2\t3\n5\n3\t1\n")
+    assert ei.value.status == 4 and "line 3" in ei.value.message
+    # The context stays usable.
+    assert ctx.solve_tsv(b"0\t1\n1\t2\n2\t0\n") == (3, 3)
+
+
+def test_cli_matches_reference_output(golden):
+    exe = os.path.join(ROOT, "kc_cuda_b200", "kt_solve")
+    for name in ("triangle", "k10", "rmat_s10_ef16_k20_k12", "empty", "square"):
+        e = golden[name]
+        p = subprocess.run([exe, "-f", os.path.join(ROOT, "tests", "golden", e["file"])],
+                           capture_output=True, text=True)
+        if "error" in e:
+            assert p.returncode == 255 and "mmap file error" in p.stderr
+        else:
+            assert p.returncode == 0, p.stderr
+            assert p.stdout == f"kmax = {e['kmax']}, Edges in kmax-truss = {e['edges']}.\n"
