@@ -1,0 +1,328 @@
+"""Benchmark: kmax-truss solve of one large graph per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rmat24|rmat21|rmat16]
+
+Workload (default rmat24): undirected R-MAT, scale 24 (16.7M vertex ids), edge
+factor 32 (536.9M draws), a/b/c/d = .57/.19/.19/.05, seed 2, cliques of 80,
+120 and 200 planted on seeded random vertices, written as the reference's TSV
+edge list (both directions, grouped by the second column).  Synthetic: the
+seeded generator in kc_cuda_b200/csrc/ktgen.cpp.
+
+One step = one solve of the whole graph:
+  value : edges / device time of kt_solve_staged (TSV bytes already in HBM:
+          parse, clean, CSR, k-core, support, peel), CUDA events on the
+          library's stream.
+  e2e   : edges / wall time of kt_solve_tsv from pinned host bytes (the
+          host-to-device copy of the TSV and the device-to-host reads of the
+          answer inside).
+The TSV (16 GB) is larger than L2, so no flush is needed between steps.
+
+Under torchrun each rank solves its own replica on its own GPU (graphs are
+independent units: no data-path collective); the step time is the max over
+ranks and value counts the edges of all ranks.
+
+--impl reference runs the reference's own CPU solver (kc_cpu, built from the
+reference sources into oracle/_ref/) on a bounded sample of the same
+workload family on all host cores; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (scale, edge factor, seed, cliques)
+    "rmat24": (24, 32, 2, [80, 120, 200]),
+    "rmat21": (21, 32, 2, [80, 120, 200]),
+    "rmat16": (16, 16, 1, [30]),
+}
+# CPU sample of the same family for the reference solver (about 10-30 s).
+CPU_SAMPLE = (20, 32, 2, [80, 120, 200])
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def make_tsv(spec_t, pinned: bool):
+    """Generates the workload graph and its TSV bytes (pinned host memory
+    when torch can provide it)."""
+    from kc_cuda_b200 import gen
+    scale, ef, seed, cliques = spec_t
+    g = gen.Graph(gen.rmat(scale, ef, seed, cliques))
+    size = g.tsv_size()
+    buf = None
+    if pinned:
+        try:
+            import torch
+            buf = torch.empty(size, dtype=torch.uint8, pin_memory=True).numpy()
+        except Exception:
+            buf = None
+    if buf is None:
+        import numpy as np
+        buf = np.empty(size, dtype=np.uint8)
+    g.tsv_into(buf)
+    return g, buf
+
+
+def cpu_baseline_run(steps: int, warmup: int, threads: int):
+    """kc_cpu (reference sources, oracle/_ref) on the CPU sample.  Returns
+    (edges/s, sample description, per-step seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import kt_oracle as O
+    if not O.have_kc_cpu():
+        return None, "oracle/_ref/kc_cpu missing", []
+    from kc_cuda_b200 import gen
+    scale, ef, seed, cliques = CPU_SAMPLE
+    g = gen.Graph(gen.rmat(scale, ef, seed, cliques))
+    m = g.num_edges
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "sample.tsv")
+        g.write_tsv(path)
+        with open(path, "rb") as f:  # page cache warm, as vmtouch would make it
+            while f.read(1 << 26):
+                pass
+        times = []
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            O.run_kc_cpu(path, threads=threads, timeout=900)
+            dt = time.perf_counter() - t0
+            if i >= warmup:
+                times.append(dt)
+    med = statistics.median(times)
+    desc = (f"kc_cpu -f on R-MAT s{scale} ef{ef} seed {seed} + K{'/K'.join(map(str, cliques))} "
+            f"({m} edges), whole-process wall time, median of {len(times)}, OMP_NUM_THREADS={threads}")
+    return m / med, desc, times
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    threads = os.cpu_count() or 1
+    metric = "kmax-truss solve edges/s per graph"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, desc, times = cpu_baseline_run(args.steps, args.warmup, threads)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": desc}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": v, "unit": "edges/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.median(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "rmat20_ef32_k80_120_200 (CPU sample of the rmat24 family)", "threads": threads},
+            "cpu_baseline": {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc},
+            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    import kc_cuda_b200 as K
+    spec_t = WORKLOADS[args.workload]
+    g, tsv = make_tsv(spec_t, pinned=True)
+    n_edges, n_vertices = g.num_edges, g.num_vertices
+    ctx = K.Context(local)
+    staged = ctx.stage_tsv(tsv)
+
+    # Warm-up (device-resident and end-to-end paths).
+    answer = None
+    for _ in range(args.warmup):
+        answer = staged.solve()
+    ctx.solve_tsv(tsv)
+
+    # Timed: device-resident solves.
+    barrier(pg)
+    ctx.reset_stats()
+    dev_ms = []
+    stats_last = None
+    sup_ms = peel_ms = 0.0
+    sup_bytes = peel_bytes = 0
+    sup_launch = peel_launch = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            got = staged.solve()
+            st = ctx.stats()
+            assert got == answer, (got, answer)
+            dev_ms.append(st["ms_total"])
+            sup_ms += st["ms_support_kernel"]
+            peel_ms += st["ms_peel_kernel"]
+            sup_bytes += st["support_bytes"]
+            peel_bytes += st["peel_bytes"]
+            stats_last = st
+    launches = ctx.stats()["kernel_launches"]
+    sup_launch = stats_last["support_launches"]
+    peel_launch = stats_last["peel_launches"]
+    barrier(pg)
+    step_ms = max_over_ranks(pg, sum(dev_ms) / len(dev_ms))
+    total_edges = sum_over_ranks(pg, float(n_edges))
+    value = total_edges / (step_ms / 1000.0)
+
+    # Timed: end to end through the public API from pinned host memory.
+    barrier(pg)
+    ctx.reset_stats()
+    e2e_s = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        got = ctx.solve_tsv(tsv)
+        e2e_s.append(time.perf_counter() - t0)
+        assert got == answer
+    est = ctx.stats()
+    barrier(pg)
+    e2e_step = max_over_ranks(pg, sum(e2e_s) / len(e2e_s))
+    e2e_value = total_edges / e2e_step
+
+    hbm, peak_kind = load_peaks()
+    # Dominant of the two truss kernels by device time.
+    if peel_ms >= sup_ms:
+        kname, kbytes, kms, klaunch = "k_cascade (truss peel)", peel_bytes, peel_ms, peel_launch * args.steps
+    else:
+        kname, kbytes, kms, klaunch = "k_support_bitmap (support)", sup_bytes, sup_ms, sup_launch * args.steps
+    achieved = (kbytes / (kms / 1000.0)) / 1e9 if kms > 0 else 0.0
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, desc, _ = cpu_baseline_run(1, 0, threads)
+        if v is not None:
+            cpu = {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc}
+    if rank == 0:
+        line = {
+            "metric": metric, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"rmat{spec_t[0]}_ef{spec_t[1]}_seed{spec_t[2]}_k" + "_".join(map(str, spec_t[3])),
+                       "vertices": n_vertices, "edges": n_edges, "tsv_bytes": int(tsv.nbytes),
+                       "kmax": answer[0], "kmax_truss_edges": answer[1], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (TSV bytes re-read every step)",
+                       "cmax": stats_last["cmax"], "core_edges": stats_last["core_edges"],
+                       "predict_edges": stats_last["predict_edges"]},
+            "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": est["h2d_bytes"] // args.steps,
+                    "d2h_bytes_per_step": est["d2h_bytes"] // args.steps, "ms_per_step": 1000 * e2e_step},
+            "gpu_launches": launches,
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_step": kbytes / args.steps, "kernel_ms_per_step": kms / args.steps,
+                         "launches_per_step": klaunch / args.steps},
+            "stage_ms": {k: round(stats_last[k], 3) for k in
+                         ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel")},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    staged.free()
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

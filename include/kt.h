@@ -85,6 +85,16 @@ kt_status kt_solve(kt_ctx* ctx, kt_graph* g, uint32_t* kmax, uint64_t* edges);
 /* kt_load_tsv + kt_solve + kt_graph_free in one call (the `-f` path). */
 kt_status kt_solve_tsv(kt_ctx* ctx, const char* bytes, uint64_t len, uint32_t* kmax, uint64_t* edges);
 
+/* TSV bytes held in device memory (for callers that keep inputs resident
+ * in HBM, and for timing the solve without the host-to-device copy). */
+typedef struct kt_tsv kt_tsv;
+/* Copies host TSV bytes into device memory owned by the context. */
+kt_status kt_tsv_stage(kt_ctx* ctx, const char* bytes, uint64_t len, kt_tsv** out);
+/* Parse + clean + solve from staged bytes (the device-resident form of
+ * kt_solve_tsv). */
+kt_status kt_solve_staged(kt_ctx* ctx, const kt_tsv* tsv, uint32_t* kmax, uint64_t* edges);
+void kt_tsv_free(kt_ctx* ctx, kt_tsv* tsv);
+
 /* ------------------------------------------------------- stage outputs */
 
 /* Members of the k-core (member_out[v] = 1 if v is in it) and, in cmax_out,
@@ -102,7 +112,10 @@ kt_status kt_edge_trussness(kt_ctx* ctx, kt_graph* g, uint32_t* truss_out);
 /* ----------------------------------------------------------- statistics */
 
 typedef struct kt_stats {
-  double ms_parse, ms_csr, ms_kcore, ms_subgraph, ms_support, ms_peel, ms_total; /* device time, last solve */
+  /* Device time (CUDA events on the context's stream) of the last solve:
+   * ms_total spans the whole call (kt_solve_tsv: from the first host-to-device
+   * copy to the answer; kt_solve_staged: from the parse). */
+  double ms_parse, ms_csr, ms_kcore, ms_subgraph, ms_support, ms_peel, ms_total;
   uint64_t kernel_launches;       /* kernels this context launched since kt_stats_reset */
   uint64_t core_vertices, core_edges;       /* search-phase subgraph */
   uint64_t predict_vertices, predict_edges; /* prediction-phase subgraph */
@@ -111,6 +124,8 @@ typedef struct kt_stats {
   double ms_support_kernel, ms_peel_kernel; /* summed kernel time (events) */
   uint64_t support_launches, peel_launches;
   uint64_t device_bytes_peak;
+  uint64_t h2d_bytes, d2h_bytes;            /* host<->device traffic since kt_stats_reset */
+  uint64_t peel_decrements;                 /* support decrements of the last solve */
 } kt_stats;
 kt_status kt_get_stats(const kt_ctx* ctx, kt_stats* out);
 kt_status kt_stats_reset(kt_ctx* ctx);

@@ -21,6 +21,10 @@ struct kt_ctx {
 struct kt_graph {
   kt::Graph g;
 };
+struct kt_tsv {
+  kt::DBuf bytes;
+  uint64_t len = 0;
+};
 
 namespace kt {
 
@@ -74,9 +78,17 @@ __global__ void k_canon_pairs(uint64_t* __restrict__ xy, uint64_t n, unsigned in
 
 }  // namespace
 
+static float event_ms(cudaEvent_t a, cudaEvent_t b) {
+  KT_CUDA(cudaEventSynchronize(b));
+  float ms = 0;
+  KT_CUDA(cudaEventElapsedTime(&ms, a, b));
+  return ms;
+}
+
 // Device bytes (padded) -> Graph.
-static void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g) {
+void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g) {
   reset_words(c);
+  KT_CUDA(cudaEventRecord(c->ev[4], c->stream));
   DBuf block_off;
   const uint64_t lines = parse_count_lines(c, dbuf, len, block_off);
   DBuf keys(c, (lines ? lines : 1) * sizeof(uint64_t));
@@ -87,7 +99,11 @@ static void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, G
   const uint64_t n = (w.counters[1] & 1) ? (uint64_t)(uint32_t)w.counters[0] + 1 : 0;
   reset_words(c);
   block_off.release();
+  KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
   build_graph(c, keys.as<uint64_t>(), lines, n, g);
+  KT_CUDA(cudaEventRecord(c->ev[6], c->stream));
+  c->stats.ms_parse = event_ms(c->ev[4], c->ev[5]);
+  c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
 }
 
 void load_tsv(Ctx* c, const char* bytes, uint64_t len, Graph& g) {
@@ -386,18 +402,83 @@ void kt_graph_free(kt_ctx* h, kt_graph* g) {
 kt_status kt_solve(kt_ctx* h, kt_graph* g, uint32_t* kmax, uint64_t* edges) {
   if (!g || !kmax || !edges) return KT_ERR_INVALID;
   KT_API_BEGIN(h)
-  kt::reset_words(&h->c);
-  kt::solve_graph(&h->c, g->g, kmax, edges);
+  kt::Ctx* c = &h->c;
+  kt::reset_words(c);
+  kt::begin_solve_stats(c);
+  KT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  kt::solve_graph(c, g->g, kmax, edges);
+  KT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  c->stats.ms_total = kt::event_ms(c->ev[0], c->ev[1]);
   KT_API_END(h)
 }
 
 kt_status kt_solve_tsv(kt_ctx* h, const char* bytes, uint64_t len, uint32_t* kmax, uint64_t* edges) {
   if (!kmax || !edges || (!bytes && len)) return KT_ERR_INVALID;
   KT_API_BEGIN(h)
-  kt::Graph g;
-  kt::load_tsv(&h->c, bytes, len, g);
-  kt::solve_graph(&h->c, g, kmax, edges);
+  kt::Ctx* c = &h->c;
+  kt::begin_solve_stats(c);
+  KT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  {
+    kt::Graph g;
+    kt::load_tsv(c, bytes, len, g);
+    const double p = c->stats.ms_parse, q = c->stats.ms_csr;
+    kt::solve_graph(c, g, kmax, edges);
+    c->stats.ms_parse = p;
+    c->stats.ms_csr = q;
+  }
+  KT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  c->stats.ms_total = kt::event_ms(c->ev[0], c->ev[1]);
   KT_API_END(h)
+}
+
+kt_status kt_tsv_stage(kt_ctx* h, const char* bytes, uint64_t len, kt_tsv** out) {
+  if (!out || (!bytes && len)) return KT_ERR_INVALID;
+  *out = nullptr;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt_tsv* t = new kt_tsv;
+  try {
+    t->len = len;
+    t->bytes.alloc(c, kt::parse_padded_bytes(len));
+    kt::zero(c, t->bytes.get(), t->bytes.bytes());
+    kt::copy_h2d(c, t->bytes.get(), bytes, len);
+    kt::sync(c);
+  } catch (...) {
+    delete t;
+    throw;
+  }
+  *out = t;
+  KT_API_END(h)
+}
+
+kt_status kt_solve_staged(kt_ctx* h, const kt_tsv* t, uint32_t* kmax, uint64_t* edges) {
+  if (!t || !kmax || !edges) return KT_ERR_INVALID;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::begin_solve_stats(c);
+  KT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  {
+    kt::Graph g;
+    kt::graph_from_device_bytes(c, t->bytes.as<uint8_t>(), t->len, g);
+    const double p = c->stats.ms_parse, q = c->stats.ms_csr;
+    kt::solve_graph(c, g, kmax, edges);
+    c->stats.ms_parse = p;
+    c->stats.ms_csr = q;
+  }
+  KT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  c->stats.ms_total = kt::event_ms(c->ev[0], c->ev[1]);
+  KT_API_END(h)
+}
+
+void kt_tsv_free(kt_ctx* h, kt_tsv* t) {
+  if (!t) return;
+  if (h) {
+    std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+    cudaSetDevice(h->c.device);
+    delete t;
+  } else {
+    delete t;
+  }
 }
 
 kt_status kt_kcore(kt_ctx* h, kt_graph* g, uint32_t k, uint8_t* member, uint32_t* cmax) {
@@ -463,6 +544,8 @@ kt_status kt_get_stats(const kt_ctx* h, kt_stats* out) {
   *out = h->c.stats;
   out->kernel_launches = h->c.launches;
   out->device_bytes_peak = h->c.peak;
+  out->h2d_bytes = h->c.h2d_bytes;
+  out->d2h_bytes = h->c.d2h_bytes;
   return KT_OK;
 }
 
@@ -471,6 +554,7 @@ kt_status kt_stats_reset(kt_ctx* h) {
   std::lock_guard<std::recursive_mutex> lk(h->c.mu);
   h->c.stats = kt_stats{};
   h->c.launches = 0;
+  h->c.h2d_bytes = h->c.d2h_bytes = 0;
   h->c.peak = h->c.in_use;
   return KT_OK;
 }

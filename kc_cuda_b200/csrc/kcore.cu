@@ -230,10 +230,54 @@ __global__ void k_core_from_tags(const uint32_t* __restrict__ rem, uint64_t n, c
   }
 }
 
+
+// Compacted copy of the alive part: row i of the new graph is alive[i] with
+// only its alive neighbours, renumbered.
+__global__ void k_compact_rows(const uint32_t* __restrict__ alive, uint64_t na, const uint64_t* __restrict__ off,
+                               const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
+                               const uint32_t* __restrict__ newid, const uint64_t* __restrict__ noff,
+                               uint32_t* __restrict__ nadj) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); i < na; i += warps) {
+    const uint32_t v = alive[i];
+    const uint64_t b = off[v], e = off[v + 1];
+    uint64_t pos = noff[i];
+    const uint64_t end = noff[i + 1];
+    for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
+      bool keep = false;
+      uint32_t w = 0;
+      if (j < e) {
+        w = adj[j];
+        keep = rem[w] == kAlive;
+      }
+      const unsigned bal = __ballot_sync(kFull, keep);
+      const uint64_t p = pos + __popc(bal & lanemask_lt());
+      if (keep && p < end) nadj[p] = newid[w];
+      pos += __popc(bal);
+    }
+  }
+}
+
+__global__ void k_compact_meta(const uint32_t* __restrict__ alive, uint64_t na, const uint32_t* __restrict__ deg,
+                               const uint32_t* __restrict__ oldmap, uint32_t* __restrict__ newid,
+                               uint32_t* __restrict__ ndeg, uint32_t* __restrict__ nmap) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = alive[i];
+    newid[v] = (uint32_t)i;
+    ndeg[i] = deg[v];
+    nmap[i] = oldmap ? oldmap[v] : v;
+  }
+}
+
+__global__ void k_members_mapped(const uint32_t* __restrict__ rem, uint64_t n, const uint32_t* __restrict__ map,
+                                 uint8_t* __restrict__ out) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    if (rem[v] == kAlive) out[map[v]] = 1;
+}
+
 }  // namespace
 
-void KCore::init(Ctx* c, const Graph& gr) {
-  g = &gr;
+void KCore::reset_state(Ctx* c, const Graph& gr) {
   n = gr.n;
   deg.ensure(c, (n ? n : 1) * sizeof(uint32_t));
   rem.ensure(c, (n ? n : 1) * sizeof(uint32_t));
@@ -247,24 +291,73 @@ void KCore::init(Ctx* c, const Graph& gr) {
                                                                              deg.as<uint32_t>(), rem.as<uint32_t>());
     KT_LAUNCHED(c);
   }
-  levels.assign(1, 1);  // tag 0 = isolated, left at level 1
   rebuild_alive(c);
+}
+
+void KCore::init(Ctx* c, const Graph& gr) {
+  base = &gr;
+  compacted = false;
+  local_level = 0;
+  levels.assign(1, 1);  // tag 0 = isolated, left at level 1
+  succ.assign(1, 0);
+  reset_state(c, gr);
 }
 
 void KCore::rebuild_alive(Ctx* c) {
   n_alive = compact(c, n, AliveF{rem.as<uint32_t>()}, alive.as<uint32_t>());
 }
 
+void KCore::compact_to_alive(Ctx* c, uint32_t level) {
+  const Graph& g = cur();
+  const uint64_t na = n_alive;
+  Graph L;
+  L.n = na;
+  DBuf newid(c, (n ? n : 1) * sizeof(uint32_t));
+  DBuf nmap(c, (na ? na : 1) * sizeof(uint32_t));
+  L.deg.alloc(c, (na + 1) * sizeof(uint32_t));
+  zero(c, L.deg.get(), (na + 1) * sizeof(uint32_t));
+  k_compact_meta<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      alive.as<uint32_t>(), na, deg.as<uint32_t>(), map(), newid.as<uint32_t>(), L.deg.as<uint32_t>(),
+      nmap.as<uint32_t>());
+  KT_LAUNCHED(c);
+  L.off.alloc(c, (na + 1) * sizeof(uint64_t));
+  scan_u32_to_u64(c, L.deg.as<uint32_t>(), L.off.as<uint64_t>(), na + 1);
+  const uint64_t n2 = read_word<uint64_t>(c, L.off.as<uint64_t>() + na);
+  L.m = n2 / 2;
+  L.adj.alloc(c, (n2 ? n2 : 1) * sizeof(uint32_t));
+  k_compact_rows<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      alive.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
+      newid.as<uint32_t>(), L.off.as<uint64_t>(), L.adj.as<uint32_t>());
+  KT_LAUNCHED(c);
+  L.max_deg = g.max_deg;  // an upper bound is enough here
+  newid.release();
+  // Install (the old local graph, if any, is released by the swap).
+  local.off = std::move(L.off);
+  local.adj = std::move(L.adj);
+  local.deg = std::move(L.deg);
+  local.edges.release();
+  local.n = L.n;
+  local.m = L.m;
+  local.max_deg = L.max_deg;
+  idmap = std::move(nmap);
+  compacted = true;
+  local_level = level;
+  levels.assign(1, level);
+  succ.assign(1, 0);
+  reset_state(c, local);
+}
+
 void KCore::recount(Ctx* c) {
   if (!n_alive) return;
+  const Graph& g = cur();
   zero(c, cnt.get(), cnt.bytes());
   unsigned long long* nbig = cnt.as<unsigned long long>() + 4;
   k_recount<<<grid_for(n_alive * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      alive.as<uint32_t>(), n_alive, g->off.as<uint64_t>(), g->adj.as<uint32_t>(), rem.as<uint32_t>(),
+      alive.as<uint32_t>(), n_alive, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
       deg.as<uint32_t>(), big.as<uint32_t>(), nbig, n, &dev_words(c)->err);
   KT_LAUNCHED(c);
-  k_recount_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), nbig, g->off.as<uint64_t>(),
-                                                       g->adj.as<uint32_t>(), rem.as<uint32_t>(),
+  k_recount_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), nbig, g.off.as<uint64_t>(),
+                                                       g.adj.as<uint32_t>(), rem.as<uint32_t>(),
                                                        deg.as<uint32_t>());
   KT_LAUNCHED(c);
 }
@@ -274,6 +367,7 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
   if (tag >= 0xfffffff0u) throw Error(KT_ERR_LIMIT, "k-core: too many probes");
   levels.push_back(k);
   if (!n_alive) return 0;
+  const Graph& g = cur();
   unsigned long long* cn = cnt.as<unsigned long long>();
   zero(c, cnt.get(), cnt.bytes());
   uint32_t* err = &dev_words(c)->err;
@@ -282,43 +376,39 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
       n, err);
   KT_LAUNCHED(c);
   uint64_t removed = 0;
-  int cur = 0;
-  uint64_t rounds_here = 0;
+  int cur_f = 0;
   while (true) {
-    const uint64_t nf = read_word<unsigned long long>(c, cn + cur);
+    const uint64_t nf = read_word<unsigned long long>(c, cn + cur_f);
     if (nf == 0) break;
     removed += nf;
-    ++rounds_here;
-    KT_CUDA(cudaMemsetAsync(cn + (cur ^ 1), 0, sizeof(unsigned long long), c->stream));
+    ++rounds;
+    KT_CUDA(cudaMemsetAsync(cn + (cur_f ^ 1), 0, sizeof(unsigned long long), c->stream));
     KT_CUDA(cudaMemsetAsync(cn + 4, 0, sizeof(unsigned long long), c->stream));
     k_expand<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-        front[cur].as<uint32_t>(), nf, g->off.as<uint64_t>(), g->adj.as<uint32_t>(), deg.as<uint32_t>(),
-        rem.as<uint32_t>(), k, tag, front[cur ^ 1].as<uint32_t>(), cn + (cur ^ 1), big.as<uint32_t>(), cn + 4, n,
-        err);
+        front[cur_f].as<uint32_t>(), nf, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), deg.as<uint32_t>(),
+        rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(), cn + (cur_f ^ 1), big.as<uint32_t>(), cn + 4,
+        n, err);
     KT_LAUNCHED(c);
-    k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g->off.as<uint64_t>(),
-                                                        g->adj.as<uint32_t>(), deg.as<uint32_t>(),
-                                                        rem.as<uint32_t>(), k, tag, front[cur ^ 1].as<uint32_t>(),
-                                                        cn + (cur ^ 1), n, err);
+    k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g.off.as<uint64_t>(),
+                                                        g.adj.as<uint32_t>(), deg.as<uint32_t>(),
+                                                        rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(),
+                                                        cn + (cur_f ^ 1), n, err);
     KT_LAUNCHED(c);
-    cur ^= 1;
+    cur_f ^= 1;
   }
-  rounds += rounds_here;
   check_words(c, "k-core probe");
-  const uint64_t left = n_alive - removed;
-  return left;
+  return n_alive - removed;
 }
 
 uint32_t KCore::find_max_core(Ctx* c) {
-  succ.assign(1, 0);  // tag 0: isolated vertices (level 1)
   if (!n_alive) {
     cmax = 0;
     return 0;
   }
   // Upper bound: a k-core holds >= k(k+1)/2 edges.
-  const double m = (double)g->m;
+  const double m = (double)base->m;
   uint64_t ub = (uint64_t)std::floor((std::sqrt(1.0 + 8.0 * m) - 1.0) / 2.0);
-  ub = std::min<uint64_t>(ub, g->max_deg);
+  ub = std::min<uint64_t>(ub, base->max_deg);
   uint64_t lo = 1, hi = ub + 1;  // the 1-core (non-isolated vertices) is non-empty
   bool ramp = true;
   while (hi - lo > 1) {
@@ -330,6 +420,8 @@ uint32_t KCore::find_max_core(Ctx* c) {
       lo = k;
       succ.push_back(tag);
       rebuild_alive(c);
+      // Work on a compacted copy once the core is a small part of the graph.
+      if (n_alive * 8 < n) compact_to_alive(c, (uint32_t)lo);
     } else {
       hi = k;
       ramp = false;
@@ -345,6 +437,15 @@ uint32_t KCore::find_max_core(Ctx* c) {
 }
 
 void KCore::restore_core(Ctx* c, uint32_t k) {
+  if (compacted && k < local_level) {
+    // Below the compacted core: start over from the input graph.
+    compacted = false;
+    local = Graph();
+    idmap.release();
+    levels.assign(1, 1);
+    succ.assign(1, 0);
+    reset_state(c, *base);
+  }
   // Last successful probe at or below level k; everything newer is revived.
   uint32_t keep = 0;
   for (uint32_t t : succ)
@@ -359,14 +460,21 @@ void KCore::restore_core(Ctx* c, uint32_t k) {
   rebuild_alive(c);
   recount(c);
   const uint32_t tag = (uint32_t)levels.size();
-  if (probe(c, k)) {
-    succ.push_back(tag);
-  }
+  if (probe(c, k)) succ.push_back(tag);
   rebuild_alive(c);
 }
 
 void KCore::members(Ctx* c, uint8_t* dout) {
-  if (!n) return;
+  if (!base->n) return;
+  if (compacted) {
+    zero(c, dout, base->n);
+    if (n) {
+      k_members_mapped<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n,
+                                                                                   idmap.as<uint32_t>(), dout);
+      KT_LAUNCHED(c);
+    }
+    return;
+  }
   k_members<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n, dout);
   KT_LAUNCHED(c);
 }
@@ -374,6 +482,7 @@ void KCore::members(Ctx* c, uint8_t* dout) {
 void KCore::core_numbers(Ctx* c, uint32_t* dcore) {
   // Peel level by level: the alive set is always a d-core where d is its
   // minimum degree, so the probe at d+1 removes exactly the core-d vertices.
+  if (compacted) throw Error(KT_ERR_INVALID, "core_numbers needs an uncompacted state");
   DBuf mn(c, 4);
   while (n_alive) {
     KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));

@@ -7,11 +7,15 @@
 namespace kt {
 
 struct KCore {
-  const Graph* g = nullptr;
-  uint64_t n = 0;
+  const Graph* base = nullptr;  // the input graph
+  Graph local;                  // compacted core (valid when compacted)
+  DBuf idmap;                   // uint32[local.n]: local id -> base id
+  bool compacted = false;
+  uint32_t local_level = 0;     // local holds the local_level-core of base
+  uint64_t n = 0;               // vertices of the current graph
   DBuf deg;        // uint32[n]: alive degree of alive vertices
   DBuf rem;        // uint32[n]: kAlive, or the tag of the probe that removed it
-  DBuf alive;      // uint32[n]: compact list of alive vertices
+  DBuf alive;      // uint32[n]: compact list of alive vertices (ascending)
   DBuf front[2];   // frontiers
   DBuf big;        // rows handled by whole blocks
   DBuf cnt;        // counters
@@ -20,6 +24,9 @@ struct KCore {
   uint64_t rounds = 0;
   std::vector<uint32_t> levels;  // levels[tag] = k of that probe
   std::vector<uint32_t> succ;    // tags of probes that were kept
+
+  const Graph& cur() const { return compacted ? local : *base; }
+  const uint32_t* map() const { return compacted ? idmap.as<uint32_t>() : nullptr; }
 
   void init(Ctx* c, const Graph& gr);
   void rebuild_alive(Ctx* c);
@@ -30,9 +37,14 @@ struct KCore {
   uint32_t find_max_core(Ctx* c);
   // Leaves the alive set at the k-core (k <= cmax after find_max_core).
   void restore_core(Ctx* c, uint32_t k);
+  // member[v] (base ids) = v is alive.
   void members(Ctx* c, uint8_t* dout);
-  // Full decomposition (consumes the state).
+  // Full decomposition (consumes the state; never compacts).
   void core_numbers(Ctx* c, uint32_t* dcore);
+
+ private:
+  void reset_state(Ctx* c, const Graph& gr);
+  void compact_to_alive(Ctx* c, uint32_t level);
 };
 
 }  // namespace kt

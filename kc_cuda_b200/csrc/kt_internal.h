@@ -51,6 +51,23 @@ struct Options {
 
 struct Ctx;
 
+// Stage timers: events recorded around kernels without synchronising; the
+// elapsed times are collected when the solve ends (resolve()).
+struct EventTimer {
+  struct Span {
+    cudaEvent_t a, b;
+    double* acc;
+  };
+  std::vector<cudaEvent_t> pool;
+  std::vector<Span> open;
+  size_t used = 0;
+  cudaEvent_t get();
+  void begin(cudaStream_t s, double* acc, cudaEvent_t* out_a);
+  void end(cudaStream_t s, cudaEvent_t a, double* acc);
+  void resolve();  // adds elapsed times into their accumulators
+  ~EventTimer();
+};
+
 // Device buffer charged to a context's budget; freed stream-ordered.
 class DBuf {
  public:
@@ -104,6 +121,7 @@ struct Ctx {
   uint64_t in_use = 0;
   uint64_t peak = 0;
   uint64_t launches = 0;
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;
   std::string last_error;
   Options opt;
   kt_stats stats{};
@@ -113,6 +131,7 @@ struct Ctx {
   cudaEvent_t ev[8] = {};
   // Device word block: bounded-wait error flag, barrier state, counters.
   DBuf words;
+  EventTimer timer;
 };
 
 // Graph held on the device: cleaned, symmetric CSR (rows unsorted) plus the
@@ -132,6 +151,7 @@ void sync(Ctx* c);
 template <typename T>
 T read_word(Ctx* c, const T* dptr) {
   static_assert(sizeof(T) <= 8, "word");
+  c->d2h_bytes += sizeof(T);
   KT_CUDA(cudaMemcpyAsync(c->pinned, dptr, sizeof(T), cudaMemcpyDeviceToHost, c->stream));
   sync(c);
   T v;

@@ -1,21 +1,31 @@
 // Stage (e): truss peeling of the working graph.
 //
 // Levels: at truss level t every alive edge with support < t-2 is removed,
-// round by round, until none is left; the alive edges then form the t-truss.
-// If edges remain, their minimum support s makes them an (s+2)-truss, which
-// is recorded as the current answer, and the next level is t = s+3 (levels
-// where nothing would be removed are skipped).  The last recorded level when
-// no edge is left is kmax.
+// round by round, until none is left (a cascade); the alive edges then form
+// the t-truss.  If edges remain, their minimum support s makes them an
+// (s+2)-truss, which is recorded, and the next level is t = s+3.  The last
+// recorded level when no edge is left is kmax.
 //
 // Rounds: the frontier edges of round r carry state r; deleted edges keep
-// their round, alive edges kAlive.  A warp takes a frontier edge (u, v) and
-// looks up each entry w of the shorter row in the longer one.  A common w
-// closes the triangle {e, a = (., w), b = (., w)}; it is skipped if a or b
+// their round, alive edges kAlive.  A warp takes a frontier edge (x, y) and
+// intersects the two sorted rows: 32-wide tiles of both rows are compared
+// with a 5-step shuffle search, and whichever tile ends lower is retired
+// (both when the ends tie), so every common neighbour is met exactly once;
+// when one row is more than 16x longer the lanes binary-search the long row
+// instead.  A common w closes the triangle {e, a, b}; it is skipped if a or b
 // was deleted in an earlier round.  Each surviving side edge loses one
 // triangle, decremented by exactly one frontier edge of the triangle (the
-// one with the smallest id among those in this round).  An edge whose
-// support steps from t-2 to t-3 (atomicSub returns t-2) joins the next
-// frontier, so each edge enters a frontier once.
+// one with the smallest id among those in this round); an edge whose support
+// steps from t-2 to t-3 joins the next frontier, so each edge enters a
+// frontier once.
+//
+// A cascade runs as one cooperative launch: rounds are separated by the
+// bounded grid barrier and the frontier sizes never leave the device.
+//
+// Jumps: without per-edge trussness output, the first level may be a guess
+// well above the lower bound (one cascade removes everything below it).  The
+// support/state arrays are snapshotted first; a guess that empties the graph
+// is undone and halved toward the last good level.
 //
 // The reference keeps doubled supports and subtracts 2 - [m1==st] - [m2==st]
 // from both side edges (src/kc.cu:61-159, 886-1056), and steps k by fixed
@@ -28,6 +38,30 @@
 
 namespace kt {
 namespace {
+
+constexpr unsigned kPeelThreads = 256;
+
+struct PeelArgs {
+  const uint64_t* ends;
+  const uint64_t* off;
+  const uint32_t* adj;
+  const uint32_t* eid;
+  uint32_t* sup;
+  uint32_t* state;
+  uint32_t* truss;  // may be null
+  const uint32_t* alive;
+  uint64_t na;
+  uint32_t* front[2];
+  unsigned long long* cnt;  // 3 rotating frontier counters + [3] rounds done + [4] decrements
+  uint64_t cap;
+  uint32_t thr;    // remove support < thr
+  uint32_t tval;   // trussness recorded for removed edges
+  uint32_t r0;     // first round number
+  uint32_t* adeg;  // alive degree per vertex (for the byte accounting)
+  unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements
+  DevWords* words;
+  unsigned long long timeout_ns;
+};
 
 __device__ __forceinline__ void push_warp_full(bool want, uint32_t item, uint32_t* list, unsigned long long* cnt,
                                                uint64_t cap, uint32_t* err) {
@@ -58,90 +92,190 @@ __device__ __forceinline__ uint64_t find_sorted(const uint32_t* a, uint64_t lo, 
   return (lo < end && a[lo] == x) ? lo : end;
 }
 
-__global__ void k_peel_init(uint64_t m, uint32_t* __restrict__ state, uint32_t* __restrict__ alive) {
+// Triangle {e, a, b} seen from frontier edge e in round r; returns which of
+// a, b crossed below the threshold (to be pushed).
+__device__ __forceinline__ void close_triangle(const PeelArgs& A, uint32_t e, uint32_t a, uint32_t b, uint32_t r,
+                                               bool& pa, bool& pb, uint32_t& ndec) {
+  const uint32_t sa = A.state[a], sb = A.state[b];
+  if (sa < r || sb < r) return;  // broken in an earlier round
+  if (sa > r && !(sb == r && b < e)) {
+    ++ndec;
+    if (atomicSub(&A.sup[a], 1u) == A.thr) {
+      A.state[a] = r + 1;
+      if (A.truss) A.truss[a] = A.tval;
+      pa = true;
+    }
+  }
+  if (sb > r && !(sa == r && a < e)) {
+    ++ndec;
+    if (atomicSub(&A.sup[b], 1u) == A.thr) {
+      A.state[b] = r + 1;
+      if (A.truss) A.truss[b] = A.tval;
+      pb = true;
+    }
+  }
+}
+
+// One frontier edge, one warp.  Pushes into next / ncnt; adds the edge's
+// alive degrees and its decrements to the per-thread tallies.
+__device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_t r, uint32_t* next,
+                                          unsigned long long* ncnt, uint64_t& tdeg, uint64_t& tdec) {
+  const uint64_t k = A.ends[e];
+  uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+  if (lane_id() == 0) tdeg += (uint64_t)atomicSub(&A.adeg[x], 1u) + atomicSub(&A.adeg[y], 1u);
+  uint32_t ndec = 0;
+  uint64_t xb = A.off[x], xe = A.off[x + 1], yb = A.off[y], ye = A.off[y + 1];
+  if (xe - xb > ye - yb) {
+    uint64_t t = xb;
+    xb = yb;
+    yb = t;
+    t = xe;
+    xe = ye;
+    ye = t;
+  }
+  const uint64_t na = xe - xb, nb = ye - yb;
+  uint32_t* err = &A.words->err;
+  const unsigned lane = lane_id();
+  if (nb > 16 * na) {
+    // Short row against a long one: binary search per lane.
+    for (uint64_t q = xb + lane; q < xb + ((na + 31) & ~31ULL); q += 32) {
+      bool pa = false, pb = false;
+      uint32_t a = 0, b = 0;
+      if (q < xe) {
+        const uint64_t p = find_sorted(A.adj, yb, ye, A.adj[q]);
+        if (p != ye) {
+          a = A.eid[q];
+          b = A.eid[p];
+          close_triangle(A, e, a, b, r, pa, pb, ndec);
+        }
+      }
+      push_warp_full(pa, a, next, ncnt, A.cap, err);
+      push_warp_full(pb, b, next, ncnt, A.cap, err);
+    }
+    tdec += ndec;
+    return;
+  }
+  // Tile merge.
+  uint64_t i = 0, j = 0;
+  while (i < na && j < nb) {
+    const uint32_t ta = (uint32_t)(na - i < 32 ? na - i : 32), tb = (uint32_t)(nb - j < 32 ? nb - j : 32);
+    const uint32_t av = lane < ta ? A.adj[xb + i + lane] : 0xffffffffu;
+    const uint32_t bv = lane < tb ? A.adj[yb + j + lane] : 0xffffffffu;
+    const uint32_t alast = __shfl_sync(kFull, av, ta - 1);
+    const uint32_t blast = __shfl_sync(kFull, bv, tb - 1);
+    // Lower bound of av in the B tile (lanes < tb hold it, ascending).
+    uint32_t q = 0;
+#pragma unroll
+    for (uint32_t s = 16; s >= 1; s >>= 1) {
+      const uint32_t probe = __shfl_sync(kFull, bv, (q + s - 1) & 31);
+      if (q + s <= tb && probe < av) q += s;
+    }
+    const uint32_t hit = __shfl_sync(kFull, bv, q & 31);
+    bool pa = false, pb = false;
+    uint32_t a = 0, b = 0;
+    if (lane < ta && q < tb && hit == av) {
+      a = A.eid[xb + i + lane];
+      b = A.eid[yb + j + q];
+      close_triangle(A, e, a, b, r, pa, pb, ndec);
+    }
+    push_warp_full(pa, a, next, ncnt, A.cap, err);
+    push_warp_full(pb, b, next, ncnt, A.cap, err);
+    if (alast <= blast) i += ta;
+    if (blast <= alast) j += tb;
+  }
+  tdec += ndec;
+}
+
+__device__ __forceinline__ void flush_tallies(const PeelArgs& A, uint64_t tdeg, uint64_t tdec) {
+  tdeg = warp_sum(tdeg);
+  tdec = warp_sum(tdec);
+  if (lane_id() == 0) {
+    if (tdeg) atomicAdd(&A.acct[0], (unsigned long long)tdeg);
+    if (tdec) atomicAdd(&A.acct[1], (unsigned long long)tdec);
+  }
+}
+
+// Frontier of a level: alive edges with support below the threshold.
+__device__ __forceinline__ void level_frontier(const PeelArgs& A, uint32_t r, uint64_t gtid, uint64_t gthreads) {
+  for (uint64_t i = gtid; i < ((A.na + 31) & ~31ULL); i += gthreads) {
+    bool want = false;
+    uint32_t e = 0;
+    if (i < A.na) {
+      e = A.alive[i];
+      if (A.state[e] == kAlive && A.sup[e] < A.thr) {
+        A.state[e] = r;
+        if (A.truss) A.truss[e] = A.tval;
+        want = true;
+      }
+    }
+    push_warp_full(want, e, A.front[0], &A.cnt[0], A.cap, &A.words->err);
+  }
+}
+
+// One whole cascade in one cooperative launch.
+__global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
+  const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  level_frontier(A, A.r0, gtid, gthreads);
+  if (!grid_barrier(A.words, A.timeout_ns)) return;
+  const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
+  uint64_t tdeg = 0, tdec = 0;
+  uint32_t i = 0;
+  while (true) {
+    const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
+    if (nf == 0) break;
+    const uint32_t r = A.r0 + i;
+    uint32_t* fr = A.front[i & 1];
+    uint32_t* nx = A.front[(i + 1) & 1];
+    unsigned long long* nc = &A.cnt[(i + 1) % 3];
+    for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
+    if (gtid == 0) A.cnt[(i + 2) % 3] = 0;  // read at the start of round i-1, next written in round i+1
+    if (!grid_barrier(A.words, A.timeout_ns)) break;
+    ++i;
+  }
+  flush_tallies(A, tdeg, tdec);
+  if (gtid == 0) A.cnt[3] = i;
+}
+
+// Host-stepped variant (one launch per round), used when cooperative launch
+// is switched off.
+__global__ void __launch_bounds__(kPeelThreads) k_level_frontier(PeelArgs A) {
+  level_frontier(A, A.r0, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
+}
+
+__global__ void __launch_bounds__(kPeelThreads) k_round(PeelArgs A, uint32_t i, uint64_t nf) {
+  const uint64_t gwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint64_t tdeg = 0, tdec = 0;
+  for (uint64_t f = gwarp; f < nf; f += gwarps)
+    peel_edge(A, A.front[i & 1][f], A.r0 + i, A.front[(i + 1) & 1], &A.cnt[(i + 1) % 3], tdeg, tdec);
+  flush_tallies(A, tdeg, tdec);
+}
+
+__global__ void k_peel_init(uint64_t m, uint32_t* __restrict__ state, uint32_t* __restrict__ alive, uint32_t n,
+                            const uint64_t* __restrict__ off, uint32_t* __restrict__ adeg) {
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
     state[e] = kAlive;
     alive[e] = (uint32_t)e;
   }
-}
-
-__global__ void k_peel_frontier(const uint32_t* __restrict__ alive, uint64_t na, const uint32_t* __restrict__ sup,
-                                uint32_t* __restrict__ state, uint32_t thr, uint32_t r, uint32_t* __restrict__ truss,
-                                uint32_t tval, uint32_t* __restrict__ front, unsigned long long* fcnt, uint64_t cap,
-                                uint32_t* err) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((na + 31) & ~31ULL);
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    bool want = false;
-    uint32_t e = 0;
-    if (i < na) {
-      e = alive[i];
-      if (state[e] == kAlive && sup[e] < thr) {
-        state[e] = r;
-        if (truss) truss[e] = tval;
-        want = true;
-      }
-    }
-    push_warp_full(want, e, front, fcnt, cap, err);
-  }
-}
-
-__global__ void k_peel_round(const uint32_t* __restrict__ front, uint64_t nf, const uint64_t* __restrict__ ends,
-                             const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
-                             const uint32_t* __restrict__ eid, uint32_t* __restrict__ sup,
-                             uint32_t* __restrict__ state, uint32_t thr, uint32_t r, uint32_t* __restrict__ truss,
-                             uint32_t tval, uint32_t* __restrict__ next, unsigned long long* ncnt, uint64_t cap,
-                             uint32_t* err) {
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t f = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); f < nf; f += warps) {
-    const uint32_t e = front[f];
-    const uint64_t k = ends[e];
-    uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
-    if (off[x + 1] - off[x] > off[y + 1] - off[y]) {
-      const uint32_t t = x;
-      x = y;
-      y = t;
-    }
-    const uint64_t ab = off[x], ae = off[x + 1], bb = off[y], be = off[y + 1];
-    for (uint64_t q = ab + lane_id(); q < ab + ((ae - ab + 31) & ~31ULL); q += 32) {
-      bool pa = false, pb = false;
-      uint32_t a = 0, b = 0;
-      if (q < ae) {
-        const uint64_t p = find_sorted(adj, bb, be, adj[q]);
-        if (p != be) {
-          a = eid[q];
-          b = eid[p];
-          const uint32_t sa = state[a], sb = state[b];
-          if (sa >= r && sb >= r) {
-            if (sa > r && !(sb == r && b < e)) {
-              if (atomicSub(&sup[a], 1u) == thr) {
-                state[a] = r + 1;
-                if (truss) truss[a] = tval;
-                pa = true;
-              }
-            }
-            if (sb > r && !(sa == r && a < e)) {
-              if (atomicSub(&sup[b], 1u) == thr) {
-                state[b] = r + 1;
-                if (truss) truss[b] = tval;
-                pb = true;
-              }
-            }
-          }
-        }
-      }
-      push_warp_full(pa, a, next, ncnt, cap, err);
-      push_warp_full(pb, b, next, ncnt, cap, err);
-    }
-  }
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    adeg[v] = (uint32_t)(off[v + 1] - off[v]);
 }
 
 __global__ void k_alive_min(const uint32_t* __restrict__ alive, uint64_t na, const uint32_t* __restrict__ sup,
                             uint32_t* out) {
-  uint32_t mn = 0xffffffffu;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x)
-    mn = min(mn, sup[alive[i]]);
+  uint32_t mn = 0xffffffffu, mx = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = sup[alive[i]];
+    mn = min(mn, s);
+    mx = max(mx, s);
+  }
   mn = warp_min(mn);
-  if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(out, mn);
+  mx = warp_max(mx);
+  if (lane_id() == 0) {
+    if (mn != 0xffffffffu) atomicMin(out, mn);
+    atomicMax(out + 1, mx);
+  }
 }
 
 struct StillAlive {
@@ -151,87 +285,199 @@ struct StillAlive {
   __device__ uint32_t value(uint64_t i) const { return list[i]; }
 };
 
-}  // namespace
-
-PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss) {
-  PeelResult res;
-  const uint64_t m = s.m;
-  if (m == 0) return res;
-  if (t0 < 3) t0 = 3;
-  DBuf state(c, m * sizeof(uint32_t));
-  DBuf alive[2] = {DBuf(c, m * sizeof(uint32_t)), DBuf(c, m * sizeof(uint32_t))};
-  DBuf front[2] = {DBuf(c, m * sizeof(uint32_t)), DBuf(c, m * sizeof(uint32_t))};
-  DBuf cnt(c, 4 * sizeof(unsigned long long));
-  DBuf mn(c, 4);
-  unsigned long long* cn = cnt.as<unsigned long long>();
-  uint32_t* err = &dev_words(c)->err;
-  k_peel_init<<<grid_for(m, 256, c->num_sms * 16), 256, 0, c->stream>>>(m, state.as<uint32_t>(),
-                                                                          alive[0].as<uint32_t>());
-  KT_LAUNCHED(c);
+// Peel state of one working graph on the device.
+struct Peeler {
+  Ctx* c;
+  const Sub* s;
+  uint32_t* sup;
+  uint32_t* truss;
+  DBuf state, alive[2], front[2], cnt, mm, adeg, acct;
+  uint64_t scanned = 0;  // alive-list entries scanned by level frontiers
   int ai = 0;
-  uint64_t na = m;
-  uint32_t t = t0;
-  uint32_t r = 0;
-  cudaEvent_t e0 = c->ev[2], e1 = c->ev[3];
-  bool first = true;
-  while (true) {
-    // Remove everything below t-2, round by round.
-    ++r;
-    zero(c, cn, 4 * sizeof(unsigned long long));
-    const uint32_t thr = t - 2, tval = t - 1;
-    if (c->opt.record_kernel_times) KT_CUDA(cudaEventRecord(e0, c->stream));
-    k_peel_frontier<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-        alive[ai].as<uint32_t>(), na, sup, state.as<uint32_t>(), thr, r, truss, tval, front[0].as<uint32_t>(), cn + 0,
-        m, err);
+  uint64_t na = 0;
+  uint32_t r = 1;  // next round number
+  unsigned coop_grid = 0;
+  PeelResult* res;
+
+  void init() {
+    const uint64_t m = s->m;
+    state.alloc(c, m * sizeof(uint32_t));
+    alive[0].alloc(c, m * sizeof(uint32_t));
+    alive[1].alloc(c, m * sizeof(uint32_t));
+    front[0].alloc(c, m * sizeof(uint32_t));
+    front[1].alloc(c, m * sizeof(uint32_t));
+    cnt.alloc(c, 8 * sizeof(unsigned long long));
+    mm.alloc(c, 8);
+    adeg.alloc(c, ((uint64_t)s->n + 1) * sizeof(uint32_t));
+    acct.alloc(c, 2 * sizeof(unsigned long long));
+    zero(c, acct.get(), acct.bytes());
+    k_peel_init<<<grid_for(std::max<uint64_t>(m, s->n), 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        m, state.as<uint32_t>(), alive[0].as<uint32_t>(), s->n, s->off.as<uint64_t>(), adeg.as<uint32_t>());
     KT_LAUNCHED(c);
-    int cur = 0;
-    while (true) {
-      const uint64_t nf = read_word<unsigned long long>(c, cn + cur);
-      if (nf == 0) break;
-      ++res.rounds;
-      KT_CUDA(cudaMemsetAsync(cn + (cur ^ 1), 0, sizeof(unsigned long long), c->stream));
-      k_peel_round<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-          front[cur].as<uint32_t>(), nf, s.ends.as<uint64_t>(), s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
-          s.eid.as<uint32_t>(), sup, state.as<uint32_t>(), thr, r, truss, tval, front[cur ^ 1].as<uint32_t>(),
-          cn + (cur ^ 1), m, err);
+    na = m;
+    if (c->opt.persistent) {
+      int per_sm = 0;
+      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade, kPeelThreads, 0));
+      coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+    }
+  }
+
+  PeelArgs args(uint32_t t) {
+    PeelArgs A;
+    A.ends = s->ends.as<uint64_t>();
+    A.off = s->off.as<uint64_t>();
+    A.adj = s->adj.as<uint32_t>();
+    A.eid = s->eid.as<uint32_t>();
+    A.sup = sup;
+    A.state = state.as<uint32_t>();
+    A.truss = truss;
+    A.alive = alive[ai].as<uint32_t>();
+    A.na = na;
+    A.front[0] = front[0].as<uint32_t>();
+    A.front[1] = front[1].as<uint32_t>();
+    A.cnt = cnt.as<unsigned long long>();
+    A.cap = s->m;
+    A.thr = t - 2;
+    A.tval = t - 1;
+    A.r0 = r;
+    A.adeg = adeg.as<uint32_t>();
+    A.acct = acct.as<unsigned long long>();
+    A.words = dev_words(c);
+    A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
+    return A;
+  }
+
+  // Removes every alive edge with support < t-2, to the fixpoint; returns
+  // the alive count.
+  uint64_t cascade(uint32_t t) {
+    PeelArgs A = args(t);
+    zero(c, cnt.get(), cnt.bytes());
+    cudaEvent_t e0;
+    c->timer.begin(c->stream, &c->stats.ms_peel_kernel, &e0);
+    uint64_t rounds = 0;
+    scanned += na;
+    if (coop_grid) {
+      void* p[] = {&A};
+      KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_cascade, dim3(coop_grid), dim3(kPeelThreads), p, 0,
+                                          c->stream));
       KT_LAUNCHED(c);
-      c->stats.peel_launches++;
-      ++r;
-      cur ^= 1;
+      rounds = read_word<unsigned long long>(c, A.cnt + 3);
+    } else {
+      k_level_frontier<<<grid_for(na, kPeelThreads, c->num_sms * 16), kPeelThreads, 0, c->stream>>>(A);
+      KT_LAUNCHED(c);
+      for (uint32_t i = 0;; ++i) {
+        const uint64_t nf = read_word<unsigned long long>(c, A.cnt + (i % 3));
+        if (nf == 0) break;
+        ++rounds;
+        KT_CUDA(cudaMemsetAsync(A.cnt + ((i + 1) % 3), 0, sizeof(unsigned long long), c->stream));
+        k_round<<<grid_for(nf * 32, kPeelThreads, c->num_sms * 16), kPeelThreads, 0, c->stream>>>(A, i, nf);
+        KT_LAUNCHED(c);
+      }
     }
-    if (c->opt.record_kernel_times) {
-      KT_CUDA(cudaEventRecord(e1, c->stream));
-      KT_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      KT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      c->stats.ms_peel_kernel += ms;
-    }
-    ++res.levels;
+    c->timer.end(c->stream, e0, &c->stats.ms_peel_kernel);
+    c->stats.peel_launches++;
     check_words(c, "truss peel");
-    // Survivors form the t-truss.
+    r += (uint32_t)rounds + 1;
+    res->rounds += rounds;
+    res->levels++;
     na = compact(c, na, StillAlive{alive[ai].as<uint32_t>(), state.as<uint32_t>()}, alive[ai ^ 1].as<uint32_t>());
     ai ^= 1;
-    if (na == 0) break;
-    if (first && stop_count && na == stop_count) {
+    return na;
+  }
+
+  // Algorithmic bytes of this peel: 8 per alive-degree unit of every deleted
+  // edge (neighbour id + edge id), 8 per support decrement (read-modify-
+  // write), 4 per alive-list entry scanned by a level frontier.
+  void account() {
+    uint64_t h[2];
+    copy_d2h(c, h, acct.get(), 16);
+    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned;
+    c->stats.peel_decrements += h[1];
+  }
+
+  // (min, max) support over alive edges.
+  void minmax(uint32_t& mn, uint32_t& mx) {
+    const uint32_t init[2] = {0xffffffffu, 0u};
+    copy_h2d(c, mm.get(), init, 8);
+    k_alive_min<<<grid_for(na, 256, c->num_sms * 8), 256, 0, c->stream>>>(alive[ai].as<uint32_t>(), na, sup,
+                                                                            mm.as<uint32_t>());
+    KT_LAUNCHED(c);
+    uint32_t h[2];
+    copy_d2h(c, h, mm.get(), 8);
+    mn = h[0];
+    mx = h[1];
+  }
+};
+
+}  // namespace
+
+PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
+                      uint32_t guess) {
+  PeelResult res;
+  if (s.m == 0) return res;
+  if (t0 < 3) t0 = 3;
+  Peeler P{c, &s, sup, truss};
+  P.res = &res;
+  P.init();
+  uint32_t t = t0;
+  // Jump phase: try `guess` (> t0) from a snapshot; halve toward t0 on failure.
+  if (!truss && guess > t0) {
+    DBuf snap_sup(c, s.m * sizeof(uint32_t)), snap_state(c, s.m * sizeof(uint32_t));
+    DBuf snap_deg(c, P.adeg.bytes());
+    KT_CUDA(cudaMemcpyAsync(snap_deg.get(), P.adeg.get(), P.adeg.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+    KT_CUDA(cudaMemcpyAsync(snap_sup.get(), sup, s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+    KT_CUDA(cudaMemcpyAsync(snap_state.get(), P.state.get(), s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            c->stream));
+    const uint64_t na0 = P.na;
+    const int ai0 = P.ai;
+    uint32_t g = guess;
+    while (g > t0) {
+      if (P.cascade(g)) {
+        t = g;
+        break;
+      }
+      // Undo: the alive list of the snapshot is still in the other buffer.
+      KT_CUDA(cudaMemcpyAsync(sup, snap_sup.get(), s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+      KT_CUDA(cudaMemcpyAsync(P.state.get(), snap_state.get(), s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                              c->stream));
+      KT_CUDA(cudaMemcpyAsync(P.adeg.get(), snap_deg.get(), P.adeg.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+      P.ai = ai0;
+      P.na = na0;
+      g = t0 + (g - t0) / 2;
+    }
+    if (t != t0) {
+      // The t-truss is non-empty: continue upward from it.
+      uint32_t mn, mx;
+      P.minmax(mn, mx);
+      res.kmax = mn + 2;
+      res.count = P.na;
+      t = mn + 3;
+      stop_count = 0;
+    }
+  }
+  bool first = true;
+  while (true) {
+    const uint64_t left = P.cascade(t);
+    if (left == 0) break;
+    if (first && stop_count && left == stop_count) {
       res.kmax = t;
-      res.count = na;
+      res.count = left;
       res.stopped_early = true;
+      P.account();
       return res;
     }
     first = false;
-    KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));
-    k_alive_min<<<grid_for(na, 256, c->num_sms * 8), 256, 0, c->stream>>>(alive[ai].as<uint32_t>(), na, sup,
-                                                                            mn.as<uint32_t>());
-    KT_LAUNCHED(c);
-    const uint32_t smin = read_word<uint32_t>(c, mn.as<uint32_t>());
-    res.kmax = smin + 2;
-    res.count = na;
-    t = smin + 3;
+    uint32_t mn, mx;
+    P.minmax(mn, mx);
+    res.kmax = mn + 2;
+    res.count = left;
+    t = mn + 3;
   }
   if (res.kmax < 3) {
     res.kmax = 0;
     res.count = 0;
   }
+  P.account();
   return res;
 }
 

@@ -51,18 +51,56 @@ void sync(Ctx* c) { KT_CUDA(cudaStreamSynchronize(c->stream)); }
 
 void copy_d2h(Ctx* c, void* dst, const void* src, size_t bytes) {
   if (!bytes) return;
+  c->d2h_bytes += bytes;
   KT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
   sync(c);
 }
 
 void copy_h2d(Ctx* c, void* dst, const void* src, size_t bytes) {
   if (!bytes) return;
+  c->h2d_bytes += bytes;
   KT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
 }
 
 void zero(Ctx* c, void* dptr, size_t bytes) {
   if (!bytes) return;
   KT_CUDA(cudaMemsetAsync(dptr, 0, bytes, c->stream));
+}
+
+cudaEvent_t EventTimer::get() {
+  if (used == pool.size()) {
+    cudaEvent_t e;
+    KT_CUDA(cudaEventCreate(&e));
+    pool.push_back(e);
+  }
+  return pool[used++];
+}
+
+void EventTimer::begin(cudaStream_t s, double* acc, cudaEvent_t* out_a) {
+  (void)acc;
+  *out_a = get();
+  KT_CUDA(cudaEventRecord(*out_a, s));
+}
+
+void EventTimer::end(cudaStream_t s, cudaEvent_t a, double* acc) {
+  cudaEvent_t b = get();
+  KT_CUDA(cudaEventRecord(b, s));
+  open.push_back({a, b, acc});
+}
+
+void EventTimer::resolve() {
+  for (const Span& sp : open) {
+    KT_CUDA(cudaEventSynchronize(sp.b));
+    float ms = 0;
+    KT_CUDA(cudaEventElapsedTime(&ms, sp.a, sp.b));
+    *sp.acc += ms;
+  }
+  open.clear();
+  used = 0;
+}
+
+EventTimer::~EventTimer() {
+  for (cudaEvent_t e : pool) cudaEventDestroy(e);
 }
 
 }  // namespace kt

@@ -66,12 +66,30 @@ struct Timer {
 
 }  // namespace
 
-void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
+void begin_solve_stats(Ctx* c) {
   kt_stats& st = c->stats;
-  st.ms_kcore = st.ms_subgraph = st.ms_support = st.ms_peel = 0;
+  st.ms_parse = st.ms_csr = st.ms_kcore = st.ms_subgraph = st.ms_support = st.ms_peel = st.ms_total = 0;
+  st.ms_support_kernel = st.ms_peel_kernel = 0;
+  st.support_bytes = st.peel_bytes = st.peel_decrements = 0;
   st.core_vertices = st.core_edges = st.predict_vertices = st.predict_edges = 0;
-  st.levels = 0;
-  st.rounds = 0;
+  st.cmax = st.kmax_lower_bound = st.levels = st.rounds = 0;
+}
+
+void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
+  struct Resolve {
+    Ctx* c;
+    ~Resolve() {
+      try {
+        c->timer.resolve();
+      } catch (...) {
+      }
+    }
+  } resolve{c};
+  solve_graph_inner(c, g, kmax, count);
+}
+
+void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
+  kt_stats& st = c->stats;
   *kmax = 0;
   *count = 0;
   Timer tm(c);
@@ -97,7 +115,8 @@ void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
     edge_support(c, s1, sup1.as<uint32_t>());
     st.ms_support += tm.stop();
     tm.start();
-    const PeelResult p1 = truss_peel(c, s1, sup1.as<uint32_t>(), 3, 0, nullptr);
+    // First try half the core number: one cascade removes everything below it.
+    const PeelResult p1 = truss_peel(c, s1, sup1.as<uint32_t>(), 3, 0, nullptr, (cmax + 1) / 2);
     st.ms_peel += tm.stop();
     st.levels += p1.levels;
     st.rounds += (uint32_t)p1.rounds;

@@ -30,11 +30,12 @@ __global__ void k_order_keys(const uint32_t* __restrict__ alive, uint64_t na, co
 }
 
 __global__ void k_order_apply(const uint64_t* __restrict__ keys, uint64_t na, uint32_t* __restrict__ orig,
-                              uint32_t* __restrict__ newid, uint32_t* __restrict__ sdeg) {
+                              uint32_t* __restrict__ newid, uint32_t* __restrict__ sdeg,
+                              const uint32_t* __restrict__ idmap) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
     const uint32_t v = (uint32_t)k;
-    orig[i] = v;
+    orig[i] = v;  // ids of the graph being read; mapped below if it is a compacted copy
     newid[v] = (uint32_t)i;
     sdeg[i] = (uint32_t)(k >> 32);
   }
@@ -125,8 +126,13 @@ struct DegPositive {
   __device__ uint32_t value(uint64_t v) const { return (uint32_t)v; }
 };
 
+__global__ void k_map_ids(uint32_t* __restrict__ ids, uint64_t n, const uint32_t* __restrict__ idmap) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    ids[i] = idmap[ids[i]];
+}
+
 void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
-                     const uint32_t* rem, Sub& s) {
+                     const uint32_t* rem, const uint32_t* idmap, Sub& s) {
   if (na >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "subgraph: too many vertices");
   s.n = (uint32_t)na;
   s.orig.alloc(c, (na ? na : 1) * sizeof(uint32_t));
@@ -149,7 +155,7 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
   DBuf sdeg(c, (na + 1) * sizeof(uint32_t));
   zero(c, sdeg.get(), (na + 1) * sizeof(uint32_t));
   k_order_apply<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>());
+      okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>(), idmap);
   KT_LAUNCHED(c);
   okeys.release();
   scan_u32_to_u64(c, sdeg.as<uint32_t>(), s.off.as<uint64_t>(), na + 1);
@@ -189,6 +195,10 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
       s.off.as<uint64_t>(), s.adj.as<uint32_t>(), na, s.up.as<uint64_t>(), eoff.as<uint64_t>(),
       s.eid.as<uint32_t>(), s.ends.as<uint64_t>());
   KT_LAUNCHED(c);
+  if (idmap) {
+    k_map_ids<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(s.orig.as<uint32_t>(), na, idmap);
+    KT_LAUNCHED(c);
+  }
   // Maximum degree (the last vertex in ascending-degree order).
   uint32_t md = 0;
   copy_d2h(c, &md, sdeg.as<uint32_t>() + (na - 1), sizeof(uint32_t));
@@ -198,13 +208,15 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
 }  // namespace
 
 void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s) {
-  build_from_list(c, g, kc.alive.as<uint32_t>(), kc.n_alive, kc.deg.as<uint32_t>(), kc.rem.as<uint32_t>(), s);
+  (void)g;
+  build_from_list(c, kc.cur(), kc.alive.as<uint32_t>(), kc.n_alive, kc.deg.as<uint32_t>(), kc.rem.as<uint32_t>(),
+                  kc.map(), s);
 }
 
 void build_sub_all(Ctx* c, const Graph& g, Sub& s) {
   DBuf list(c, (g.n ? g.n : 1) * sizeof(uint32_t));
   const uint64_t na = compact(c, g.n, DegPositive{g.deg.as<uint32_t>()}, list.as<uint32_t>());
-  build_from_list(c, g, list.as<uint32_t>(), na, g.deg.as<uint32_t>(), nullptr, s);
+  build_from_list(c, g, list.as<uint32_t>(), na, g.deg.as<uint32_t>(), nullptr, nullptr, s);
 }
 
 }  // namespace kt

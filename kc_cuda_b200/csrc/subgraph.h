@@ -37,6 +37,9 @@ struct PeelResult {
 // Peels from truss level t0 upwards until no edge is left.  stop_count: if
 // nonzero and the t0-truss has exactly that many edges, stop there.
 // truss (optional, device uint32[m]) receives each edge's trussness.
-PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss);
+// guess (> t0, 0 = none): first level to try, undone and halved toward t0 if
+// it empties the graph (only without truss output).
+PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
+                      uint32_t guess = 0);
 
 }  // namespace kt

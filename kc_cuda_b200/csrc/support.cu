@@ -99,12 +99,26 @@ __global__ void k_support_search(uint64_t m, const uint64_t* __restrict__ ends, 
   }
 }
 
+// Algorithmic bytes of a merge-based support count over the degree-oriented
+// graph: 4 * sum over oriented edges (u -> v) of (d+(u) + d+(v)).
+__global__ void k_support_alg(uint64_t m, const uint64_t* __restrict__ ends, const uint64_t* __restrict__ off,
+                              const uint64_t* __restrict__ up, unsigned long long* out) {
+  uint64_t s = 0;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = ends[e];
+    const uint32_t u = (uint32_t)(k >> 32), v = (uint32_t)k;
+    s += (off[u + 1] - up[u]) + (off[v + 1] - up[v]);
+  }
+  s = warp_sum(s);
+  if (lane_id() == 0 && s) atomicAdd(out, (unsigned long long)s);
+}
+
 }  // namespace
 
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup) {
   if (s.m == 0) return;
-  cudaEvent_t e0 = c->ev[0], e1 = c->ev[1];
-  if (c->opt.record_kernel_times) KT_CUDA(cudaEventRecord(e0, c->stream));
+  cudaEvent_t e0;
+  c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
     const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
@@ -124,14 +138,18 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup) {
         s.m, s.ends.as<uint64_t>(), s.off.as<uint64_t>(), s.adj.as<uint32_t>(), sup);
     KT_LAUNCHED(c);
   }
+  c->timer.end(c->stream, e0, &c->stats.ms_support_kernel);
   c->stats.support_launches++;
-  if (c->opt.record_kernel_times) {
-    KT_CUDA(cudaEventRecord(e1, c->stream));
-    KT_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    KT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    c->stats.ms_support_kernel += ms;
-  }
+  // Algorithmic bytes (outside the timed span).
+  DBuf acc(c, 8);
+  zero(c, acc.get(), 8);
+  k_support_alg<<<grid_for(s.m, 256, c->num_sms * 8), 256, 0, c->stream>>>(s.m, s.ends.as<uint64_t>(),
+                                                                             s.off.as<uint64_t>(),
+                                                                             s.up.as<uint64_t>(),
+                                                                             acc.as<unsigned long long>());
+  KT_LAUNCHED(c);
+  const uint64_t sum = read_word<uint64_t>(c, acc.as<uint64_t>());
+  c->stats.support_bytes += 4 * sum + 4 * s.m + 8 * ((uint64_t)s.n + 1);
 }
 
 }  // namespace kt

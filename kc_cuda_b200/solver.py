@@ -47,6 +47,8 @@ class Stats(ctypes.Structure):
         ("ms_support_kernel", ctypes.c_double), ("ms_peel_kernel", ctypes.c_double),
         ("support_launches", ctypes.c_uint64), ("peel_launches", ctypes.c_uint64),
         ("device_bytes_peak", ctypes.c_uint64),
+        ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+        ("peel_decrements", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -73,6 +75,9 @@ SIGNATURES = [
     ("kt_solve", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
     ("kt_solve_tsv", ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32),
                                     ctypes.POINTER(ctypes.c_uint64)]),
+    ("kt_tsv_stage", ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("kt_solve_staged", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
+    ("kt_tsv_free", None, [_P, _P]),
     ("kt_kcore", ctypes.c_int, [_P, _P, ctypes.c_uint32, _U8P, ctypes.POINTER(ctypes.c_uint32)]),
     ("kt_core_numbers", ctypes.c_int, [_P, _P, _U32P]),
     ("kt_edge_support", ctypes.c_int, [_P, _P, _U32P]),
@@ -181,6 +186,13 @@ class Context:
         p = np.asarray(pairs, dtype=np.uint64).reshape(-1, 2)
         return self.load_pairs((p[:, 0] << np.uint64(32)) | p[:, 1])
 
+    def stage_tsv(self, data) -> "StagedTsv":
+        """Copies TSV bytes into device memory (inputs resident in HBM)."""
+        p, n, keep = _buf(data)
+        t = ctypes.c_void_p()
+        self.check(self._L.kt_tsv_stage(self._h, p, n, ctypes.byref(t)))
+        return StagedTsv(self, t, n)
+
     # ---- one-call solve
     def solve_tsv(self, data) -> Tuple[int, int]:
         p, n, keep = _buf(data)
@@ -188,6 +200,29 @@ class Context:
         e = ctypes.c_uint64()
         self.check(self._L.kt_solve_tsv(self._h, p, n, ctypes.byref(k), ctypes.byref(e)))
         return k.value, e.value
+
+
+class StagedTsv:
+    """TSV bytes held in device memory by a context."""
+
+    def __init__(self, ctx: Context, h, nbytes: int):
+        self.ctx = ctx
+        self._h = h
+        self.nbytes = nbytes
+
+    def solve(self) -> Tuple[int, int]:
+        k = ctypes.c_uint32()
+        e = ctypes.c_uint64()
+        self.ctx.check(self.ctx._L.kt_solve_staged(self.ctx._h, self._h, ctypes.byref(k), ctypes.byref(e)))
+        return k.value, e.value
+
+    def free(self):
+        if getattr(self, "_h", None) and self.ctx._h:
+            self.ctx._L.kt_tsv_free(self.ctx._h, self._h)
+        self._h = None
+
+    def __del__(self):
+        self.free()
 
 
 class Graph:
