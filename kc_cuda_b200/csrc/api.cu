@@ -303,6 +303,9 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
   } tab[] = {{"predict", &o.predict},
              {"persistent", &o.persistent},
              {"support_bitmap_max_n", &o.support_bitmap_max_n},
+             {"dense_max_n", &o.dense_max_n},
+             {"dense_min_fill", &o.dense_min_fill},
+             {"recount_gamma", &o.recount_gamma},
              {"timeout_ms", &o.timeout_ms},
              {"parse_pipeline_mb", &o.parse_pipeline_mb},
              {"record_kernel_times", &o.record_kernel_times},

@@ -43,6 +43,9 @@ struct Options {
   int64_t predict = 1;            // run the prediction phase (truss of the max core)
   int64_t persistent = 1;         // peel / k-core rounds inside one cooperative launch
   int64_t support_bitmap_max_n = 1 << 20;  // vertex-centric bitmap support up to this many vertices
+  int64_t dense_max_n = 1 << 16;  // adjacency bitsets (dense mode) up to this many vertices
+  int64_t dense_min_fill = 32;    // dense mode when avg degree * this >= words per row
+  int64_t recount_gamma = 16;     // recount round when |F| * thr * gamma > alive * words
   int64_t timeout_ms = 20000;     // bound on any device-side wait
   int64_t parse_pipeline_mb = 256;  // host->device chunk for file ingest
   int64_t record_kernel_times = 0;  // events around support / peel kernels

@@ -34,6 +34,7 @@
 #include <algorithm>
 
 #include "compact.cuh"
+#include "dense.cuh"
 #include "subgraph.h"
 
 namespace kt {
@@ -58,7 +59,10 @@ struct PeelArgs {
   uint32_t tval;   // trussness recorded for removed edges
   uint32_t r0;     // first round number
   uint32_t* adeg;  // alive degree per vertex (for the byte accounting)
-  unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements
+  uint32_t* bits;  // dense mode: alive adjacency bitsets (null otherwise)
+  uint32_t W;      // words per bitset row
+  uint32_t gamma;  // recount round when nf * thr * gamma > alive * W
+  unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements, [2] recounted edges
   DevWords* words;
   unsigned long long timeout_ns;
 };
@@ -212,15 +216,63 @@ __device__ __forceinline__ void level_frontier(const PeelArgs& A, uint32_t r, ui
   }
 }
 
+__device__ __forceinline__ void clear_edge_bits(const PeelArgs& A, uint32_t e) {
+  const uint64_t k = A.ends[e];
+  const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+  atomicAnd(&A.bits[(uint64_t)x * A.W + (y >> 5)], ~(1u << (y & 31)));
+  atomicAnd(&A.bits[(uint64_t)y * A.W + (x >> 5)], ~(1u << (x & 31)));
+}
+
+// Clears the bits of alive-list edges deleted in rounds (lo, hi].
+__device__ __forceinline__ void clear_deleted(const PeelArgs& A, uint32_t lo, uint32_t hi, uint64_t gtid,
+                                              uint64_t gthreads) {
+  for (uint64_t i = gtid; i < A.na; i += gthreads) {
+    const uint32_t e = A.alive[i];
+    const uint32_t st = A.state[e];
+    if (st > lo && st <= hi) clear_edge_bits(A, e);
+  }
+}
+
+// Dense recount round r: every surviving edge gets its exact support in the
+// graph without this round's frontier; those below the threshold form the
+// next frontier.  Replaces per-triangle decrements when the frontier is a
+// large part of the graph.
+template <int R>
+__device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uint32_t* next,
+                                              unsigned long long* ncnt, uint64_t gwarp, uint64_t gwarps,
+                                              uint64_t& trec) {
+  const uint64_t groups = (A.na + 31) / 32;
+  for (uint64_t g = gwarp; g < groups; g += gwarps) {
+    uint32_t e, sc;
+    bool ok;
+    dense_group<R>(A.alive, g * 32, A.na, A.ends, A.bits, A.W, A.state, e, sc, ok);
+    trec += __popc(__ballot_sync(kFull, ok));
+    bool want = false;
+    if (ok) {
+      A.sup[e] = sc;
+      if (sc < A.thr) {
+        A.state[e] = r + 1;
+        if (A.truss) A.truss[e] = A.tval;
+        want = true;
+      }
+    }
+    push_warp_full(want, e, next, ncnt, A.cap, &A.words->err);
+  }
+}
+
 // One whole cascade in one cooperative launch.
+template <int R>
 __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   level_frontier(A, A.r0, gtid, gthreads);
   if (!grid_barrier(A.words, A.timeout_ns)) return;
   const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
-  uint64_t tdeg = 0, tdec = 0;
+  uint64_t tdeg = 0, tdec = 0, trec = 0;
+  uint64_t alive = A.na;
+  uint32_t cleared = A.r0 - 1;  // bits are current for deletions up to this round
   uint32_t i = 0;
+  bool ok = true;
   while (true) {
     const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
     if (nf == 0) break;
@@ -228,12 +280,31 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
     uint32_t* fr = A.front[i & 1];
     uint32_t* nx = A.front[(i + 1) & 1];
     unsigned long long* nc = &A.cnt[(i + 1) % 3];
-    for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
+    const bool recount = A.bits && (double)nf * (double)(A.thr > 0 ? A.thr : 1) * (double)A.gamma >
+                                       (double)alive * (double)A.W;
+    if (recount) {
+      clear_deleted(A, cleared, r, gtid, gthreads);
+      cleared = r;
+      if (!grid_barrier(A.words, A.timeout_ns)) {
+        ok = false;
+        break;
+      }
+      recount_round<R>(A, r, nx, nc, gwarp, gwarps, trec);
+    } else {
+      for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
+    }
     if (gtid == 0) A.cnt[(i + 2) % 3] = 0;  // read at the start of round i-1, next written in round i+1
-    if (!grid_barrier(A.words, A.timeout_ns)) break;
+    if (!grid_barrier(A.words, A.timeout_ns)) {
+      ok = false;
+      break;
+    }
+    alive -= nf;
     ++i;
   }
+  // Bring the bitsets up to date with this cascade's remaining deletions.
+  if (ok && A.bits) clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
   flush_tallies(A, tdeg, tdec);
+  if (lane_id() == 0 && trec) atomicAdd(&A.acct[2], (unsigned long long)trec);
   if (gtid == 0) A.cnt[3] = i;
 }
 
@@ -297,7 +368,17 @@ struct Peeler {
   uint64_t na = 0;
   uint32_t r = 1;  // next round number
   unsigned coop_grid = 0;
+  int regs = 8;
   PeelResult* res;
+
+  const void* kernel() const {
+    switch (regs) {
+      case 8: return (const void*)k_cascade<8>;
+      case 16: return (const void*)k_cascade<16>;
+      case 32: return (const void*)k_cascade<32>;
+      default: return (const void*)k_cascade<64>;
+    }
+  }
 
   void init() {
     const uint64_t m = s->m;
@@ -309,15 +390,16 @@ struct Peeler {
     cnt.alloc(c, 8 * sizeof(unsigned long long));
     mm.alloc(c, 8);
     adeg.alloc(c, ((uint64_t)s->n + 1) * sizeof(uint32_t));
-    acct.alloc(c, 2 * sizeof(unsigned long long));
+    acct.alloc(c, 4 * sizeof(unsigned long long));
     zero(c, acct.get(), acct.bytes());
     k_peel_init<<<grid_for(std::max<uint64_t>(m, s->n), 256, c->num_sms * 16), 256, 0, c->stream>>>(
         m, state.as<uint32_t>(), alive[0].as<uint32_t>(), s->n, s->off.as<uint64_t>(), adeg.as<uint32_t>());
     KT_LAUNCHED(c);
     na = m;
-    if (c->opt.persistent) {
+    regs = dense_regs(s->W);
+    if (c->opt.persistent || s->W) {
       int per_sm = 0;
-      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade, kPeelThreads, 0));
+      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel(), kPeelThreads, 0));
       coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
     }
   }
@@ -342,6 +424,9 @@ struct Peeler {
     A.r0 = r;
     A.adeg = adeg.as<uint32_t>();
     A.acct = acct.as<unsigned long long>();
+    A.bits = s->W ? s->bits.as<uint32_t>() : nullptr;
+    A.W = s->W;
+    A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
     return A;
@@ -358,8 +443,7 @@ struct Peeler {
     scanned += na;
     if (coop_grid) {
       void* p[] = {&A};
-      KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_cascade, dim3(coop_grid), dim3(kPeelThreads), p, 0,
-                                          c->stream));
+      KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, 0, c->stream));
       KT_LAUNCHED(c);
       rounds = read_word<unsigned long long>(c, A.cnt + 3);
     } else {
@@ -387,11 +471,12 @@ struct Peeler {
 
   // Algorithmic bytes of this peel: 8 per alive-degree unit of every deleted
   // edge (neighbour id + edge id), 8 per support decrement (read-modify-
-  // write), 4 per alive-list entry scanned by a level frontier.
+  // write), 4 per alive-list entry scanned by a level frontier, and in dense
+  // recount rounds one bitset row (4 W bytes) per recounted edge.
   void account() {
-    uint64_t h[2];
-    copy_d2h(c, h, acct.get(), 16);
-    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned;
+    uint64_t h[3];
+    copy_d2h(c, h, acct.get(), 24);
+    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned + 4ULL * s->W * h[2];
     c->stats.peel_decrements += h[1];
   }
 
@@ -424,6 +509,11 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
   if (!truss && guess > t0) {
     DBuf snap_sup(c, s.m * sizeof(uint32_t)), snap_state(c, s.m * sizeof(uint32_t));
     DBuf snap_deg(c, P.adeg.bytes());
+    DBuf snap_bits;
+    if (s.W) {
+      snap_bits.alloc(c, s.bits.bytes());
+      KT_CUDA(cudaMemcpyAsync(snap_bits.get(), s.bits.get(), s.bits.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+    }
     KT_CUDA(cudaMemcpyAsync(snap_deg.get(), P.adeg.get(), P.adeg.bytes(), cudaMemcpyDeviceToDevice, c->stream));
     KT_CUDA(cudaMemcpyAsync(snap_sup.get(), sup, s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
     KT_CUDA(cudaMemcpyAsync(snap_state.get(), P.state.get(), s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
@@ -441,6 +531,8 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
       KT_CUDA(cudaMemcpyAsync(P.state.get(), snap_state.get(), s.m * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                               c->stream));
       KT_CUDA(cudaMemcpyAsync(P.adeg.get(), snap_deg.get(), P.adeg.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+      if (s.W)
+        KT_CUDA(cudaMemcpyAsync(s.bits.get(), snap_bits.get(), s.bits.bytes(), cudaMemcpyDeviceToDevice, c->stream));
       P.ai = ai0;
       P.na = na0;
       g = t0 + (g - t0) / 2;

@@ -16,6 +16,9 @@ struct Sub {
   DBuf up;          // uint64[n]   first entry of each row with neighbour > row
   DBuf ends;        // uint64[m]   u << 32 | v of each edge (new ids, u < v)
   uint32_t max_deg = 0;
+  // Dense mode: alive adjacency as bitsets, row u = words [u*W, (u+1)*W).
+  DBuf bits;
+  uint32_t W = 0;   // 0 = not built
 };
 
 // Builds the subgraph induced by the k-core state's alive vertices.
@@ -23,8 +26,11 @@ void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s);
 // Builds the whole graph as a subgraph (every vertex of degree > 0).
 void build_sub_all(Ctx* c, const Graph& g, Sub& s);
 
-// support.cu: sup[e] = triangles through edge e (all edges of s).
+// support.cu: sup[e] = triangles through edge e (all edges of s).  Uses the
+// bitsets when they are built.
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup);
+// Builds s.bits when the subgraph qualifies for dense mode; returns whether.
+bool build_bits(Ctx* c, Sub& s);
 
 // peel.cu
 struct PeelResult {

@@ -14,6 +14,9 @@
 //
 // Graphs whose vertex count exceeds the bitmap limit use k_support_search:
 // warp per edge, lanes binary-search the shorter row in the longer one.
+#include <algorithm>
+
+#include "dense.cuh"
 #include "subgraph.h"
 
 namespace kt {
@@ -99,6 +102,42 @@ __global__ void k_support_search(uint64_t m, const uint64_t* __restrict__ ends, 
   }
 }
 
+// Dense mode: row bitsets from the sorted rows.
+__global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
+                             uint32_t* __restrict__ bits, uint32_t W) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t u = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); u < n; u += warps) {
+    uint32_t* row = bits + u * W;
+    for (uint64_t j = off[u] + lane_id(); j < off[u + 1]; j += 32) {
+      const uint32_t v = adj[j];
+      atomicOr(&row[v >> 5], 1u << (v & 31));
+    }
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint64_t* __restrict__ ends,
+                                                       const uint32_t* __restrict__ bits, uint32_t W,
+                                                       uint32_t* __restrict__ sup) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t groups = (m + 31) / 32;
+  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
+    uint32_t e, s;
+    bool ok;
+    dense_group<R>(nullptr, g * 32, m, ends, bits, W, nullptr, e, s, ok);
+    if (ok) sup[e] = s;
+  }
+}
+
+template <int R>
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup) {
+  int per_sm = 0;
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<R>, 256, 0));
+  const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
+  k_dense_support<R><<<grid, 256, 0, c->stream>>>(s.m, s.ends.as<uint64_t>(), s.bits.as<uint32_t>(), s.W, sup);
+  KT_LAUNCHED(c);
+}
+
 // Algorithmic bytes of a merge-based support count over the degree-oriented
 // graph: 4 * sum over oriented edges (u -> v) of (d+(u) + d+(v)).
 __global__ void k_support_alg(uint64_t m, const uint64_t* __restrict__ ends, const uint64_t* __restrict__ off,
@@ -115,11 +154,36 @@ __global__ void k_support_alg(uint64_t m, const uint64_t* __restrict__ ends, con
 
 }  // namespace
 
+bool build_bits(Ctx* c, Sub& s) {
+  s.W = 0;
+  s.bits.release();
+  if (s.n == 0 || s.m == 0 || (int64_t)s.n > c->opt.dense_max_n) return false;
+  const uint32_t W = (s.n + 31) / 32;
+  const double avg = 2.0 * (double)s.m / s.n;
+  if (avg * (double)c->opt.dense_min_fill < (double)W) return false;
+  const uint64_t bytes = (uint64_t)s.n * W * 4;
+  if (c->budget && c->in_use + 2 * bytes > c->budget) return false;
+  s.bits.alloc(c, bytes);
+  zero(c, s.bits.get(), bytes);
+  k_bits_build<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), s.bits.as<uint32_t>(), W);
+  KT_LAUNCHED(c);
+  s.W = W;
+  return true;
+}
+
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup) {
   if (s.m == 0) return;
   cudaEvent_t e0;
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
-  if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
+  if (s.W) {
+    switch (dense_regs(s.W)) {
+      case 8: launch_dense_support<8>(c, s, sup); break;
+      case 16: launch_dense_support<16>(c, s, sup); break;
+      case 32: launch_dense_support<32>(c, s, sup); break;
+      default: launch_dense_support<64>(c, s, sup); break;
+    }
+  } else if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
     const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
       KT_CUDA(cudaFuncSetAttribute(k_support_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

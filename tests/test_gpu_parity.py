@@ -138,9 +138,36 @@ def test_without_prediction_same_answer(ctx, golden):
         ctx.set_option("predict", 1)
 
 
+@pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never"])
+def test_modes_support_trussness_answer(ctx, golden, mode):
+    """Sparse lists vs dense bitsets, and dense peels that recount every
+    round vs never: all bit-identical to the oracle."""
+    opts = {"sparse": {"dense_max_n": 0},
+            "dense_recount_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1 << 30},
+            "dense_recount_never": {"dense_min_fill": 1 << 30, "recount_gamma": 1}}[mode]
+    old = {k: ctx.get_option(k) for k in opts}
+    for k, v in opts.items():
+        ctx.set_option(k, v)
+    try:
+        for name, e in golden.items():
+            if "file" not in e or "error" in e:
+                continue
+            g = ctx.load_tsv(golden_bytes(e))
+            edges = g.edges()
+            assert np.array_equal(g.tricount(), O.support(edges)), (mode, name)
+            assert np.array_equal(g.trussness(), O.trussness(edges)), (mode, name)
+            assert g.kmax_truss() == (e["kmax"], e["edges"]), (mode, name)
+        for name, e, gg in spec_graphs(golden):
+            assert ctx.solve_tsv(gg.tsv_bytes()) == (e["kmax"], e["edges"]), (mode, name)
+    finally:
+        for k, v in old.items():
+            ctx.set_option(k, v)
+
+
 def test_search_fallback_support_kernel(ctx, golden):
     """The binary-search support kernel (used above the bitmap size limit)."""
     ctx.set_option("support_bitmap_max_n", 0)
+    ctx.set_option("dense_max_n", 0)
     try:
         for name, e in golden.items():
             if "file" not in e or "error" in e:
@@ -150,6 +177,7 @@ def test_search_fallback_support_kernel(ctx, golden):
             assert g.kmax_truss() == (e["kmax"], e["edges"]), name
     finally:
         ctx.set_option("support_bitmap_max_n", 1 << 20)
+        ctx.set_option("dense_max_n", 1 << 16)
 
 
 def test_parse_error_reports_line(ctx):
