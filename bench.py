@@ -303,8 +303,10 @@ def main():
                        "vertices": n_vertices, "edges": n_edges, "tsv_bytes": int(tsv.nbytes),
                        "kmax": answer[0], "kmax_truss_edges": answer[1], "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (TSV bytes re-read every step)",
-                       "cmax": stats_last["cmax"], "core_edges": stats_last["core_edges"],
-                       "predict_edges": stats_last["predict_edges"]},
+                       "cmax": stats_last["cmax"], "core_vertices": stats_last["core_vertices"],
+                       "core_edges": stats_last["core_edges"], "predict_vertices": stats_last["predict_vertices"],
+                       "predict_edges": stats_last["predict_edges"], "levels": stats_last["levels"],
+                       "rounds": stats_last["rounds"], "peel_decrements": stats_last["peel_decrements"]},
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": est["h2d_bytes"] // args.steps,
                     "d2h_bytes_per_step": est["d2h_bytes"] // args.steps, "ms_per_step": 1000 * e2e_step},
             "gpu_launches": launches,

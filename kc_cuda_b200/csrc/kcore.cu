@@ -180,22 +180,27 @@ __global__ void k_recount(const uint32_t* __restrict__ alive, uint64_t n_alive, 
   }
 }
 
+// Big rows of the recount: 1024-entry chunks spread over all warps, one
+// atomic per chunk.
 __global__ void k_recount_big(const uint32_t* __restrict__ big, const unsigned long long* nbig_p,
                               const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
                               const uint32_t* __restrict__ rem, uint32_t* __restrict__ deg) {
-  __shared__ uint32_t tmp[33];
   const uint64_t nbig = *nbig_p;
+  const uint64_t gwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint64_t base = 0;
   for (uint64_t bi = 0; bi < nbig; ++bi) {
     const uint32_t v = big[bi];
     const uint64_t b = off[v], e = off[v + 1];
     const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
-    uint32_t c = 0;
-    for (uint64_t cidx = blockIdx.x; cidx < chunks; cidx += gridDim.x) {
-      const uint64_t cb = b + cidx * kChunkRow, ce = min(e, cb + kChunkRow);
-      for (uint64_t j = cb + threadIdx.x; j < ce; j += blockDim.x) c += rem[adj[j]] == kAlive;
+    for (uint64_t q = (gwarp + gwarps - base % gwarps) % gwarps; q < chunks; q += gwarps) {
+      const uint64_t cb = b + q * kChunkRow, ce = min(e, cb + kChunkRow);
+      uint32_t c = 0;
+      for (uint64_t j = cb + lane_id(); j < ce; j += 32) c += rem[adj[j]] == kAlive;
+      c = warp_sum(c);
+      if (lane_id() == 0 && c) atomicAdd(&deg[v], c);
     }
-    c = block_sum<uint32_t>(c, tmp);
-    if (threadIdx.x == 0 && c) atomicAdd(&deg[v], c);
+    base += chunks;
   }
 }
 
@@ -241,6 +246,7 @@ __global__ void k_compact_rows(const uint32_t* __restrict__ alive, uint64_t na, 
   for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); i < na; i += warps) {
     const uint32_t v = alive[i];
     const uint64_t b = off[v], e = off[v + 1];
+    if (e - b > kBigRow) continue;  // k_compact_big_rows
     uint64_t pos = noff[i];
     const uint64_t end = noff[i + 1];
     for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
@@ -254,6 +260,35 @@ __global__ void k_compact_rows(const uint32_t* __restrict__ alive, uint64_t na, 
       const uint64_t p = pos + __popc(bal & lanemask_lt());
       if (keep && p < end) nadj[p] = newid[w];
       pos += __popc(bal);
+    }
+  }
+}
+
+// Rows longer than kBigRow in the compaction: one block per row, tiles of
+// blockDim entries with a block scan for the output positions.
+__global__ void k_compact_big_rows(const uint32_t* __restrict__ alive, uint64_t na, const uint64_t* __restrict__ off,
+                                   const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
+                                   const uint32_t* __restrict__ newid, const uint64_t* __restrict__ noff,
+                                   uint32_t* __restrict__ nadj) {
+  __shared__ uint32_t tmp[33];
+  for (uint64_t i = blockIdx.x; i < na; i += gridDim.x) {
+    const uint32_t v = alive[i];
+    const uint64_t b = off[v], e = off[v + 1];
+    if (e - b <= kBigRow) continue;  // uniform per block
+    uint64_t pos = noff[i];
+    const uint64_t end = noff[i + 1];
+    for (uint64_t j0 = b; j0 < e; j0 += blockDim.x) {
+      const uint64_t j = j0 + threadIdx.x;
+      uint32_t w = 0;
+      uint32_t keep = 0;
+      if (j < e) {
+        w = adj[j];
+        keep = rem[w] == kAlive;
+      }
+      uint32_t total;
+      const uint32_t r = block_excl_scan<uint32_t>(keep, tmp, &total);
+      if (keep && pos + r < end) nadj[pos + r] = newid[w];
+      pos += total;
     }
   }
 }
@@ -273,6 +308,114 @@ __global__ void k_members_mapped(const uint32_t* __restrict__ rem, uint64_t n, c
                                  uint8_t* __restrict__ out) {
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
     if (rem[v] == kAlive) out[map[v]] = 1;
+}
+
+
+struct ProbeArgs {
+  const uint64_t* off;
+  const uint32_t* adj;
+  uint32_t* deg;
+  uint32_t* rem;
+  const uint32_t* alive;
+  uint64_t n_alive;
+  uint32_t* front[2];
+  uint32_t* big;
+  unsigned long long* cnt;  // [0..2] frontier sizes, [3..4] big-row counts, [5] rounds, [6] removed
+  uint64_t cap;
+  uint32_t k, tag;
+  DevWords* words;
+  unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ void drop_neighbours(const ProbeArgs& A, uint64_t b, uint64_t e, uint32_t* next,
+                                                unsigned long long* ncnt) {
+  for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
+    bool want = false;
+    uint32_t w = 0;
+    if (j < e) {
+      w = A.adj[j];
+      if (A.rem[w] == kAlive) {
+        const uint32_t old = atomicSub(&A.deg[w], 1u);
+        if (old == A.k) {
+          A.rem[w] = A.tag;
+          want = true;
+        }
+      }
+    }
+    push_warp(want, w, next, ncnt, A.cap, &A.words->err);
+  }
+}
+
+// A whole probe (frontier init and every round) in one cooperative launch.
+__global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
+  const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
+  for (uint64_t i = gtid; i < ((A.n_alive + 31) & ~31ULL); i += gthreads) {
+    bool want = false;
+    uint32_t v = 0;
+    if (i < A.n_alive) {
+      v = A.alive[i];
+      if (A.rem[v] == kAlive && A.deg[v] < A.k) {
+        A.rem[v] = A.tag;
+        want = true;
+      }
+    }
+    push_warp(want, v, A.front[0], &A.cnt[0], A.cap, &A.words->err);
+  }
+  if (!grid_barrier(A.words, A.timeout_ns)) return;
+  uint32_t i = 0;
+  uint64_t removed = 0;
+  while (true) {
+    const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
+    if (nf == 0) break;
+    removed += nf;
+    const uint32_t* fr = A.front[i & 1];
+    uint32_t* nx = A.front[(i + 1) & 1];
+    unsigned long long* nc = &A.cnt[(i + 1) % 3];
+    unsigned long long* bc = &A.cnt[3 + (i & 1)];
+    for (uint64_t f = gwarp; f < nf; f += gwarps) {
+      const uint32_t v = fr[f];
+      const uint64_t b = A.off[v], e = A.off[v + 1];
+      if (e - b > kBigRow) {
+        if (lane_id() == 0) {
+          const unsigned long long p = atomicAdd(bc, 1ULL);
+          if (p < A.cap)
+            A.big[p] = v;
+          else
+            atomicOr(&A.words->err, kDevErrCapacity);
+        }
+        continue;
+      }
+      drop_neighbours(A, b, e, nx, nc);
+    }
+    if (gtid == 0) {
+      A.cnt[(i + 2) % 3] = 0;        // read at the start of round i-1
+      A.cnt[3 + ((i + 1) & 1)] = 0;  // big count of round i-1, read before the barrier ending it
+    }
+    if (!grid_barrier(A.words, A.timeout_ns)) return;
+    const uint64_t nbig = ld_acquire_u64(bc);
+    if (nbig) {
+      // Rows longer than kBigRow: 1024-entry chunks spread over all warps.
+      uint64_t base = 0;
+      for (uint64_t bi = 0; bi < nbig; ++bi) {
+        const uint32_t v = A.big[bi];
+        const uint64_t b = A.off[v], e = A.off[v + 1];
+        const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
+        for (uint64_t q = (gwarp + gwarps - base % gwarps) % gwarps; q < chunks; q += gwarps) {
+          const uint64_t cb = b + q * kChunkRow;
+          drop_neighbours(A, cb, min(e, cb + kChunkRow), nx, nc);
+        }
+        base += chunks;
+      }
+      if (!grid_barrier(A.words, A.timeout_ns)) return;
+    }
+    ++i;
+  }
+  if (gtid == 0) {
+    A.cnt[5] = i;
+    A.cnt[6] = removed;
+  }
 }
 
 }  // namespace
@@ -329,6 +472,10 @@ void KCore::compact_to_alive(Ctx* c, uint32_t level) {
       alive.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
       newid.as<uint32_t>(), L.off.as<uint64_t>(), L.adj.as<uint32_t>());
   KT_LAUNCHED(c);
+  k_compact_big_rows<<<c->num_sms * 8, 256, 0, c->stream>>>(
+      alive.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
+      newid.as<uint32_t>(), L.off.as<uint64_t>(), L.adj.as<uint32_t>());
+  KT_LAUNCHED(c);
   L.max_deg = g.max_deg;  // an upper bound is enough here
   newid.release();
   // Install (the old local graph, if any, is released by the swap).
@@ -371,31 +518,63 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
   unsigned long long* cn = cnt.as<unsigned long long>();
   zero(c, cnt.get(), cnt.bytes());
   uint32_t* err = &dev_words(c)->err;
-  k_frontier_init<<<grid_for(n_alive, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), k, tag, front[0].as<uint32_t>(), cn + 0,
-      n, err);
-  KT_LAUNCHED(c);
   uint64_t removed = 0;
-  int cur_f = 0;
-  while (true) {
-    const uint64_t nf = read_word<unsigned long long>(c, cn + cur_f);
-    if (nf == 0) break;
-    removed += nf;
-    ++rounds;
-    KT_CUDA(cudaMemsetAsync(cn + (cur_f ^ 1), 0, sizeof(unsigned long long), c->stream));
-    KT_CUDA(cudaMemsetAsync(cn + 4, 0, sizeof(unsigned long long), c->stream));
-    k_expand<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-        front[cur_f].as<uint32_t>(), nf, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), deg.as<uint32_t>(),
-        rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(), cn + (cur_f ^ 1), big.as<uint32_t>(), cn + 4,
-        n, err);
+  if (c->opt.persistent) {
+    ProbeArgs A;
+    A.off = g.off.as<uint64_t>();
+    A.adj = g.adj.as<uint32_t>();
+    A.deg = deg.as<uint32_t>();
+    A.rem = rem.as<uint32_t>();
+    A.alive = alive.as<uint32_t>();
+    A.n_alive = n_alive;
+    A.front[0] = front[0].as<uint32_t>();
+    A.front[1] = front[1].as<uint32_t>();
+    A.big = big.as<uint32_t>();
+    A.cnt = cn;
+    A.cap = n;
+    A.k = k;
+    A.tag = tag;
+    A.words = dev_words(c);
+    A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
+    if (!coop_grid) {
+      int per_sm = 0;
+      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe, 256, 0));
+      coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+    }
+    void* p[] = {&A};
+    KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_probe, dim3(coop_grid), dim3(256), p, 0, c->stream));
     KT_LAUNCHED(c);
-    k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g.off.as<uint64_t>(),
-                                                        g.adj.as<uint32_t>(), deg.as<uint32_t>(),
-                                                        rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(),
-                                                        cn + (cur_f ^ 1), n, err);
+    uint64_t h[2];
+    copy_d2h(c, h, cn + 5, 16);
+    rounds += h[0];
+    removed = h[1];
+  } else {
+    k_frontier_init<<<grid_for(n_alive, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), k, tag, front[0].as<uint32_t>(),
+        cn + 0, n, err);
     KT_LAUNCHED(c);
-    cur_f ^= 1;
+    int cur_f = 0;
+    while (true) {
+      const uint64_t nf = read_word<unsigned long long>(c, cn + cur_f);
+      if (nf == 0) break;
+      removed += nf;
+      ++rounds;
+      KT_CUDA(cudaMemsetAsync(cn + (cur_f ^ 1), 0, sizeof(unsigned long long), c->stream));
+      KT_CUDA(cudaMemsetAsync(cn + 4, 0, sizeof(unsigned long long), c->stream));
+      k_expand<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+          front[cur_f].as<uint32_t>(), nf, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), deg.as<uint32_t>(),
+          rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(), cn + (cur_f ^ 1), big.as<uint32_t>(),
+          cn + 4, n, err);
+      KT_LAUNCHED(c);
+      k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g.off.as<uint64_t>(),
+                                                          g.adj.as<uint32_t>(), deg.as<uint32_t>(),
+                                                          rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(),
+                                                          cn + (cur_f ^ 1), n, err);
+      KT_LAUNCHED(c);
+      cur_f ^= 1;
+    }
   }
+  ++probes;
   check_words(c, "k-core probe");
   return n_alive - removed;
 }

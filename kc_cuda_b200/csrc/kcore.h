@@ -22,6 +22,8 @@ struct KCore {
   uint64_t n_alive = 0;
   uint32_t cmax = 0;
   uint64_t rounds = 0;
+  uint64_t probes = 0;
+  unsigned coop_grid = 0;
   std::vector<uint32_t> levels;  // levels[tag] = k of that probe
   std::vector<uint32_t> succ;    // tags of probes that were kept
 
