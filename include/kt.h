@@ -101,6 +101,21 @@ void kt_tsv_free(kt_ctx* ctx, kt_tsv* tsv);
  * the largest k with a non-empty k-core.  Replaces kmax_core_gpu
  * (src/kc.cu:770-884).  Either output may be NULL. */
 kt_status kt_kcore(kt_ctx* ctx, kt_graph* g, uint32_t k, uint8_t* member_out, uint32_t* cmax_out);
+/* k-core membership for callers that cannot allocate device memory at the
+ * moment they need it (inside another runtime's fully reserved pool, from
+ * host callbacks where an allocating CUDA call may block, or on paths that
+ * cannot afford the synchronisation an allocation may imply).  No
+ * counterpart in the reference.  DEVICE pointers: d_off (n+1 row offsets)
+ * and d_adj (neighbour ids; symmetric, no self-loops, any row order) in,
+ * d_member (n bytes, 1 = in the k-core) out; stream may be NULL (default
+ * stream).  Allocates nothing: its working memory is one fixed device array
+ * of about 16 MB that every GPU loading the library holds until exit, which
+ * caps n at 1,048,576 (KT_ERR_LIMIT above).  The first call on a device looks
+ * up that array's device address and should come before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race.  Returns
+ * after the stream has finished the call. */
+kt_status kt_kcore_noalloc(const uint64_t* d_off, const uint32_t* d_adj, uint32_t n, uint32_t k, uint8_t* d_member,
+                           void* stream);
 /* Core number of every vertex (num_vertices entries). */
 kt_status kt_core_numbers(kt_ctx* ctx, kt_graph* g, uint32_t* core_out);
 /* Triangles through each edge, in kt_graph_edges order.  Replaces

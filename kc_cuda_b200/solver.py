@@ -79,6 +79,8 @@ SIGNATURES = [
     ("kt_solve_staged", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
     ("kt_tsv_free", None, [_P, _P]),
     ("kt_kcore", ctypes.c_int, [_P, _P, ctypes.c_uint32, _U8P, ctypes.POINTER(ctypes.c_uint32)]),
+    ("kt_kcore_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
     ("kt_core_numbers", ctypes.c_int, [_P, _P, _U32P]),
     ("kt_edge_support", ctypes.c_int, [_P, _P, _U32P]),
     ("kt_edge_trussness", ctypes.c_int, [_P, _P, _U32P]),
