@@ -394,6 +394,10 @@ struct Peeler {
     zero(c, acct.get(), acct.bytes());
     k_peel_init<<<grid_for(std::max<uint64_t>(m, s->n), 256, c->num_sms * 16), 256, 0, c->stream>>>(
         m, state.as<uint32_t>(), alive[0].as<uint32_t>(), s->n, s->off.as<uint64_t>(), adeg.as<uint32_t>());
+    // Dense mode: keep the alive list in tile order (compaction preserves it).
+    if (s->W)
+      KT_CUDA(cudaMemcpyAsync(alive[0].get(), s->order.get(), m * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                              c->stream));
     KT_LAUNCHED(c);
     na = m;
     regs = dense_regs(s->W);

@@ -19,6 +19,11 @@ struct Sub {
   // Dense mode: alive adjacency as bitsets, row u = words [u*W, (u+1)*W).
   DBuf bits;
   uint32_t W = 0;   // 0 = not built
+  // Dense mode: edge ids in tile order (u >> tb, v >> tb, u, v), so that the
+  // rows read by concurrently processed edges stay within two vertex blocks
+  // whose bitsets fit in L2 together.
+  DBuf order;
+  uint32_t tile_bits = 0;
 };
 
 // Builds the subgraph induced by the k-core state's alive vertices.

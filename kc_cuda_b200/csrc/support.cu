@@ -116,7 +116,8 @@ __global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint64_t* __restrict__ ends,
+__global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
+                                                       const uint64_t* __restrict__ ends,
                                                        const uint32_t* __restrict__ bits, uint32_t W,
                                                        uint32_t* __restrict__ sup) {
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
@@ -124,8 +125,18 @@ __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint64_
   for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
     uint32_t e, s;
     bool ok;
-    dense_group<R>(nullptr, g * 32, m, ends, bits, W, nullptr, e, s, ok);
+    dense_group<R>(order, g * 32, m, ends, bits, W, nullptr, e, s, ok);
     if (ok) sup[e] = s;
+  }
+}
+
+// Tile keys: (u >> tb) << 16 | (v >> tb), stable-sorted with the edge ids.
+__global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint32_t tb, uint64_t* __restrict__ keys,
+                            uint32_t* __restrict__ ids) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = ends[e];
+    keys[e] = ((k >> (32 + tb)) << 16) | (((uint32_t)k) >> tb);
+    ids[e] = (uint32_t)e;
   }
 }
 
@@ -134,7 +145,8 @@ void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup) {
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<R>, 256, 0));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-  k_dense_support<R><<<grid, 256, 0, c->stream>>>(s.m, s.ends.as<uint64_t>(), s.bits.as<uint32_t>(), s.W, sup);
+  k_dense_support<R><<<grid, 256, 0, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+                                                  s.bits.as<uint32_t>(), s.W, sup);
   KT_LAUNCHED(c);
 }
 
@@ -169,6 +181,17 @@ bool build_bits(Ctx* c, Sub& s) {
       s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), s.bits.as<uint32_t>(), W);
   KT_LAUNCHED(c);
   s.W = W;
+  // Tile order: blocks of 2^tb vertices, two blocks' bitsets within ~48 MB.
+  uint32_t tb = 16;
+  while (tb > 6 && 2ull * (1ull << tb) * W * 4 > (48ull << 20)) --tb;
+  s.tile_bits = tb;
+  s.order.alloc(c, s.m * sizeof(uint32_t));
+  DBuf keys(c, s.m * sizeof(uint64_t));
+  k_tile_keys<<<grid_for(s.m, 256, c->num_sms * 16), 256, 0, c->stream>>>(s.m, s.ends.as<uint64_t>(), tb,
+                                                                            keys.as<uint64_t>(),
+                                                                            s.order.as<uint32_t>());
+  KT_LAUNCHED(c);
+  radix_sort_u64(c, keys.as<uint64_t>(), s.order.as<uint32_t>(), s.m, 32);
   return true;
 }
 
