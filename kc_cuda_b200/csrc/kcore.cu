@@ -5,8 +5,8 @@
 // decrements the degrees of its surviving neighbours; a neighbour whose
 // degree steps from k to k-1 (atomicSub returns k) joins the next frontier,
 // so every vertex enters a frontier at most once.  Rows of more than
-// kBigRow entries are expanded by whole blocks, in chunks, so hub rows do
-// not serialise on one warp.
+// kBigRow entries are expanded by a whole block each, so hub rows do not
+// serialise on one warp.
 //
 // The search for the maximum core (the reference steps k by a fixed stride
 // with host backups, src/kc.cu:770-884) ramps k geometrically from the
@@ -27,7 +27,6 @@ namespace kt {
 namespace {
 
 constexpr unsigned kBigRow = 2048;
-constexpr unsigned kChunkRow = 1024;
 
 struct AliveF {
   const uint32_t* rem;
@@ -118,38 +117,32 @@ __global__ void k_expand(const uint32_t* __restrict__ front, uint64_t nf, const 
   }
 }
 
-// Big rows: every block takes chunks of every big row.
+// Big rows: one block per row (rows round-robin over blocks), each warp
+// taking 32-entry windows of it.
 __global__ void k_expand_big(const uint32_t* __restrict__ big, const unsigned long long* nbig_p,
                              const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
                              uint32_t* __restrict__ deg, uint32_t* __restrict__ rem, uint32_t k, uint32_t tag,
                              uint32_t* __restrict__ next, unsigned long long* ncnt, uint64_t cap, uint32_t* err) {
   const uint64_t nbig = *nbig_p;
-  uint64_t chunk_base = 0;
-  for (uint64_t bi = 0; bi < nbig; ++bi) {
+  for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
     const uint32_t v = big[bi];
     const uint64_t b = off[v], e = off[v + 1];
-    const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
-    // Chunks are numbered across all big rows so blocks stay balanced.
-    for (uint64_t cidx = (blockIdx.x + gridDim.x - chunk_base % gridDim.x) % gridDim.x; cidx < chunks;
-         cidx += gridDim.x) {
-      const uint64_t cb = b + cidx * kChunkRow, ce = min(e, cb + kChunkRow);
-      for (uint64_t j = cb + threadIdx.x; j < cb + ((ce - cb + 31) & ~31ULL); j += blockDim.x) {
-        bool want = false;
-        uint32_t w = 0;
-        if (j < ce) {
-          w = adj[j];
-          if (rem[w] == kAlive) {
-            const uint32_t old = atomicSub(&deg[w], 1u);
-            if (old == k) {
-              rem[w] = tag;
-              want = true;
-            }
+    for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x) {
+      const uint64_t j = j0 + lane_id();
+      bool want = false;
+      uint32_t w = 0;
+      if (j < e) {
+        w = adj[j];
+        if (rem[w] == kAlive) {
+          const uint32_t old = atomicSub(&deg[w], 1u);
+          if (old == k) {
+            rem[w] = tag;
+            want = true;
           }
         }
-        push_warp(want, w, next, ncnt, cap, err);
       }
+      push_warp(want, w, next, ncnt, cap, err);
     }
-    chunk_base += chunks;
   }
 }
 
@@ -180,27 +173,19 @@ __global__ void k_recount(const uint32_t* __restrict__ alive, uint64_t n_alive, 
   }
 }
 
-// Big rows of the recount: 1024-entry chunks spread over all warps, one
-// atomic per chunk.
+// Big rows of the recount: one block per row, a warp-level count and one
+// atomic per warp per row.
 __global__ void k_recount_big(const uint32_t* __restrict__ big, const unsigned long long* nbig_p,
                               const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
                               const uint32_t* __restrict__ rem, uint32_t* __restrict__ deg) {
   const uint64_t nbig = *nbig_p;
-  const uint64_t gwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint64_t base = 0;
-  for (uint64_t bi = 0; bi < nbig; ++bi) {
+  for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
     const uint32_t v = big[bi];
     const uint64_t b = off[v], e = off[v + 1];
-    const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
-    for (uint64_t q = (gwarp + gwarps - base % gwarps) % gwarps; q < chunks; q += gwarps) {
-      const uint64_t cb = b + q * kChunkRow, ce = min(e, cb + kChunkRow);
-      uint32_t c = 0;
-      for (uint64_t j = cb + lane_id(); j < ce; j += 32) c += rem[adj[j]] == kAlive;
-      c = warp_sum(c);
-      if (lane_id() == 0 && c) atomicAdd(&deg[v], c);
-    }
-    base += chunks;
+    uint32_t c = 0;
+    for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) c += rem[adj[j]] == kAlive;
+    c = warp_sum(c);
+    if (lane_id() == 0 && c) atomicAdd(&deg[v], c);
   }
 }
 
@@ -396,17 +381,12 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
     if (!grid_barrier(A.words, A.timeout_ns)) return;
     const uint64_t nbig = ld_acquire_u64(bc);
     if (nbig) {
-      // Rows longer than kBigRow: 1024-entry chunks spread over all warps.
-      uint64_t base = 0;
-      for (uint64_t bi = 0; bi < nbig; ++bi) {
+      // Rows longer than kBigRow: one block per row, warps on 32-entry windows.
+      for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
         const uint32_t v = A.big[bi];
         const uint64_t b = A.off[v], e = A.off[v + 1];
-        const uint64_t chunks = (e - b + kChunkRow - 1) / kChunkRow;
-        for (uint64_t q = (gwarp + gwarps - base % gwarps) % gwarps; q < chunks; q += gwarps) {
-          const uint64_t cb = b + q * kChunkRow;
-          drop_neighbours(A, cb, min(e, cb + kChunkRow), nx, nc);
-        }
-        base += chunks;
+        for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x)
+          drop_neighbours(A, j0, min(e, j0 + 32), nx, nc);
       }
       if (!grid_barrier(A.words, A.timeout_ns)) return;
     }

@@ -7,11 +7,13 @@
 // digit run is an error here (the reference would silently merge it with
 // the next line).
 //
-// Layout: each thread owns a 32-byte chunk; a line belongs to the thread whose
-// chunk holds the '\n' before it (line 0 belongs to thread 0).  Pass 1 counts
-// lines per 8 KB block with 16-byte loads; after a scan, pass 2 stages the
-// block's bytes (plus a 1 KB overhang) in shared memory, block-scans the
-// per-thread line counts and parses each owned line into slot
+// Layout: each thread owns a 36-byte chunk (9 words, so the 32 chunk starts
+// of a warp fall on distinct shared-memory banks); a line belongs to the
+// thread whose chunk holds the '\n' before it (line 0 belongs to thread 0).
+// Pass 1 counts lines per 9 KB block with 16-byte loads; after a scan, pass 2
+// stages the block's bytes (plus a 1 KB overhang) in shared memory, finds the
+// chunk's newlines a word at a time (__vcmpeq4), block-scans the per-thread
+// line counts and parses each owned line word by word into slot
 // block_offset + thread_offset + i.  A slot gets min(x,y) << 32 | max(x,y),
 // or ~0 for a blank line or a self-loop (sorted to the end, then dropped).
 #include "kt_device.cuh"
@@ -22,122 +24,165 @@ namespace kt {
 namespace {
 
 constexpr unsigned kParseThreads = 256;
-constexpr unsigned kChunk = 32;
-constexpr unsigned kBlockBytes = kParseThreads * kChunk;  // 8192
+constexpr unsigned kChunk = 36;  // 9 words: chunk starts fall on distinct smem banks
+constexpr unsigned kBlockBytes = kParseThreads * kChunk;  // 9216 (a multiple of 16)
 constexpr unsigned kOverhang = 1024;
 
-__device__ __forceinline__ uint32_t count_nl16(uint4 v) {
-  const uint32_t nl = 0x0a0a0a0au;
-  return (__popc(__vcmpeq4(v.x, nl)) + __popc(__vcmpeq4(v.y, nl)) + __popc(__vcmpeq4(v.z, nl)) +
-          __popc(__vcmpeq4(v.w, nl))) >> 3;
-}
+__device__ __forceinline__ uint32_t count_nl4(uint32_t w) { return __popc(__vcmpeq4(w, 0x0a0a0a0au)) >> 3; }
 
-// Lines owned by one chunk: its '\n' bytes except one at len-1, plus line 0.
-__device__ __forceinline__ uint32_t owned_lines(const uint8_t* buf, uint64_t len, uint64_t s) {
-  if (s >= len) return 0;
-  uint32_t c = 0;
-  if (s + kChunk <= len) {
-    const uint4* p = reinterpret_cast<const uint4*>(buf + s);
-    c = count_nl16(p[0]) + count_nl16(p[1]);
-    if (s + kChunk == len && buf[len - 1] == '\n') c -= 1;
-  } else {
-    for (uint64_t q = s; q < len; ++q) c += (buf[q] == '\n' && q + 1 < len);
-  }
-  return c + (s == 0 ? 1u : 0u);
-}
-
+// Lines owned by a block: its '\n' bytes except one at len-1, plus line 0.
 __global__ void __launch_bounds__(kParseThreads) k_count_lines(const uint8_t* __restrict__ buf, uint64_t len,
                                                                uint32_t* __restrict__ block_lines) {
   __shared__ uint32_t tmp[33];
-  const uint64_t s = (uint64_t)blockIdx.x * kBlockBytes + (uint64_t)threadIdx.x * kChunk;
-  const uint32_t c = owned_lines(buf, len, s);
-  const uint32_t t = block_sum<uint32_t>(c, tmp);
-  if (threadIdx.x == 0) block_lines[blockIdx.x] = t;
+  const uint64_t blo = (uint64_t)blockIdx.x * kBlockBytes;
+  const uint64_t bhi = min(len, blo + kBlockBytes);
+  const uint64_t nvec = (bhi - blo + 15) / 16;  // the padding past len is zero
+  uint32_t c = 0;
+  for (uint64_t i = threadIdx.x; i < nvec; i += kParseThreads) {
+    const uint4 v = reinterpret_cast<const uint4*>(buf + blo)[i];
+    c += count_nl4(v.x) + count_nl4(v.y) + count_nl4(v.z) + count_nl4(v.w);
+  }
+  c = block_sum<uint32_t>(c, tmp);
+  if (threadIdx.x == 0) {
+    if (bhi == len && len > 0 && buf[len - 1] == '\n') c -= 1;
+    if (blockIdx.x == 0 && len > 0) c += 1;
+    block_lines[blockIdx.x] = c;
+  }
 }
 
-struct ByteSrc {
-  const uint8_t* sm;   // staged bytes [lo, hi)
-  const uint8_t* g;    // global buffer
+__device__ __forceinline__ bool is_digit(uint32_t b) { return b >= '0' && b < 128; }
+
+struct Bytes {
+  const uint32_t* sm;  // staged words of [lo, hi)
+  const uint8_t* g;    // global buffer (zero-padded past len)
   uint64_t lo, hi, len;
-  __device__ __forceinline__ int at(uint64_t q) const {  // -1 past the end
-    if (q >= len) return -1;
-    return (q >= lo && q < hi) ? sm[q - lo] : g[q];
+  // Word holding byte address a (a multiple of 4).
+  __device__ __forceinline__ uint32_t word(uint64_t a) const {
+    if (a >= lo && a + 4 <= hi) return sm[(a - lo) >> 2];
+    return *reinterpret_cast<const uint32_t*>(g + a);
   }
 };
 
-__device__ __forceinline__ bool is_digit(int b) { return b >= '0' && b < 128; }
+// Parses the line starting at `start`: ~0 for a blank line or a self-loop,
+// min << 32 | max otherwise; *bad when the line holds a single number.
+__device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t start, bool* bad, uint32_t* vmax) {
+  enum { kPreX, kX, kPreY, kY };
+  int st = kPreX;
+  uint32_t x = 0, y = 0;
+  uint64_t a = start & ~3ull;
+  uint32_t k0 = (uint32_t)(start & 3);
+  while (true) {
+    const uint32_t w = B.word(a);
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      if (k < k0) continue;
+      const uint64_t pos = a + k;
+      const uint32_t b = (w >> (8 * k)) & 0xffu;
+      const bool end = pos >= B.len || b == '\n';
+      const bool dig = !end && is_digit(b);
+      if (st == kPreX) {
+        if (end) return ~0ull;
+        if (dig) {
+          x = b - '0';
+          st = kX;
+        }
+      } else if (st == kX) {
+        if (dig) {
+          x = x * 10u + (b - '0');
+        } else if (end) {
+          *bad = true;
+          return ~0ull;
+        } else {
+          st = kPreY;
+        }
+      } else if (st == kPreY) {
+        if (dig) {
+          y = b - '0';
+          st = kY;
+        } else if (end) {
+          *bad = true;
+          return ~0ull;
+        }
+      } else {
+        if (dig) {
+          y = y * 10u + (b - '0');
+        } else {
+          *vmax = max(*vmax, max(x, y));
+          if (x == y) return ~0ull;
+          return x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
+        }
+      }
+    }
+    k0 = 0;
+    a += 4;
+  }
+}
 
 __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __restrict__ buf, uint64_t len,
                                                                const uint64_t* __restrict__ block_off,
                                                                uint64_t* __restrict__ keys, DevWords* words) {
-  __shared__ __align__(16) uint8_t stage[kBlockBytes + kOverhang];
+  __shared__ __align__(16) uint32_t stage[(kBlockBytes + kOverhang) / 4];
   __shared__ uint32_t tmp[33];
   const uint64_t blo = (uint64_t)blockIdx.x * kBlockBytes;
   const uint64_t bhi = min(len, blo + kBlockBytes + kOverhang);
-  // The device buffer is padded to a multiple of 16 bytes plus 16, so whole
-  // 16-byte loads below bhi rounded up stay inside the allocation.
+  // The device buffer is padded (zeros) to whole 16-byte words past len.
   const uint64_t nvec = (bhi - blo + 15) / 16;
   for (uint64_t i = threadIdx.x; i < nvec; i += kParseThreads)
     reinterpret_cast<uint4*>(stage)[i] = reinterpret_cast<const uint4*>(buf + blo)[i];
   __syncthreads();
-  const ByteSrc src{stage, buf, blo, bhi, len};
+  const Bytes B{stage, buf, blo, blo + nvec * 16, len};
 
   const uint64_t s = blo + (uint64_t)threadIdx.x * kChunk;
-  // Owned-line count from the staged copy.
+  const uint64_t e = min(len, s + kChunk);
+  // Owned lines: one per '\n' in [s, e) that is not the last byte, plus line 0.
+  uint32_t nlmask[kChunk / 4];
   uint32_t c = 0;
-  if (s < len) {
-    const uint64_t e = min(len, s + kChunk);
-    for (uint64_t q = s; q < e; ++q) c += (stage[q - blo] == '\n' && q + 1 < len);
-    c += (s == 0);
+#pragma unroll
+  for (uint32_t j = 0; j < kChunk / 4; ++j) {
+    const uint64_t a = s + 4 * j;
+    uint32_t m = 0;
+    if (a < e) {
+      m = __vcmpeq4(stage[(a - blo) >> 2], 0x0a0a0a0au);
+      // Drop bytes at or past e, and a '\n' at len-1 (it starts no line).
+      const uint64_t lim = min(e, len - 1);
+      if (a + 4 > lim) m &= lim > a ? (0xffffffffu >> (8 * (4 - (uint32_t)(lim - a)))) : 0u;
+    }
+    nlmask[j] = m;
+    c += __popc(m) >> 3;
   }
+  if (s == 0 && len > 0) c += 1;
   uint32_t total;
   uint64_t slot = block_off[blockIdx.x] + block_excl_scan<uint32_t>(c, tmp, &total);
   if (c == 0) return;
   uint32_t vmax = 0;
-  bool any = false;
-  const uint64_t e = min(len, s + kChunk);
-  uint64_t q = s;
-  bool first = (s == 0);
-  while (true) {
-    uint64_t start;
-    if (first) {
-      start = 0;
-      first = false;
-    } else {
-      while (q < e && src.at(q) != '\n') ++q;
-      if (q >= e) break;
-      start = q + 1;
-      ++q;
-      if (start >= len) break;
+  bool any = false, bad = false;
+  if (s == 0 && len > 0) {
+    const uint64_t key = parse_line(B, 0, &bad, &vmax);
+    if (bad) {
+      atomicOr(&words->err, kDevErrParse);
+      atomicMin(&words->bad_line, (unsigned long long)slot);
+      bad = false;
     }
-    // Parse the line at `start`.
-    uint64_t p = start;
-    int b = src.at(p);
-    while (b >= 0 && b != '\n' && !is_digit(b)) b = src.at(++p);
-    uint64_t key = ~0ULL;
-    if (is_digit(b)) {
-      uint32_t x = 0, y = 0;
-      while (is_digit(b)) {
-        x = x * 10u + (uint32_t)(b - '0');
-        b = src.at(++p);
-      }
-      while (b >= 0 && b != '\n' && !is_digit(b)) b = src.at(++p);
-      if (!is_digit(b)) {
-        atomicOr(&words->err, kDevErrParse);
-        atomicMin(&words->bad_line, (unsigned long long)slot);
-      } else {
-        while (is_digit(b)) {
-          y = y * 10u + (uint32_t)(b - '0');
-          b = src.at(++p);
-        }
-        vmax = max(vmax, max(x, y));
-        any = true;
-        if (x != y) key = x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
-      }
-    }
+    any = true;
     keys[slot++] = key;
   }
-  if (any) atomicMax(reinterpret_cast<unsigned int*>(&words->counters[0]), vmax + 0u);
+#pragma unroll
+  for (uint32_t j = 0; j < kChunk / 4; ++j) {
+    uint32_t m = nlmask[j];
+    while (m) {
+      const uint32_t k = (__ffs(m) - 1) >> 3;
+      m &= ~(0xffu << (8 * k));
+      const uint64_t key = parse_line(B, s + 4 * j + k + 1, &bad, &vmax);
+      if (bad) {
+        atomicOr(&words->err, kDevErrParse);
+        atomicMin(&words->bad_line, (unsigned long long)slot);
+        bad = false;
+      }
+      any = true;
+      keys[slot++] = key;
+    }
+  }
+  if (any) atomicMax(reinterpret_cast<unsigned int*>(&words->counters[0]), vmax);
   if (any) atomicOr(reinterpret_cast<unsigned int*>(&words->counters[1]), 1u);
 }
 

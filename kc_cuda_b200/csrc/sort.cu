@@ -4,7 +4,9 @@
 // One pass = tile histograms -> digit-major exclusive scan -> stable scatter.
 // A tile is 4096 keys: each of the 8 warps owns 512 consecutive keys, ranks
 // them with __match_any_sync against warp-private running digit counters,
-// then the block turns the per-warp counts into per-warp digit offsets.  A
+// then the block turns the per-warp counts into per-warp digit offsets,
+// places the tile in shared memory sorted by digit, and writes every digit's
+// run with consecutive threads on consecutive addresses.  A
 // first pass histograms all eight digit positions at once so passes whose
 // digit is the same for every key are skipped.
 #include "kt_device.cuh"
@@ -50,21 +52,31 @@ __global__ void __launch_bounds__(kSortThreads) k_tile_hist(const uint64_t* __re
   tile_hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Scatter of one tile: rank every key (stable), place the tile sorted by
+// digit in shared memory, then write each digit's run with consecutive
+// threads on consecutive addresses.
 template <bool kVals>
 __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __restrict__ keys,
                                                           const uint32_t* __restrict__ vals, uint64_t n, int shift,
                                                           uint32_t ntiles, const uint32_t* __restrict__ tile_off,
                                                           uint64_t* __restrict__ keys_out,
                                                           uint32_t* __restrict__ vals_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(smem_raw);                          // kSortTile
+  uint32_t* svals = reinterpret_cast<uint32_t*>(smem_raw + kSortTile * 8);          // kSortTile (kVals)
   __shared__ uint32_t wrun[kSortWarps][256];
   __shared__ uint32_t toff[256];
+  __shared__ uint32_t dstart[256];
+  __shared__ uint32_t tmp[33];
   const unsigned w = warp_id(), l = lane_id();
   toff[threadIdx.x] = tile_off[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
 #pragma unroll
   for (unsigned q = 0; q < kSortWarps; ++q) wrun[q][threadIdx.x] = 0;
   __syncthreads();
 
-  const uint64_t wbase = (uint64_t)blockIdx.x * kSortTile + (uint64_t)w * kWarpKeys;
+  const uint64_t tbase = (uint64_t)blockIdx.x * kSortTile;
+  const uint32_t tn = (uint32_t)(n - tbase < kSortTile ? n - tbase : kSortTile);
+  const uint64_t wbase = tbase + (uint64_t)w * kWarpKeys;
   uint64_t k[kSortIpt];
   uint32_t v[kSortIpt];
   uint32_t rank[kSortIpt];
@@ -85,6 +97,7 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __rest
   }
   __syncthreads();
   {
+    // Per digit: warp prefixes, then the tile-local start of the digit.
     const unsigned d = threadIdx.x;
     uint32_t s = 0;
 #pragma unroll
@@ -93,6 +106,8 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __rest
       wrun[q][d] = s;
       s += t;
     }
+    uint32_t total;
+    dstart[d] = block_excl_scan<uint32_t>(s, tmp, &total);
   }
   __syncthreads();
 #pragma unroll
@@ -100,10 +115,18 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __rest
     const uint64_t idx = wbase + j * 32 + l;
     if (idx < n) {
       const uint32_t d = (uint32_t)((k[j] >> shift) & 255);
-      const uint32_t pos = toff[d] + wrun[w][d] + rank[j];
-      keys_out[pos] = k[j];
-      if (kVals) vals_out[pos] = v[j];
+      const uint32_t p = dstart[d] + wrun[w][d] + rank[j];
+      skeys[p] = k[j];
+      if (kVals) svals[p] = v[j];
     }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < tn; i += kSortThreads) {
+    const uint64_t key = skeys[i];
+    const uint32_t d = (uint32_t)((key >> shift) & 255);
+    const uint32_t pos = toff[d] + (i - dstart[d]);
+    keys_out[pos] = key;
+    if (kVals) vals_out[pos] = svals[i];
   }
 }
 
@@ -123,6 +146,12 @@ void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits
   copy_d2h(c, h.data(), hist.get(), h.size() * sizeof(unsigned long long));
 
   const uint32_t ntiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  static bool attr_set = false;
+  if (!attr_set) {
+    KT_CUDA(cudaFuncSetAttribute(k_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortTile * 12));
+    KT_CUDA(cudaFuncSetAttribute(k_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortTile * 8));
+    attr_set = true;
+  }
   DBuf keys_alt(c, n * sizeof(uint64_t));
   DBuf vals_alt;
   if (vals) vals_alt.alloc(c, n * sizeof(uint32_t));
@@ -140,11 +169,11 @@ void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits
     KT_LAUNCHED(c);
     scan_u32(c, th.as<uint32_t>(), th.as<uint32_t>(), (uint64_t)ntiles * 256);
     if (vals)
-      k_scatter<true><<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, vsrc, n, shift, ntiles, th.as<uint32_t>(), kdst,
-                                                              vdst);
+      k_scatter<true><<<ntiles, kSortThreads, kSortTile * 12, c->stream>>>(ksrc, vsrc, n, shift, ntiles,
+                                                                           th.as<uint32_t>(), kdst, vdst);
     else
-      k_scatter<false><<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, nullptr, n, shift, ntiles, th.as<uint32_t>(),
-                                                               kdst, nullptr);
+      k_scatter<false><<<ntiles, kSortThreads, kSortTile * 8, c->stream>>>(ksrc, nullptr, n, shift, ntiles,
+                                                                           th.as<uint32_t>(), kdst, nullptr);
     KT_LAUNCHED(c);
     std::swap(ksrc, kdst);
     std::swap(vsrc, vdst);
