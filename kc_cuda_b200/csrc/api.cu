@@ -306,6 +306,7 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"dense_max_n", &o.dense_max_n},
              {"dense_min_fill", &o.dense_min_fill},
              {"recount_gamma", &o.recount_gamma},
+             {"capped_support", &o.capped_support},
              {"timeout_ms", &o.timeout_ms},
              {"parse_pipeline_mb", &o.parse_pipeline_mb},
              {"record_kernel_times", &o.record_kernel_times},

@@ -46,6 +46,7 @@ struct Options {
   int64_t dense_max_n = 1 << 16;  // adjacency bitsets (dense mode) up to this many vertices
   int64_t dense_min_fill = 32;    // dense mode when avg degree * this >= words per row
   int64_t recount_gamma = 16;     // recount round when |F| * thr * gamma > alive * words
+  int64_t capped_support = 1;     // search phase: abandon supports that cannot reach the threshold
   int64_t timeout_ms = 20000;     // bound on any device-side wait
   int64_t parse_pipeline_mb = 256;  // host->device chunk for file ingest
   int64_t record_kernel_times = 0;  // events around support / peel kernels

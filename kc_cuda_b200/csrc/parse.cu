@@ -12,9 +12,9 @@
 // thread whose chunk holds the '\n' before it (line 0 belongs to thread 0).
 // Pass 1 counts lines per 9 KB block with 16-byte loads; after a scan, pass 2
 // stages the block's bytes (plus a 1 KB overhang) in shared memory, finds the
-// chunk's newlines a word at a time (__vcmpeq4), block-scans the per-thread
-// line counts and parses each owned line word by word into slot
-// block_offset + thread_offset + i.  A slot gets min(x,y) << 32 | max(x,y),
+// chunk's newlines a word at a time (__vcmpeq4), lists the block's line
+// starts in shared memory, and deals the lines round-robin to the threads;
+// line i of the block goes to slot block_offset + i.  A slot gets min(x,y) << 32 | max(x,y),
 // or ~0 for a blank line or a self-loop (sorted to the end, then dropped).
 #include "kt_device.cuh"
 #include "kt_internal.h"
@@ -50,78 +50,52 @@ __global__ void __launch_bounds__(kParseThreads) k_count_lines(const uint8_t* __
   }
 }
 
-__device__ __forceinline__ bool is_digit(uint32_t b) { return b >= '0' && b < 128; }
+__device__ __forceinline__ bool is_digit(int b) { return b >= '0' && b < 128; }
 
 struct Bytes {
-  const uint32_t* sm;  // staged words of [lo, hi)
-  const uint8_t* g;    // global buffer (zero-padded past len)
+  const uint8_t* sm;  // staged bytes [lo, hi)
+  const uint8_t* g;   // global buffer
   uint64_t lo, hi, len;
-  // Word holding byte address a (a multiple of 4).
-  __device__ __forceinline__ uint32_t word(uint64_t a) const {
-    if (a >= lo && a + 4 <= hi) return sm[(a - lo) >> 2];
-    return *reinterpret_cast<const uint32_t*>(g + a);
+  __device__ __forceinline__ int at(uint64_t q) const {  // -1 past the end
+    if (q >= len) return -1;
+    return q < hi ? sm[q - lo] : g[q];
   }
 };
 
-// Parses the line starting at `start`: ~0 for a blank line or a self-loop,
-// min << 32 | max otherwise; *bad when the line holds a single number.
-__device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t start, bool* bad, uint32_t* vmax) {
-  enum { kPreX, kX, kPreY, kY };
-  int st = kPreX;
+// The line at `start`: ~0 for a blank line or a self-loop, min << 32 | max
+// otherwise; *bad when it holds a single number.
+__device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t p, bool* bad, uint32_t* vmax) {
+  int b = B.at(p);
+  while (b >= 0 && b != '\n' && !is_digit(b)) b = B.at(++p);
+  if (!is_digit(b)) return ~0ull;
   uint32_t x = 0, y = 0;
-  uint64_t a = start & ~3ull;
-  uint32_t k0 = (uint32_t)(start & 3);
-  while (true) {
-    const uint32_t w = B.word(a);
-#pragma unroll
-    for (uint32_t k = 0; k < 4; ++k) {
-      if (k < k0) continue;
-      const uint64_t pos = a + k;
-      const uint32_t b = (w >> (8 * k)) & 0xffu;
-      const bool end = pos >= B.len || b == '\n';
-      const bool dig = !end && is_digit(b);
-      if (st == kPreX) {
-        if (end) return ~0ull;
-        if (dig) {
-          x = b - '0';
-          st = kX;
-        }
-      } else if (st == kX) {
-        if (dig) {
-          x = x * 10u + (b - '0');
-        } else if (end) {
-          *bad = true;
-          return ~0ull;
-        } else {
-          st = kPreY;
-        }
-      } else if (st == kPreY) {
-        if (dig) {
-          y = b - '0';
-          st = kY;
-        } else if (end) {
-          *bad = true;
-          return ~0ull;
-        }
-      } else {
-        if (dig) {
-          y = y * 10u + (b - '0');
-        } else {
-          *vmax = max(*vmax, max(x, y));
-          if (x == y) return ~0ull;
-          return x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
-        }
-      }
-    }
-    k0 = 0;
-    a += 4;
+  while (is_digit(b)) {
+    x = x * 10u + (uint32_t)(b - '0');
+    b = B.at(++p);
   }
+  while (b >= 0 && b != '\n' && !is_digit(b)) b = B.at(++p);
+  if (!is_digit(b)) {
+    *bad = true;
+    return ~0ull;
+  }
+  while (is_digit(b)) {
+    y = y * 10u + (uint32_t)(b - '0');
+    b = B.at(++p);
+  }
+  *vmax = max(*vmax, max(x, y));
+  if (x == y) return ~0ull;
+  return x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
 }
 
+// Phase 1 finds the block's line starts (newlines a word at a time, a block
+// scan, offsets into shared memory); phase 2 deals the lines round-robin to
+// the threads, so the per-line work is balanced and the keys are written
+// with consecutive threads on consecutive slots.
 __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __restrict__ buf, uint64_t len,
                                                                const uint64_t* __restrict__ block_off,
                                                                uint64_t* __restrict__ keys, DevWords* words) {
   __shared__ __align__(16) uint32_t stage[(kBlockBytes + kOverhang) / 4];
+  __shared__ uint16_t starts[kBlockBytes + 1];
   __shared__ uint32_t tmp[33];
   const uint64_t blo = (uint64_t)blockIdx.x * kBlockBytes;
   const uint64_t bhi = min(len, blo + kBlockBytes + kOverhang);
@@ -130,7 +104,6 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
   for (uint64_t i = threadIdx.x; i < nvec; i += kParseThreads)
     reinterpret_cast<uint4*>(stage)[i] = reinterpret_cast<const uint4*>(buf + blo)[i];
   __syncthreads();
-  const Bytes B{stage, buf, blo, blo + nvec * 16, len};
 
   const uint64_t s = blo + (uint64_t)threadIdx.x * kChunk;
   const uint64_t e = min(len, s + kChunk);
@@ -150,40 +123,41 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
     nlmask[j] = m;
     c += __popc(m) >> 3;
   }
-  if (s == 0 && len > 0) c += 1;
+  const bool first = (s == 0 && len > 0);
+  if (first) c += 1;
   uint32_t total;
-  uint64_t slot = block_off[blockIdx.x] + block_excl_scan<uint32_t>(c, tmp, &total);
-  if (c == 0) return;
-  uint32_t vmax = 0;
-  bool any = false, bad = false;
-  if (s == 0 && len > 0) {
-    const uint64_t key = parse_line(B, 0, &bad, &vmax);
-    if (bad) {
-      atomicOr(&words->err, kDevErrParse);
-      atomicMin(&words->bad_line, (unsigned long long)slot);
-      bad = false;
-    }
-    any = true;
-    keys[slot++] = key;
-  }
+  uint32_t pos = block_excl_scan<uint32_t>(c, tmp, &total);
+  if (first) starts[pos++] = 0;
 #pragma unroll
   for (uint32_t j = 0; j < kChunk / 4; ++j) {
     uint32_t m = nlmask[j];
     while (m) {
       const uint32_t k = (__ffs(m) - 1) >> 3;
       m &= ~(0xffu << (8 * k));
-      const uint64_t key = parse_line(B, s + 4 * j + k + 1, &bad, &vmax);
-      if (bad) {
-        atomicOr(&words->err, kDevErrParse);
-        atomicMin(&words->bad_line, (unsigned long long)slot);
-        bad = false;
-      }
-      any = true;
-      keys[slot++] = key;
+      starts[pos++] = (uint16_t)(s + 4 * j + k + 1 - blo);
     }
   }
-  if (any) atomicMax(reinterpret_cast<unsigned int*>(&words->counters[0]), vmax);
-  if (any) atomicOr(reinterpret_cast<unsigned int*>(&words->counters[1]), 1u);
+  __syncthreads();
+  const Bytes B{reinterpret_cast<const uint8_t*>(stage), buf, blo, blo + nvec * 16, len};
+  const uint64_t slot0 = block_off[blockIdx.x];
+  uint32_t vmax = 0;
+  bool any = false;
+  for (uint32_t i = threadIdx.x; i < total; i += kParseThreads) {
+    bool bad = false;
+    const uint64_t key = parse_line(B, blo + starts[i], &bad, &vmax);
+    if (bad) {
+      atomicOr(&words->err, kDevErrParse);
+      atomicMin(&words->bad_line, (unsigned long long)(slot0 + i));
+    }
+    any = true;
+    keys[slot0 + i] = key;
+  }
+  vmax = warp_max(vmax);
+  const unsigned anyw = __ballot_sync(kFull, any);
+  if (lane_id() == 0 && anyw) {
+    atomicMax(reinterpret_cast<unsigned int*>(&words->counters[0]), vmax);
+    atomicOr(reinterpret_cast<unsigned int*>(&words->counters[1]), 1u);
+  }
 }
 
 }  // namespace

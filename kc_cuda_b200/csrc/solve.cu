@@ -143,10 +143,13 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   st.ms_subgraph += tm.stop();
   tm.start();
   DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
-  edge_support(c, s2, sup2.as<uint32_t>());
+  // The search peel starts at level max(L, 3) with no jump, so supports
+  // below its threshold only need to be known as "below".
+  const uint32_t t2 = std::max<uint32_t>(L, 3);
+  edge_support(c, s2, sup2.as<uint32_t>(), c->opt.capped_support ? t2 - 2 : 0);
   st.ms_support += tm.stop();
   tm.start();
-  const PeelResult p2 = truss_peel(c, s2, sup2.as<uint32_t>(), std::max<uint32_t>(L, 3), L >= 3 ? C : 0, nullptr);
+  const PeelResult p2 = truss_peel(c, s2, sup2.as<uint32_t>(), t2, L >= 3 ? C : 0, nullptr);
   st.ms_peel += tm.stop();
   st.levels += p2.levels;
   st.rounds += (uint32_t)p2.rounds;

@@ -32,8 +32,10 @@ void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s);
 void build_sub_all(Ctx* c, const Graph& g, Sub& s);
 
 // support.cu: sup[e] = triangles through edge e (all edges of s).  Uses the
-// bitsets when they are built.
-void edge_support(Ctx* c, const Sub& s, uint32_t* sup);
+// bitsets when they are built.  cap > 0 (dense mode only): an edge whose
+// support is below cap may get any value below cap -- enough for a peel whose
+// first level removes everything below cap.
+void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap = 0);
 // Builds s.bits when the subgraph qualifies for dense mode; returns whether.
 bool build_bits(Ctx* c, Sub& s);
 
