@@ -32,6 +32,7 @@
 // strides with host backups and rollbacks (src/kc.cu:1140-1309); the result
 // is the same kmax and edge count.
 #include <algorithm>
+#include <memory>
 
 #include "compact.cuh"
 #include "dense.cuh"
@@ -356,6 +357,15 @@ struct StillAlive {
   __device__ uint32_t value(uint64_t i) const { return list[i]; }
 };
 
+// Ends (u << 32 | v) of the alive edges of a list.
+struct AliveEnds {
+  const uint32_t* list;
+  const uint32_t* state;
+  const uint64_t* ends;
+  __device__ bool keep(uint64_t i) const { return state[list[i]] == kAlive; }
+  __device__ uint64_t value(uint64_t i) const { return ends[list[i]]; }
+};
+
 // Peel state of one working graph on the device.
 struct Peeler {
   Ctx* c;
@@ -382,16 +392,19 @@ struct Peeler {
 
   void init() {
     const uint64_t m = s->m;
-    state.alloc(c, m * sizeof(uint32_t));
-    alive[0].alloc(c, m * sizeof(uint32_t));
-    alive[1].alloc(c, m * sizeof(uint32_t));
-    front[0].alloc(c, m * sizeof(uint32_t));
-    front[1].alloc(c, m * sizeof(uint32_t));
-    cnt.alloc(c, 8 * sizeof(unsigned long long));
-    mm.alloc(c, 8);
-    adeg.alloc(c, ((uint64_t)s->n + 1) * sizeof(uint32_t));
-    acct.alloc(c, 4 * sizeof(unsigned long long));
-    zero(c, acct.get(), acct.bytes());
+    state = DBuf(c, m * sizeof(uint32_t));
+    alive[0] = DBuf(c, m * sizeof(uint32_t));
+    alive[1] = DBuf(c, m * sizeof(uint32_t));
+    front[0] = DBuf(c, m * sizeof(uint32_t));
+    front[1] = DBuf(c, m * sizeof(uint32_t));
+    cnt = DBuf(c, 8 * sizeof(unsigned long long));
+    mm = DBuf(c, 8);
+    adeg = DBuf(c, ((uint64_t)s->n + 1) * sizeof(uint32_t));
+    if (!acct.get()) {
+      acct = DBuf(c, 4 * sizeof(unsigned long long));
+      zero(c, acct.get(), acct.bytes());
+    }
+    ai = 0;
     k_peel_init<<<grid_for(std::max<uint64_t>(m, s->n), 256, c->num_sms * 16), 256, 0, c->stream>>>(
         m, state.as<uint32_t>(), alive[0].as<uint32_t>(), s->n, s->off.as<uint64_t>(), adeg.as<uint32_t>());
     // Dense mode: keep the alive list in tile order (compaction preserves it).
@@ -401,6 +414,7 @@ struct Peeler {
     KT_LAUNCHED(c);
     na = m;
     regs = dense_regs(s->W);
+    coop_grid = 0;
     if (c->opt.persistent || s->W) {
       int per_sm = 0;
       KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel(), kPeelThreads, 0));
@@ -484,6 +498,31 @@ struct Peeler {
     c->stats.peel_decrements += h[1];
   }
 
+  // Replaces the working graph by its alive part (renumbered, with its own
+  // bitsets and exact supports) once most edges are gone; the alive edges
+  // form a truss, so their supports in the new graph equal their current
+  // ones.  Returns whether it compacted.
+  bool compact_graph(std::unique_ptr<Sub>& own, DBuf& own_sup) {
+    if (truss || na == 0 || na * 4 > s->m || s->m < (1u << 20)) return false;
+    account();
+    zero(c, acct.get(), acct.bytes());
+    scanned = 0;
+    DBuf keys(c, na * sizeof(uint64_t));
+    const uint64_t k = kt::compact(c, na, AliveEnds{alive[ai].as<uint32_t>(), state.as<uint32_t>(),
+                                                    s->ends.as<uint64_t>()},
+                                   keys.as<uint64_t>());
+    std::unique_ptr<Sub> ns(new Sub);
+    build_sub_from_keys(c, keys.as<uint64_t>(), k, s->n, *ns);
+    DBuf nsup(c, (ns->m ? ns->m : 1) * sizeof(uint32_t));
+    edge_support(c, *ns, nsup.as<uint32_t>());
+    own.swap(ns);
+    own_sup = std::move(nsup);
+    s = own.get();
+    sup = own_sup.as<uint32_t>();
+    init();
+    return true;
+  }
+
   // (min, max) support over alive edges.
   void minmax(uint32_t& mn, uint32_t& mx) {
     const uint32_t init[2] = {0xffffffffu, 0u};
@@ -500,11 +539,20 @@ struct Peeler {
 
 }  // namespace
 
+void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out) {
+  Graph g;
+  build_graph(c, keys, m, n_ids, g);
+  build_sub_all(c, g, out);
+  build_bits(c, out);
+}
+
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
                       uint32_t guess) {
   PeelResult res;
   if (s.m == 0) return res;
   if (t0 < 3) t0 = 3;
+  std::unique_ptr<Sub> own;
+  DBuf own_sup;
   Peeler P{c, &s, sup, truss};
   P.res = &res;
   P.init();
@@ -568,6 +616,7 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
     res.kmax = mn + 2;
     res.count = left;
     t = mn + 3;
+    P.compact_graph(own, own_sup);
   }
   if (res.kmax < 3) {
     res.kmax = 0;

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 
+#include "compact.cuh"
 #include "solve.h"
 
 namespace kt {
@@ -42,6 +43,15 @@ __global__ void k_map_back(const uint64_t* __restrict__ ends, uint64_t m, const 
     if (p < gm && gedges[p] == key) out[p] = val[e];
   }
 }
+
+// Ends of the edges whose (capped) support reaches a threshold.
+struct AtLeast {
+  const uint32_t* sup;
+  const uint64_t* ends;
+  uint32_t thr;
+  __device__ bool keep(uint64_t e) const { return sup[e] >= thr; }
+  __device__ uint64_t value(uint64_t e) const { return ends[e]; }
+};
 
 struct Timer {
   Ctx* c;
@@ -146,10 +156,32 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   // The search peel starts at level max(L, 3) with no jump, so supports
   // below its threshold only need to be known as "below".
   const uint32_t t2 = std::max<uint32_t>(L, 3);
-  edge_support(c, s2, sup2.as<uint32_t>(), c->opt.capped_support ? t2 - 2 : 0);
+  const bool capped = c->opt.capped_support && s2.W;
+  edge_support(c, s2, sup2.as<uint32_t>(), capped ? t2 - 2 : 0);
+  // Edges below the first threshold leave in the first round: when they are
+  // most of the graph, continue on the rest (the L-truss of the survivors is
+  // the L-truss of the core) instead of clearing them one by one.
+  Sub s3;
+  DBuf sup3;
+  const Sub* sp = &s2;
+  uint32_t* supp = sup2.as<uint32_t>();
+  if (capped) {
+    DBuf keys(c, (s2.m ? s2.m : 1) * sizeof(uint64_t));
+    const uint64_t k = compact(c, s2.m, AtLeast{sup2.as<uint32_t>(), s2.ends.as<uint64_t>(), t2 - 2},
+                               keys.as<uint64_t>());
+    if (k * 2 < s2.m) {
+      build_sub_from_keys(c, keys.as<uint64_t>(), k, s2.n, s3);
+      sup3 = DBuf(c, (s3.m ? s3.m : 1) * sizeof(uint32_t));
+      edge_support(c, s3, sup3.as<uint32_t>());
+      sp = &s3;
+      supp = sup3.as<uint32_t>();
+    } else {
+      edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
+    }
+  }
   st.ms_support += tm.stop();
   tm.start();
-  const PeelResult p2 = truss_peel(c, s2, sup2.as<uint32_t>(), t2, L >= 3 ? C : 0, nullptr);
+  const PeelResult p2 = truss_peel(c, *sp, supp, t2, L >= 3 ? C : 0, nullptr);
   st.ms_peel += tm.stop();
   st.levels += p2.levels;
   st.rounds += (uint32_t)p2.rounds;

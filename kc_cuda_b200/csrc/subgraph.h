@@ -50,6 +50,9 @@ struct PeelResult {
 // Peels from truss level t0 upwards until no edge is left.  stop_count: if
 // nonzero and the t0-truss has exactly that many edges, stop there.
 // truss (optional, device uint32[m]) receives each edge's trussness.
+// The subgraph of edge keys (u << 32 | v, ids below n_ids; consumed), with
+// bitsets when it qualifies.
+void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out);
 // guess (> t0, 0 = none): first level to try, undone and halved toward t0 if
 // it empties the graph (only without truss output).
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
