@@ -1,0 +1,63 @@
+"""Small, named workloads for profiling single kernels of the solver.
+
+    python -m kc_cuda_b200.cases <case> [--reps N]
+
+Cases (each fits in a few GB of device memory, inputs larger than L2):
+  dense-support   Erdos-Renyi G(n=40000, M=48,000,000 draws), seed 7: one
+                  kt_edge_support call -> k_dense_support<64> on ~46M edges
+                  (bitset rows of 1250 words).
+  rmat21-solve    R-MAT scale 21, edge factor 32, seed 2, cliques 80/120/200:
+                  one kt_solve_staged (every stage; peel kernel k_cascade<8>).
+  rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+from . import gen
+from .solver import Context
+
+
+def dense_support(reps: int) -> None:
+    spec = gen.GraphSpec(kind=gen.KTG_ER, n=40000, draws=48_000_000, seed=7)
+    g = gen.Graph(spec)
+    with Context(0) as ctx:
+        dg = ctx.load_pairs(g.edges())
+        for _ in range(reps):
+            t = time.perf_counter()
+            sup = dg.tricount()
+            print(f"support of {dg.num_edges} edges: {1e3 * (time.perf_counter() - t):.1f} ms, "
+                  f"sum {int(sup.astype(np.uint64).sum())}", flush=True)
+        dg.free()
+
+
+def solve(spec: gen.GraphSpec, reps: int) -> None:
+    g = gen.Graph(spec)
+    data = g.tsv_bytes()
+    with Context(0) as ctx:
+        t = ctx.stage_tsv(data)
+        for _ in range(reps):
+            r = t.solve()
+            st = ctx.stats()
+            print(f"{r} in {st['ms_total']:.1f} ms device", flush=True)
+        t.free()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve"])
+    ap.add_argument("--reps", type=int, default=1)
+    a = ap.parse_args()
+    if a.case == "dense-support":
+        dense_support(a.reps)
+    elif a.case == "rmat21-solve":
+        solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps)
+    else:
+        solve(gen.rmat_s16_k30(), a.reps)
+
+
+if __name__ == "__main__":
+    main()
