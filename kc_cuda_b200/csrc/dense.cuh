@@ -2,49 +2,51 @@
 // 32-bit words), so |N(u) n N(v)| is a popcount of W word-ANDs.
 //
 // A warp takes 32 consecutive edges of a list.  Each lane fetches one edge's
-// ends, then the warp walks the 32 edges: row u is cached in registers (R
-// words per lane, W <= 32 R) and reused while consecutive edges share u (the
-// edge lists are sorted by u), row v streams from L2.  Lane j keeps the
-// count of the j-th edge, so results are written or pushed once per group.
+// ends, then the warp walks the 32 edges: row u is copied into the warp's
+// slice of shared memory (W words) and reused while consecutive edges share
+// u (the lists are tile-ordered by (u block, v block, u, v)), row v streams
+// from L2 with every lane on consecutive words.  Keeping row u in shared
+// memory rather than registers leaves the kernels at few registers, so many
+// warps hide the L2 latency.  Lane j keeps the count of the j-th edge, so
+// results are written or pushed once per group.
 #pragma once
 #include "kt_device.cuh"
 
 namespace kt {
 
-template <int R>
+// Shared memory a block of `threads` needs for rows of W words.
+inline size_t dense_smem_bytes(uint32_t W, unsigned threads) { return (size_t)(threads / 32) * W * 4; }
+
 __device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ bits, uint32_t W, uint32_t u,
-                                               uint32_t (&w)[R]) {
+                                               uint32_t* su) {
   const uint32_t* p = bits + (uint64_t)u * W;
-  const unsigned l = lane_id();
-#pragma unroll
-  for (int k = 0; k < R; ++k) {
-    const uint32_t idx = k * 32 + l;
-    w[k] = idx < W ? p[idx] : 0u;
-  }
+  for (uint32_t i = lane_id(); i < W; i += 32) su[i] = p[i];
+  __syncwarp();
 }
 
-template <int R>
+// popcount(row u & row v) over words [w0, w1); every lane returns the warp
+// total.
 __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ bits, uint32_t W,
-                                                   const uint32_t (&w)[R], uint32_t v) {
+                                                   const uint32_t* su, uint32_t v, uint32_t w0, uint32_t w1) {
   const uint32_t* p = bits + (uint64_t)v * W;
-  const unsigned l = lane_id();
   uint32_t s = 0;
-#pragma unroll
-  for (int k = 0; k < R; ++k) {
-    const uint32_t idx = k * 32 + l;
-    if (idx < W) s += __popc(w[k] & p[idx]);
+  uint32_t i = w0 + lane_id();
+  for (; i + 96 < w1; i += 128) {
+    const uint32_t a0 = p[i], a1 = p[i + 32], a2 = p[i + 64], a3 = p[i + 96];
+    s += __popc(su[i] & a0) + __popc(su[i + 32] & a1) + __popc(su[i + 64] & a2) + __popc(su[i + 96] & a3);
   }
+  for (; i < w1; i += 32) s += __popc(su[i] & p[i]);
   return warp_sum(s);
 }
 
 // One group of up to 32 list entries [base, min(base+32, cnt)).  Entries
 // whose state is not kAlive (when state != nullptr) are skipped.  On return
 // lane j holds (my_e, my_s) of the group's j-th entry, my_ok = counted.
-template <int R>
+// su is this warp's W-word slice of shared memory.
 __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                             const uint64_t* __restrict__ ends, const uint32_t* __restrict__ bits,
-                                            uint32_t W, const uint32_t* __restrict__ state, uint32_t& my_e,
-                                            uint32_t& my_s, bool& my_ok) {
+                                            uint32_t W, const uint32_t* __restrict__ state, uint32_t* su,
+                                            uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -62,31 +64,30 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
   my_ok = ok;
   my_s = 0;
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t w[R];
   uint32_t cu = 0xffffffffu;
   while (todo) {
     const int j = __ffs(todo) - 1;
     todo &= todo - 1;
     const uint32_t uj = __shfl_sync(kFull, u, j), vj = __shfl_sync(kFull, v, j);
     if (uj != cu) {
-      dense_load_row<R>(bits, W, uj, w);
+      __syncwarp();
+      dense_load_row(bits, W, uj, su);
       cu = uj;
     }
-    const uint32_t s = dense_and_popc<R>(bits, W, w, vj);
+    const uint32_t s = dense_and_popc(bits, W, su, vj, 0, W);
     if (l == (unsigned)j) my_s = s;
   }
+  __syncwarp();
 }
 
 // As dense_group, but an edge whose count can no longer reach `thr` is
-// abandoned: the row is ANDed in four segments, and after each one the count
-// so far plus the set bits left in row u bounds the result.  An abandoned
-// edge reports a count below thr (not its support).
-template <int R>
+// abandoned: the rows are ANDed in four segments, and after each one the
+// count so far plus the set bits left in row u bounds the result.  An
+// abandoned edge reports a count below thr (not its support).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends,
                                                    const uint32_t* __restrict__ bits, uint32_t W, uint32_t thr,
-                                                   uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
-  constexpr int Q = R / 4;
+                                                   uint32_t* su, uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -101,8 +102,12 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_e = e;
   my_ok = ok;
   my_s = 0;
+  // Segment bounds: four runs of whole 32-word strides.
+  const uint32_t strides = (W + 31) / 32;
+  uint32_t cut[5];
+#pragma unroll
+  for (int q = 0; q <= 4; ++q) cut[q] = min(W, ((strides * q) / 4) * 32);
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t w[R];
   uint32_t seg[4] = {0, 0, 0, 0};
   uint32_t cu = 0xffffffffu;
   while (todo) {
@@ -110,35 +115,26 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     todo &= todo - 1;
     const uint32_t uj = __shfl_sync(kFull, u, j), vj = __shfl_sync(kFull, v, j);
     if (uj != cu) {
-      dense_load_row<R>(bits, W, uj, w);
+      __syncwarp();
+      dense_load_row(bits, W, uj, su);
       cu = uj;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         uint32_t c = 0;
-#pragma unroll
-        for (int k = q * Q; k < (q + 1) * Q; ++k) c += __popc(w[k]);
+        for (uint32_t i = cut[q] + l; i < cut[q + 1]; i += 32) c += __popc(su[i]);
         seg[q] = warp_sum(c);
       }
     }
-    const uint32_t* p = bits + (uint64_t)vj * W;
     uint32_t found = 0, left = seg[0] + seg[1] + seg[2] + seg[3];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      uint32_t c = 0;
-#pragma unroll
-      for (int k = q * Q; k < (q + 1) * Q; ++k) {
-        const uint32_t wi = k * 32 + l;
-        if (wi < W) c += __popc(w[k] & p[wi]);
-      }
-      found += warp_sum(c);
+      found += dense_and_popc(bits, W, su, vj, cut[q], cut[q + 1]);
       left -= seg[q];
       if (found + left < thr) break;  // uniform: every lane holds the same sums
     }
     if (l == (unsigned)j) my_s = found;
   }
+  __syncwarp();
 }
-
-// Row-cache size (words per lane) for W words per row: 8, 16, 32 or 64.
-inline int dense_regs(uint32_t W) { return W <= 256 ? 8 : W <= 512 ? 16 : W <= 1024 ? 32 : 64; }
 
 }  // namespace kt

@@ -238,15 +238,14 @@ __device__ __forceinline__ void clear_deleted(const PeelArgs& A, uint32_t lo, ui
 // graph without this round's frontier; those below the threshold form the
 // next frontier.  Replaces per-triangle decrements when the frontier is a
 // large part of the graph.
-template <int R>
 __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uint32_t* next,
                                               unsigned long long* ncnt, uint64_t gwarp, uint64_t gwarps,
-                                              uint64_t& trec) {
+                                              uint64_t& trec, uint32_t* su) {
   const uint64_t groups = (A.na + 31) / 32;
   for (uint64_t g = gwarp; g < groups; g += gwarps) {
     uint32_t e, sc;
     bool ok;
-    dense_group<R>(A.alive, g * 32, A.na, A.ends, A.bits, A.W, A.state, e, sc, ok);
+    dense_group(A.alive, g * 32, A.na, A.ends, A.bits, A.W, A.state, su, e, sc, ok);
     trec += __popc(__ballot_sync(kFull, ok));
     bool want = false;
     if (ok) {
@@ -261,9 +260,11 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
   }
 }
 
-// One whole cascade in one cooperative launch.
-template <int R>
+// One whole cascade in one cooperative launch.  Dense mode uses W words of
+// shared memory per warp for the recount rounds.
 __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
+  extern __shared__ uint32_t dense_smem[];
+  uint32_t* su = dense_smem + warp_id() * A.W;
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   level_frontier(A, A.r0, gtid, gthreads);
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
         ok = false;
         break;
       }
-      recount_round<R>(A, r, nx, nc, gwarp, gwarps, trec);
+      recount_round(A, r, nx, nc, gwarp, gwarps, trec, su);
     } else {
       for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
     }
@@ -378,17 +379,10 @@ struct Peeler {
   uint64_t na = 0;
   uint32_t r = 1;  // next round number
   unsigned coop_grid = 0;
-  int regs = 8;
+  size_t smem = 0;
   PeelResult* res;
 
-  const void* kernel() const {
-    switch (regs) {
-      case 8: return (const void*)k_cascade<8>;
-      case 16: return (const void*)k_cascade<16>;
-      case 32: return (const void*)k_cascade<32>;
-      default: return (const void*)k_cascade<64>;
-    }
-  }
+  const void* kernel() const { return (const void*)k_cascade; }
 
   void init() {
     const uint64_t m = s->m;
@@ -413,11 +407,12 @@ struct Peeler {
                               c->stream));
     KT_LAUNCHED(c);
     na = m;
-    regs = dense_regs(s->W);
+    smem = dense_smem_bytes(s->W, kPeelThreads);
     coop_grid = 0;
     if (c->opt.persistent || s->W) {
+      KT_CUDA(cudaFuncSetAttribute(k_cascade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       int per_sm = 0;
-      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel(), kPeelThreads, 0));
+      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade, kPeelThreads, smem));
       coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
     }
   }
@@ -461,7 +456,7 @@ struct Peeler {
     scanned += na;
     if (coop_grid) {
       void* p[] = {&A};
-      KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, 0, c->stream));
+      KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, smem, c->stream));
       KT_LAUNCHED(c);
       rounds = read_word<unsigned long long>(c, A.cnt + 3);
     } else {

@@ -115,32 +115,21 @@ __global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const
   }
 }
 
-template <int R>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends,
-                                                       const uint32_t* __restrict__ bits, uint32_t W,
+                                                       const uint32_t* __restrict__ bits, uint32_t W, uint32_t cap,
                                                        uint32_t* __restrict__ sup) {
+  extern __shared__ uint32_t dense_smem[];
+  uint32_t* su = dense_smem + warp_id() * W;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t groups = (m + 31) / 32;
   for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
     uint32_t e, s;
     bool ok;
-    dense_group<R>(order, g * 32, m, ends, bits, W, nullptr, e, s, ok);
-    if (ok) sup[e] = s;
-  }
-}
-
-template <int R>
-__global__ void __launch_bounds__(256) k_dense_support_capped(uint64_t m, const uint32_t* __restrict__ order,
-                                                              const uint64_t* __restrict__ ends,
-                                                              const uint32_t* __restrict__ bits, uint32_t W,
-                                                              uint32_t thr, uint32_t* __restrict__ sup) {
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  const uint64_t groups = (m + 31) / 32;
-  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
-    uint32_t e, s;
-    bool ok;
-    dense_group_capped<R>(order, g * 32, m, ends, bits, W, thr, e, s, ok);
+    if (cap)
+      dense_group_capped(order, g * 32, m, ends, bits, W, cap, su, e, s, ok);
+    else
+      dense_group(order, g * 32, m, ends, bits, W, nullptr, su, e, s, ok);
     if (ok) sup[e] = s;
   }
 }
@@ -155,20 +144,14 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
   }
 }
 
-template <int R>
 void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
+  const size_t smem = dense_smem_bytes(s.W, 256);
+  KT_CUDA(cudaFuncSetAttribute(k_dense_support, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  if (cap) {
-    KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support_capped<R>, 256, 0));
-    const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-    k_dense_support_capped<R><<<grid, 256, 0, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           s.bits.as<uint32_t>(), s.W, cap, sup);
-  } else {
-    KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<R>, 256, 0));
-    const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-    k_dense_support<R><<<grid, 256, 0, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                    s.bits.as<uint32_t>(), s.W, sup);
-  }
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support, 256, smem));
+  const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
+  k_dense_support<<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+                                                  s.bits.as<uint32_t>(), s.W, cap, sup);
   KT_LAUNCHED(c);
 }
 
@@ -222,12 +205,7 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   cudaEvent_t e0;
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
-    switch (dense_regs(s.W)) {
-      case 8: launch_dense_support<8>(c, s, sup, cap); break;
-      case 16: launch_dense_support<16>(c, s, sup, cap); break;
-      case 32: launch_dense_support<32>(c, s, sup, cap); break;
-      default: launch_dense_support<64>(c, s, sup, cap); break;
-    }
+    launch_dense_support(c, s, sup, cap);
   } else if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
     const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
