@@ -25,17 +25,28 @@ __device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ bits
 }
 
 // popcount(row u & row v) over words [w0, w1); every lane returns the warp
-// total.
+// total.  Row v is read 16 strides at a time (16 loads in flight per lane,
+// L2-only caching: each row v is used once per edge).
 __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ bits, uint32_t W,
                                                    const uint32_t* su, uint32_t v, uint32_t w0, uint32_t w1) {
   const uint32_t* p = bits + (uint64_t)v * W;
   uint32_t s = 0;
   uint32_t i = w0 + lane_id();
-  for (; i + 96 < w1; i += 128) {
-    const uint32_t a0 = p[i], a1 = p[i + 32], a2 = p[i + 64], a3 = p[i + 96];
-    s += __popc(su[i] & a0) + __popc(su[i + 32] & a1) + __popc(su[i + 64] & a2) + __popc(su[i + 96] & a3);
+  for (; i + 15 * 32 < w1; i += 16 * 32) {
+    uint32_t a[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = __ldcg(p + i + 32 * k);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += __popc(su[i + 32 * k] & a[k]);
   }
-  for (; i < w1; i += 32) s += __popc(su[i] & p[i]);
+  for (; i + 3 * 32 < w1; i += 4 * 32) {
+    uint32_t a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __ldcg(p + i + 32 * k);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s += __popc(su[i + 32 * k] & a[k]);
+  }
+  for (; i < w1; i += 32) s += __popc(su[i] & __ldcg(p + i));
   return warp_sum(s);
 }
 
