@@ -92,13 +92,15 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 }
 
 // As dense_group, but an edge whose count can no longer reach `thr` is
-// abandoned: the rows are ANDed in four segments, and after each one the
-// count so far plus the set bits left in row u bounds the result.  An
-// abandoned edge reports a count below thr (not its support).
+// abandoned: the rows are ANDed in eight segments, highest vertex ids (the
+// highest degrees, where common neighbours concentrate) first, and after
+// each one the count so far plus the set bits left in row u bounds the
+// result.  An abandoned edge reports a count below thr (not its support).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends,
                                                    const uint32_t* __restrict__ bits, uint32_t W, uint32_t thr,
                                                    uint32_t* su, uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
+  constexpr int S = 8;
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -113,13 +115,14 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_e = e;
   my_ok = ok;
   my_s = 0;
-  // Segment bounds: four runs of whole 32-word strides.
+  // Segment bounds: S runs of whole 32-word strides.
   const uint32_t strides = (W + 31) / 32;
-  uint32_t cut[5];
+  uint32_t cut[S + 1];
 #pragma unroll
-  for (int q = 0; q <= 4; ++q) cut[q] = min(W, ((strides * q) / 4) * 32);
+  for (int q = 0; q <= S; ++q) cut[q] = min(W, ((strides * q) / S) * 32);
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t seg[4] = {0, 0, 0, 0};
+  uint32_t seg[S];
+  uint32_t total_u = 0;
   uint32_t cu = 0xffffffffu;
   while (todo) {
     const int j = __ffs(todo) - 1;
@@ -129,16 +132,18 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       __syncwarp();
       dense_load_row(bits, W, uj, su);
       cu = uj;
+      total_u = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < S; ++q) {
         uint32_t c = 0;
         for (uint32_t i = cut[q] + l; i < cut[q + 1]; i += 32) c += __popc(su[i]);
         seg[q] = warp_sum(c);
+        total_u += seg[q];
       }
     }
-    uint32_t found = 0, left = seg[0] + seg[1] + seg[2] + seg[3];
+    uint32_t found = 0, left = total_u;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = S - 1; q >= 0; --q) {
       found += dense_and_popc(bits, W, su, vj, cut[q], cut[q + 1]);
       left -= seg[q];
       if (found + left < thr) break;  // uniform: every lane holds the same sums

@@ -115,6 +115,7 @@ __global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const
   }
 }
 
+template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends,
                                                        const uint32_t* __restrict__ bits, uint32_t W, uint32_t cap,
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_
   for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
     uint32_t e, s;
     bool ok;
-    if (cap)
+    if (kCapped)
       dense_group_capped(order, g * 32, m, ends, bits, W, cap, su, e, s, ok);
     else
       dense_group(order, g * 32, m, ends, bits, W, nullptr, su, e, s, ok);
@@ -144,14 +145,15 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
   }
 }
 
+template <bool kCapped>
 void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   const size_t smem = dense_smem_bytes(s.W, 256);
-  KT_CUDA(cudaFuncSetAttribute(k_dense_support, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KT_CUDA(cudaFuncSetAttribute(k_dense_support<kCapped>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support, 256, smem));
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-  k_dense_support<<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                  s.bits.as<uint32_t>(), s.W, cap, sup);
+  k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+                                                           s.bits.as<uint32_t>(), s.W, cap, sup);
   KT_LAUNCHED(c);
 }
 
@@ -205,7 +207,10 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   cudaEvent_t e0;
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
-    launch_dense_support(c, s, sup, cap);
+    if (cap)
+      launch_dense_support<true>(c, s, sup, cap);
+    else
+      launch_dense_support<false>(c, s, sup, 0);
   } else if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
     const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
