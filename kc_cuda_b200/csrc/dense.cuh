@@ -92,15 +92,13 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 }
 
 // As dense_group, but an edge whose count can no longer reach `thr` is
-// abandoned: the rows are ANDed in eight segments, highest vertex ids (the
-// highest degrees, where common neighbours concentrate) first, and after
-// each one the count so far plus the set bits left in row u bounds the
-// result.  An abandoned edge reports a count below thr (not its support).
+// abandoned: the rows are ANDed in four segments, and after each one the
+// count so far plus the set bits left in row u bounds the result.  An
+// abandoned edge reports a count below thr (not its support).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends,
                                                    const uint32_t* __restrict__ bits, uint32_t W, uint32_t thr,
                                                    uint32_t* su, uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
-  constexpr int S = 8;
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -115,14 +113,12 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_e = e;
   my_ok = ok;
   my_s = 0;
-  // Segment bounds: S runs of whole 32-word strides.
+  // Segment bounds: four runs of whole 32-word strides.
   const uint32_t strides = (W + 31) / 32;
-  uint32_t cut[S + 1];
-#pragma unroll
-  for (int q = 0; q <= S; ++q) cut[q] = min(W, ((strides * q) / S) * 32);
+  const uint32_t c1 = min(W, (strides / 4) * 32), c2 = min(W, (strides / 2) * 32),
+                 c3 = min(W, ((3 * strides) / 4) * 32);
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t seg[S];
-  uint32_t total_u = 0;
+  uint32_t s1 = 0, s2 = 0, s3 = 0;  // set bits of row u in segments 2..4
   uint32_t cu = 0xffffffffu;
   while (todo) {
     const int j = __ffs(todo) - 1;
@@ -132,21 +128,22 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       __syncwarp();
       dense_load_row(bits, W, uj, su);
       cu = uj;
-      total_u = 0;
-#pragma unroll
-      for (int q = 0; q < S; ++q) {
-        uint32_t c = 0;
-        for (uint32_t i = cut[q] + l; i < cut[q + 1]; i += 32) c += __popc(su[i]);
-        seg[q] = warp_sum(c);
-        total_u += seg[q];
+      uint32_t b = 0, c = 0, d = 0;
+      for (uint32_t i = c1 + l; i < W; i += 32) {
+        const uint32_t pc = __popc(su[i]);
+        if (i < c2) b += pc; else if (i < c3) c += pc; else d += pc;
       }
+      s1 = warp_sum(b);
+      s2 = warp_sum(c);
+      s3 = warp_sum(d);
     }
-    uint32_t found = 0, left = total_u;
-#pragma unroll
-    for (int q = S - 1; q >= 0; --q) {
-      found += dense_and_popc(bits, W, su, vj, cut[q], cut[q + 1]);
-      left -= seg[q];
-      if (found + left < thr) break;  // uniform: every lane holds the same sums
+    uint32_t found = dense_and_popc(bits, W, su, vj, 0, c1);
+    if (found + s1 + s2 + s3 >= thr) {
+      found += dense_and_popc(bits, W, su, vj, c1, c2);
+      if (found + s2 + s3 >= thr) {
+        found += dense_and_popc(bits, W, su, vj, c2, c3);
+        if (found + s3 >= thr) found += dense_and_popc(bits, W, su, vj, c3, W);
+      }
     }
     if (l == (unsigned)j) my_s = found;
   }
