@@ -95,6 +95,30 @@ kt_status kt_tsv_stage(kt_ctx* ctx, const char* bytes, uint64_t len, kt_tsv** ou
 kt_status kt_solve_staged(kt_ctx* ctx, const kt_tsv* tsv, uint32_t* kmax, uint64_t* edges);
 void kt_tsv_free(kt_ctx* ctx, kt_tsv* tsv);
 
+/* ----------------------------------------------------------------- batch */
+
+/* Many graphs solved together (no counterpart in the reference, which
+ * solves one graph per process).  Graphs are packed into waves that fit the
+ * context's HBM budget; each wave is one disjoint union sent once through the
+ * CSR build, the core decomposition, and a shared support count and peel in
+ * which every graph keeps its own answer. */
+typedef struct kt_batch kt_batch;
+kt_status kt_batch_create(kt_ctx* ctx, kt_batch** out);
+/* Adds a graph given as records x << 32 | y (copied); *graph_id = its index. */
+kt_status kt_batch_add_pairs(kt_batch* b, const uint64_t* xy, uint64_t count, uint32_t* graph_id);
+/* Adds graphs first_index .. first_index+count-1 of the batched mix
+ * (generated on the device at run time from their seeds). */
+kt_status kt_batch_add_mix(kt_batch* b, uint64_t first_index, uint64_t count, uint64_t base_seed);
+kt_status kt_batch_size(const kt_batch* b, uint64_t* graphs, uint64_t* edge_records);
+/* Solves every graph of the batch; ms_total / batch_waves in kt_get_stats. */
+kt_status kt_batch_run(kt_batch* b);
+/* kmax and kmax-truss edge count of every graph, in graph-id order. */
+kt_status kt_batch_results(const kt_batch* b, uint32_t* kmax, uint64_t* edges);
+void kt_batch_free(kt_batch* b);
+/* Graph `index` of the batched mix, generated on the device (the per-graph
+ * path's input, identical to the batch's). */
+kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_graph** out);
+
 /* ------------------------------------------------------- stage outputs */
 
 /* Members of the k-core (member_out[v] = 1 if v is in it) and, in cmax_out,
@@ -141,6 +165,7 @@ typedef struct kt_stats {
   uint64_t device_bytes_peak;
   uint64_t h2d_bytes, d2h_bytes;            /* host<->device traffic since kt_stats_reset */
   uint64_t peel_decrements;                 /* support decrements of the last solve */
+  uint32_t batch_waves, batch_graphs;       /* last kt_batch_run */
 } kt_stats;
 kt_status kt_get_stats(const kt_ctx* ctx, kt_stats* out);
 kt_status kt_stats_reset(kt_ctx* ctx);

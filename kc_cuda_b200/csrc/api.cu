@@ -13,6 +13,7 @@
 #include <new>
 
 #include "kt.h"
+#include "batch.h"
 #include "solve.h"
 
 struct kt_ctx {
@@ -24,6 +25,10 @@ struct kt_graph {
 struct kt_tsv {
   kt::DBuf bytes;
   uint64_t len = 0;
+};
+struct kt_batch {
+  kt_ctx* ctx = nullptr;
+  std::vector<kt::BatchItem> items;
 };
 
 namespace kt {
@@ -78,7 +83,7 @@ __global__ void k_canon_pairs(uint64_t* __restrict__ xy, uint64_t n, unsigned in
 
 }  // namespace
 
-static float event_ms(cudaEvent_t a, cudaEvent_t b) {
+float event_ms(cudaEvent_t a, cudaEvent_t b) {
   KT_CUDA(cudaEventSynchronize(b));
   float ms = 0;
   KT_CUDA(cudaEventElapsedTime(&ms, a, b));
@@ -483,6 +488,104 @@ void kt_tsv_free(kt_ctx* h, kt_tsv* t) {
   } else {
     delete t;
   }
+}
+
+kt_status kt_batch_create(kt_ctx* h, kt_batch** out) {
+  if (!h || !out) return KT_ERR_INVALID;
+  *out = new (std::nothrow) kt_batch;
+  if (!*out) return KT_ERR_NOMEM;
+  (*out)->ctx = h;
+  return KT_OK;
+}
+
+kt_status kt_batch_add_pairs(kt_batch* b, const uint64_t* xy, uint64_t count, uint32_t* graph_id) {
+  if (!b || (!xy && count)) return KT_ERR_INVALID;
+  try {
+    b->items.emplace_back();
+    b->items.back().from_pairs(xy, count);
+  } catch (const std::bad_alloc&) {
+    return KT_ERR_NOMEM;
+  }
+  if (graph_id) *graph_id = (uint32_t)(b->items.size() - 1);
+  return KT_OK;
+}
+
+kt_status kt_batch_add_mix(kt_batch* b, uint64_t first, uint64_t count, uint64_t base_seed) {
+  if (!b) return KT_ERR_INVALID;
+  try {
+    for (uint64_t i = 0; i < count; ++i) {
+      b->items.emplace_back();
+      b->items.back().from_mix(first + i, base_seed);
+    }
+  } catch (const std::bad_alloc&) {
+    return KT_ERR_NOMEM;
+  }
+  return KT_OK;
+}
+
+kt_status kt_batch_size(const kt_batch* b, uint64_t* graphs, uint64_t* records) {
+  if (!b) return KT_ERR_INVALID;
+  if (graphs) *graphs = b->items.size();
+  if (records) {
+    uint64_t s = 0;
+    for (const auto& it : b->items) s += it.nkeys;
+    *records = s;
+  }
+  return KT_OK;
+}
+
+kt_status kt_batch_run(kt_batch* b) {
+  if (!b) return KT_ERR_INVALID;
+  kt_ctx* h = b->ctx;
+  KT_API_BEGIN(h)
+  kt::Ctx* c = &h->c;
+  kt::reset_words(c);
+  kt::begin_solve_stats(c);
+  KT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  kt::BatchRun run;
+  {
+    struct Resolve {
+      kt::Ctx* c;
+      ~Resolve() {
+        try {
+          c->timer.resolve();
+        } catch (...) {
+        }
+      }
+    } resolve{c};
+    kt::run_batch(c, b->items, run);
+  }
+  KT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  c->stats.ms_total = kt::event_ms(c->ev[0], c->ev[1]);
+  c->stats.batch_waves = run.waves;
+  c->stats.batch_graphs = (uint32_t)b->items.size();
+  KT_API_END(h)
+}
+
+kt_status kt_batch_results(const kt_batch* b, uint32_t* kmax, uint64_t* edges) {
+  if (!b) return KT_ERR_INVALID;
+  for (size_t i = 0; i < b->items.size(); ++i) {
+    if (kmax) kmax[i] = b->items[i].kmax;
+    if (edges) edges[i] = b->items[i].count;
+  }
+  return KT_OK;
+}
+
+void kt_batch_free(kt_batch* b) { delete b; }
+
+kt_status kt_load_mix_graph(kt_ctx* h, uint64_t index, uint64_t base_seed, kt_graph** out) {
+  if (!out) return KT_ERR_INVALID;
+  *out = nullptr;
+  KT_API_BEGIN(h)
+  kt_graph* g = new kt_graph;
+  try {
+    kt::load_mix_graph(&h->c, index, base_seed, g->g);
+  } catch (...) {
+    delete g;
+    throw;
+  }
+  *out = g;
+  KT_API_END(h)
 }
 
 kt_status kt_kcore(kt_ctx* h, kt_graph* g, uint32_t k, uint8_t* member, uint32_t* cmax) {

@@ -1,0 +1,377 @@
+// Batched solving of many graphs (thousands, of uneven sizes) per launch
+// sequence, and the device generator of the batched mix.
+//
+// A batch is cut into waves that fit the context's HBM budget.  A wave is
+// one disjoint union: every graph's vertex ids are offset by the vertex
+// count of the graphs before it (vbase), all their edges go through ONE
+// sort/dedup/CSR build, ONE core decomposition, and -- on the union of the
+// graphs' cores, grouped by graph -- ONE support count and ONE peel whose
+// levels are shared by all graphs while every graph keeps its own record
+// (per-graph alive edges and minimum support after each level).  Triangles
+// never cross graphs, so each graph's answer is exactly its own.
+//
+// Per graph the two phases of the single-graph driver are kept: the truss of
+// its maximum core gives L (and the answer when L = cmax + 1); otherwise its
+// (L-1)-core joins the second union.
+//
+// Graphs of the batched mix (ktg_mix_spec: R-MAT or Erdos-Renyi, one planted
+// clique) are generated on the device from their seeds straight into the
+// wave's key buffer, with the host generator's integer conventions
+// (ktgen_core.h), so a device-generated graph equals ktg_make's.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "batch.h"
+#include "compact.cuh"
+#include "ktgen.h"
+#include "ktgen_core.h"
+#include "solve.h"
+
+namespace kt {
+namespace {
+
+// Device specs of the generated graphs of a wave.
+struct GenSpec {
+  uint64_t seed;
+  uint64_t n;
+  uint64_t draws;
+  uint64_t gen_off;  // first draw index of this graph in the wave's draw space
+  uint64_t key_off;  // first key slot
+  uint64_t vbase;    // first union vertex id
+  uint32_t kind;
+  uint32_t scale;
+};
+
+__global__ void k_gen_draws(const GenSpec* __restrict__ specs, uint32_t ns, uint64_t total, ktg_rmat_t thr,
+                            uint64_t* __restrict__ keys) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ns;  // last spec with gen_off <= i
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (specs[mid].gen_off <= i)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const GenSpec& s = specs[lo];
+    const uint64_t j = i - s.gen_off;
+    const uint64_t xy = s.kind == KTG_RMAT ? ktg_rmat_draw(s.seed, thr, s.scale, j) : ktg_er_draw(s.seed, s.n, j);
+    const uint64_t k = ktg_canon(xy, s.n);
+    keys[s.key_off + j] = k == ~0ULL ? ~0ULL : (((k >> 32) + s.vbase) << 32) | ((uint32_t)k + s.vbase);
+  }
+}
+
+// Host records x << 32 | y -> canonical union keys (self-loops -> ~0).
+__global__ void k_canon_offset(uint64_t* __restrict__ keys, uint64_t n, uint64_t vbase) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const uint64_t x = k >> 32, y = (uint32_t)k;
+    keys[i] = x == y ? ~0ULL : (x < y ? ((x + vbase) << 32) | (y + vbase) : ((y + vbase) << 32) | (x + vbase));
+  }
+}
+
+__global__ void k_group_of(const uint64_t* __restrict__ vbase, uint32_t ng, uint64_t n, uint32_t* __restrict__ gid) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ng;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (vbase[mid] <= v)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    gid[v] = lo;
+  }
+}
+
+__global__ void k_group_max(const uint32_t* __restrict__ val, const uint32_t* __restrict__ gid, uint64_t n,
+                            uint32_t* __restrict__ out) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < ((n + 31) & ~31ULL);
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ok = v < n;
+    const uint32_t g = ok ? gid[v] : 0xffffffffu;
+    const uint32_t x = ok ? val[v] : 0u;
+    const unsigned peers = __match_any_sync(kFull, g);
+    const uint32_t mx = __reduce_max_sync(peers, x);
+    if (ok && lane_id() == (unsigned)(__ffs(peers) - 1)) atomicMax(&out[g], mx);
+  }
+}
+
+// Vertices of graph g with core >= need[g] (need 0 = graph not taken).
+struct CoreAtLeast {
+  const uint32_t* core;
+  const uint32_t* gid;
+  const uint32_t* need;
+  __device__ bool keep(uint64_t v) const {
+    const uint32_t k = need[gid[v]];
+    return k && core[v] >= k;
+  }
+  __device__ uint32_t value(uint64_t v) const { return (uint32_t)v; }
+};
+
+__global__ void k_mark(const uint32_t* __restrict__ list, uint64_t na, uint32_t* __restrict__ rem) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x)
+    rem[list[i]] = kAlive;
+}
+
+// deg[v] = alive neighbours, warp per alive vertex.
+__global__ void k_alive_degree(const uint32_t* __restrict__ list, uint64_t na, const uint64_t* __restrict__ off,
+                               const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
+                               uint32_t* __restrict__ deg) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); i < na; i += warps) {
+    const uint32_t v = list[i];
+    uint32_t c = 0;
+    for (uint64_t j = off[v] + lane_id(); j < off[v + 1]; j += 32) c += rem[adj[j]] == kAlive;
+    c = warp_sum(c);
+    if (lane_id() == 0) deg[v] = c;
+  }
+}
+
+// Clique keys (local canonical u << 32 | v) of a planted clique.
+void clique_keys(const std::vector<uint32_t>& vs, std::vector<uint64_t>& out) {
+  for (size_t i = 0; i < vs.size(); ++i)
+    for (size_t j = i + 1; j < vs.size(); ++j) {
+      const uint64_t a = vs[i], b = vs[j];
+      out.push_back(a < b ? (a << 32 | b) : (b << 32 | a));
+    }
+}
+
+}  // namespace
+
+void BatchItem::from_mix(uint64_t index, uint64_t base_seed) {
+  generated = true;
+  ktg_spec s;
+  ktg_mix_spec(index, base_seed, &s);
+  kind = s.kind;
+  scale = s.scale;
+  n = s.n;
+  draws = s.draws;
+  seed = s.seed;
+  extra.clear();
+  for (uint32_t c = 0; c < s.n_cliques; ++c) {
+    std::vector<uint32_t> vs(s.clique_sizes[c]);
+    ktg_sample_vertices(s.seed, KTG_STREAM_CLIQUE + c, n, s.clique_sizes[c], vs.data());
+    clique_keys(vs, extra);
+  }
+  nkeys = draws + extra.size();
+}
+
+void BatchItem::from_pairs(const uint64_t* xy, uint64_t count) {
+  generated = false;
+  extra.assign(xy, xy + count);
+  uint64_t mx = 0;
+  bool any = false;
+  for (uint64_t i = 0; i < count; ++i) {
+    mx = std::max<uint64_t>(mx, std::max<uint64_t>(xy[i] >> 32, (uint32_t)xy[i]));
+    any = true;
+  }
+  n = any ? mx + 1 : 0;
+  draws = 0;
+  nkeys = count;
+}
+
+// Keys of one wave (union ids) into `keys`; returns the union vertex count.
+static uint64_t wave_keys(Ctx* c, const std::vector<BatchItem*>& items, DBuf& keys, uint64_t& nkeys,
+                          std::vector<uint64_t>& vbase) {
+  const uint32_t G = (uint32_t)items.size();
+  vbase.assign(G + 1, 0);
+  std::vector<uint64_t> key_off(G + 1, 0);
+  for (uint32_t g = 0; g < G; ++g) {
+    vbase[g + 1] = vbase[g] + items[g]->n;
+    key_off[g + 1] = key_off[g] + items[g]->nkeys;
+  }
+  nkeys = key_off[G];
+  keys.alloc(c, (nkeys ? nkeys : 1) * sizeof(uint64_t));
+  std::vector<GenSpec> specs;
+  uint64_t gen_total = 0;
+  std::vector<uint64_t> extra_all;  // clique keys, already in union ids
+  for (uint32_t g = 0; g < G; ++g) {
+    const BatchItem& it = *items[g];
+    if (it.generated) {
+      GenSpec s;
+      s.seed = it.seed;
+      s.n = it.n;
+      s.draws = it.draws;
+      s.gen_off = gen_total;
+      s.key_off = key_off[g];
+      s.vbase = vbase[g];
+      s.kind = it.kind;
+      s.scale = it.scale;
+      specs.push_back(s);
+      gen_total += it.draws;
+    }
+  }
+  if (!specs.empty() && gen_total) {
+    DBuf dspecs(c, specs.size() * sizeof(GenSpec));
+    copy_h2d(c, dspecs.get(), specs.data(), specs.size() * sizeof(GenSpec));
+    const ktg_rmat_t thr = ktg_rmat_thresholds(570000, 190000, 190000);
+    k_gen_draws<<<grid_for(gen_total, 256, c->num_sms * 32), 256, 0, c->stream>>>(
+        dspecs.as<GenSpec>(), (uint32_t)specs.size(), gen_total, thr, keys.as<uint64_t>());
+    KT_LAUNCHED(c);
+    sync(c);
+  }
+  // Clique keys of generated graphs and records of host graphs.
+  for (uint32_t g = 0; g < G; ++g) {
+    const BatchItem& it = *items[g];
+    if (it.extra.empty()) continue;
+    uint64_t* dst = keys.as<uint64_t>() + key_off[g] + it.draws;
+    if (it.generated) {
+      std::vector<uint64_t> k(it.extra.size());
+      for (size_t i = 0; i < k.size(); ++i)
+        k[i] = (((it.extra[i] >> 32) + vbase[g]) << 32) | ((uint32_t)it.extra[i] + vbase[g]);
+      copy_h2d(c, dst, k.data(), k.size() * sizeof(uint64_t));
+      sync(c);
+    } else {
+      copy_h2d(c, dst, it.extra.data(), it.extra.size() * sizeof(uint64_t));
+      k_canon_offset<<<grid_for(it.extra.size(), 256, c->num_sms * 16), 256, 0, c->stream>>>(dst, it.extra.size(),
+                                                                                             vbase[g]);
+      KT_LAUNCHED(c);
+    }
+  }
+  return vbase[G];
+}
+
+// One union stage: the subgraph of vertices whose core reaches need[graph],
+// its support and its tracked peel; kmax/count receive the per-graph records.
+static void union_truss(Ctx* c, const Graph& U, const uint32_t* dcore, const uint32_t* dgid, uint32_t G,
+                        const std::vector<uint32_t>& need, std::vector<uint32_t>& kmax, std::vector<uint64_t>& count,
+                        kt_stats& st) {
+  DBuf dneed(c, G * sizeof(uint32_t));
+  copy_h2d(c, dneed.get(), need.data(), G * sizeof(uint32_t));
+  DBuf list(c, (U.n ? U.n : 1) * sizeof(uint32_t));
+  const uint64_t na = compact(c, U.n, CoreAtLeast{dcore, dgid, dneed.as<uint32_t>()}, list.as<uint32_t>());
+  kmax.assign(G, 0);
+  count.assign(G, 0);
+  if (na == 0) return;
+  DBuf rem(c, U.n * sizeof(uint32_t)), deg(c, U.n * sizeof(uint32_t));
+  zero(c, rem.get(), rem.bytes());
+  k_mark<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(list.as<uint32_t>(), na, rem.as<uint32_t>());
+  KT_LAUNCHED(c);
+  k_alive_degree<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      list.as<uint32_t>(), na, U.off.as<uint64_t>(), U.adj.as<uint32_t>(), rem.as<uint32_t>(), deg.as<uint32_t>());
+  KT_LAUNCHED(c);
+  Sub s;
+  build_sub_grouped(c, U, list.as<uint32_t>(), na, deg.as<uint32_t>(), rem.as<uint32_t>(), dgid, G, s);
+  list.release();
+  rem.release();
+  deg.release();
+  st.core_vertices += s.n;
+  st.core_edges += s.m;
+  if (s.m == 0) return;
+  DBuf sup(c, s.m * sizeof(uint32_t));
+  edge_support(c, s, sup.as<uint32_t>());
+  DBuf dk(c, G * sizeof(uint32_t)), dc(c, G * sizeof(uint64_t));
+  zero(c, dk.get(), dk.bytes());
+  zero(c, dc.get(), dc.bytes());
+  GraphTrack tr{s.vgid.as<uint32_t>(), G, dk.as<uint32_t>(), dc.as<uint64_t>()};
+  const PeelResult pr = truss_peel(c, s, sup.as<uint32_t>(), 3, 0, nullptr, 0, &tr);
+  st.levels += pr.levels;
+  st.rounds += (uint32_t)pr.rounds;
+  copy_d2h(c, kmax.data(), dk.get(), G * sizeof(uint32_t));
+  copy_d2h(c, count.data(), dc.get(), G * sizeof(uint64_t));
+}
+
+void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
+  const uint32_t G = (uint32_t)items.size();
+  kt_stats& st = c->stats;
+  DBuf keys;
+  uint64_t nkeys = 0;
+  std::vector<uint64_t> vbase;
+  const uint64_t nv = wave_keys(c, items, keys, nkeys, vbase);
+  Graph U;
+  build_graph(c, keys.as<uint64_t>(), nkeys, nv, U);
+  keys.release();
+  // Core numbers of the union and each graph's maximum core.
+  DBuf dcore(c, (nv ? nv : 1) * sizeof(uint32_t));
+  {
+    KCore kc;
+    kc.init(c, U);
+    kc.core_numbers(c, dcore.as<uint32_t>());
+  }
+  DBuf dvb(c, (G + 1) * sizeof(uint64_t)), dgid(c, (nv ? nv : 1) * sizeof(uint32_t)), dcm(c, G * sizeof(uint32_t));
+  copy_h2d(c, dvb.get(), vbase.data(), (G + 1) * sizeof(uint64_t));
+  zero(c, dcm.get(), dcm.bytes());
+  if (nv) {
+    k_group_of<<<grid_for(nv, 256, c->num_sms * 16), 256, 0, c->stream>>>(dvb.as<uint64_t>(), G, nv,
+                                                                            dgid.as<uint32_t>());
+    KT_LAUNCHED(c);
+    k_group_max<<<grid_for(nv, 256, c->num_sms * 16), 256, 0, c->stream>>>(dcore.as<uint32_t>(), dgid.as<uint32_t>(),
+                                                                             nv, dcm.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
+  std::vector<uint32_t> cmax(G);
+  copy_d2h(c, cmax.data(), dcm.get(), G * sizeof(uint32_t));
+  // Phase 1: the maximum core of every graph that can hold a triangle.
+  std::vector<uint32_t> need(G, 0);
+  for (uint32_t g = 0; g < G; ++g) need[g] = cmax[g] >= 2 ? cmax[g] : 0;
+  std::vector<uint32_t> k1;
+  std::vector<uint64_t> c1;
+  union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, k1, c1, st);
+  // Phase 2: the (L-1)-core of every graph whose bound is not met.
+  bool any = false;
+  for (uint32_t g = 0; g < G; ++g) {
+    items[g]->kmax = 0;
+    items[g]->count = 0;
+    need[g] = 0;
+    if (cmax[g] < 2) continue;
+    const uint32_t L = k1[g] >= 3 ? k1[g] : 0;
+    if (L && L == cmax[g] + 1) {
+      items[g]->kmax = L;
+      items[g]->count = c1[g];
+      continue;
+    }
+    need[g] = L ? L - 1 : 2;
+    any = true;
+  }
+  if (any) {
+    std::vector<uint32_t> k2;
+    std::vector<uint64_t> c2;
+    union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, k2, c2, st);
+    for (uint32_t g = 0; g < G; ++g) {
+      if (!need[g]) continue;
+      items[g]->kmax = k2[g] >= 3 ? k2[g] : 0;
+      items[g]->count = k2[g] >= 3 ? c2[g] : 0;
+    }
+  }
+}
+
+void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
+  // Waves: consecutive graphs while the estimated footprint fits half the
+  // free budget (keys, sort buffers, CSR, k-core state ~ 48 B per key and
+  // 40 B per vertex), the union stays below 2^28 vertices and 65536 graphs.
+  const uint64_t budget = (c->budget > c->in_use ? c->budget - c->in_use : 0) / 2;
+  size_t i = 0;
+  out.waves = 0;
+  while (i < items.size()) {
+    std::vector<BatchItem*> wave;
+    uint64_t bytes = 0, verts = 0;
+    while (i < items.size()) {
+      const BatchItem& it = items[i];
+      const uint64_t b = 48 * it.nkeys + 40 * it.n;
+      if (!wave.empty() && (bytes + b > budget || verts + it.n >= (1ull << 28) || wave.size() >= 65535)) break;
+      if (it.n >= (1ull << 28)) throw Error(KT_ERR_LIMIT, "batch: a graph with 2^28 or more vertex ids");
+      wave.push_back(&items[i]);
+      bytes += b;
+      verts += it.n;
+      ++i;
+    }
+    solve_wave(c, wave);
+    ++out.waves;
+  }
+}
+
+void load_mix_graph(Ctx* c, uint64_t index, uint64_t base_seed, Graph& g) {
+  BatchItem it;
+  it.from_mix(index, base_seed);
+  std::vector<BatchItem*> one{&it};
+  DBuf keys;
+  uint64_t nkeys = 0;
+  std::vector<uint64_t> vbase;
+  const uint64_t nv = wave_keys(c, one, keys, nkeys, vbase);
+  build_graph(c, keys.as<uint64_t>(), nkeys, nv, g);
+}
+
+}  // namespace kt

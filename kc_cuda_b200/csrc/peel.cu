@@ -351,6 +351,42 @@ __global__ void k_alive_min(const uint32_t* __restrict__ alive, uint64_t na, con
   }
 }
 
+// Per-graph alive edges and minimum support after a level (batched unions).
+__global__ void k_track(const uint32_t* __restrict__ alive, uint64_t na, const uint64_t* __restrict__ ends,
+                        const uint32_t* __restrict__ sup, const uint32_t* __restrict__ vgid,
+                        unsigned long long* __restrict__ gcnt, uint32_t* __restrict__ gmin) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((na + 31) & ~31ULL);
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool valid = i < na;
+    uint32_t g = 0xffffffffu, sv = 0xffffffffu;
+    if (valid) {
+      const uint32_t e = alive[i];
+      g = vgid[(uint32_t)(ends[e] >> 32)];
+      sv = sup[e];
+    }
+    // Graphs are contiguous in the edge order: aggregate equal graphs.
+    const unsigned peers = __match_any_sync(kFull, g);
+    const unsigned leader = __ffs(peers) - 1;
+    const uint32_t mn = __reduce_min_sync(peers, sv);
+    if (valid && lane_id() == leader) {
+      atomicAdd(&gcnt[g], (unsigned long long)__popc(peers));
+      atomicMin(&gmin[g], mn);
+    }
+  }
+}
+
+__global__ void k_track_record(uint32_t ngroups, unsigned long long* __restrict__ gcnt, uint32_t* __restrict__ gmin,
+                               uint32_t* __restrict__ kmax, uint64_t* __restrict__ count) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    if (gcnt[g]) {
+      kmax[g] = gmin[g] + 2;
+      count[g] = gcnt[g];
+    }
+    gcnt[g] = 0;
+    gmin[g] = 0xffffffffu;
+  }
+}
+
 struct StillAlive {
   const uint32_t* list;
   const uint32_t* state;
@@ -493,12 +529,34 @@ struct Peeler {
     c->stats.peel_decrements += h[1];
   }
 
+  // Batched unions: per-graph records after a level.
+  const GraphTrack* track = nullptr;
+  DBuf tcnt, tmin;
+  void record_groups() {
+    if (!track || track->ngroups == 0) return;
+    if (!tcnt.get()) {
+      tcnt = DBuf(c, (uint64_t)track->ngroups * 8);
+      tmin = DBuf(c, (uint64_t)track->ngroups * 4);
+      zero(c, tcnt.get(), tcnt.bytes());
+      KT_CUDA(cudaMemsetAsync(tmin.get(), 0xff, tmin.bytes(), c->stream));
+    }
+    if (na) {
+      k_track<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+          alive[ai].as<uint32_t>(), na, s->ends.as<uint64_t>(), sup, track->vgid, tcnt.as<unsigned long long>(),
+          tmin.as<uint32_t>());
+      KT_LAUNCHED(c);
+    }
+    k_track_record<<<grid_for(track->ngroups, 256, c->num_sms * 4), 256, 0, c->stream>>>(
+        track->ngroups, tcnt.as<unsigned long long>(), tmin.as<uint32_t>(), track->kmax, track->count);
+    KT_LAUNCHED(c);
+  }
+
   // Replaces the working graph by its alive part (renumbered, with its own
   // bitsets and exact supports) once most edges are gone; the alive edges
   // form a truss, so their supports in the new graph equal their current
   // ones.  Returns whether it compacted.
   bool compact_graph(std::unique_ptr<Sub>& own, DBuf& own_sup) {
-    if (truss || na == 0 || na * 4 > s->m || s->m < (1u << 20)) return false;
+    if (truss || track || na == 0 || na * 4 > s->m || s->m < (1u << 20)) return false;
     account();
     zero(c, acct.get(), acct.bytes());
     scanned = 0;
@@ -542,7 +600,7 @@ void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub
 }
 
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
-                      uint32_t guess) {
+                      uint32_t guess, const GraphTrack* track) {
   PeelResult res;
   if (s.m == 0) return res;
   if (t0 < 3) t0 = 3;
@@ -550,8 +608,14 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
   DBuf own_sup;
   Peeler P{c, &s, sup, truss};
   P.res = &res;
+  P.track = track;
   P.init();
   uint32_t t = t0;
+  if (track) {
+    // Batched: every graph is tracked, so no early stop and no jump.
+    stop_count = 0;
+    guess = 0;
+  }
   // Jump phase: try `guess` (> t0) from a snapshot; halve toward t0 on failure.
   if (!truss && guess > t0) {
     DBuf snap_sup(c, s.m * sizeof(uint32_t)), snap_state(c, s.m * sizeof(uint32_t));
@@ -597,6 +661,7 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
   bool first = true;
   while (true) {
     const uint64_t left = P.cascade(t);
+    P.record_groups();
     if (left == 0) break;
     if (first && stop_count && left == stop_count) {
       res.kmax = t;

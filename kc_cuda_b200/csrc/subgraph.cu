@@ -9,6 +9,9 @@
 // 2*ceil(log2 n') bits gives the sorted rows; edge ids follow from the
 // per-row start of the upper part (neighbours > row), found by binary
 // search, and an exclusive scan of the upper-part sizes.
+#include <algorithm>
+#include <vector>
+
 #include "compact.cuh"
 #include "subgraph.h"
 
@@ -22,11 +25,31 @@ int bits_for(uint64_t n) {
 }
 
 __global__ void k_order_keys(const uint32_t* __restrict__ alive, uint64_t na, const uint32_t* __restrict__ deg,
-                             uint64_t* __restrict__ keys) {
+                             const uint32_t* __restrict__ group_of, uint64_t* __restrict__ keys) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t v = alive[i];
-    keys[i] = ((uint64_t)deg[v] << 32) | v;
+    if (group_of)  // graph (16 bits) | degree (20 bits, saturated) | id (28 bits)
+      keys[i] = ((uint64_t)group_of[v] << 48) | ((uint64_t)min(deg[v], 0xfffffu) << 28) | v;
+    else
+      keys[i] = ((uint64_t)deg[v] << 32) | v;
   }
+}
+
+__global__ void k_group_meta(const uint32_t* __restrict__ orig, uint64_t na, const uint32_t* __restrict__ group_of,
+                             uint32_t* __restrict__ vgid, uint32_t* __restrict__ gstart,
+                             uint32_t* __restrict__ gsize) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = group_of[orig[i]];
+    vgid[i] = g;
+    if (i == 0 || group_of[orig[i - 1]] != g) gstart[g] = (uint32_t)i;
+    atomicAdd(&gsize[g], 1u);
+  }
+}
+
+__global__ void k_group_base(const uint32_t* __restrict__ vgid, uint64_t na, const uint32_t* __restrict__ gstart,
+                             uint32_t* __restrict__ vbase) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x)
+    vbase[i] = gstart[vgid[i]];
 }
 
 __global__ void k_order_apply(const uint64_t* __restrict__ keys, uint64_t na, uint32_t* __restrict__ orig,
@@ -132,7 +155,8 @@ __global__ void k_map_ids(uint32_t* __restrict__ ids, uint64_t n, const uint32_t
 }
 
 void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
-                     const uint32_t* rem, const uint32_t* idmap, Sub& s) {
+                     const uint32_t* rem, const uint32_t* idmap, Sub& s, const uint32_t* group_of = nullptr,
+                     uint32_t ngroups = 0) {
   if (na >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "subgraph: too many vertices");
   s.n = (uint32_t)na;
   s.orig.alloc(c, (na ? na : 1) * sizeof(uint32_t));
@@ -148,7 +172,8 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
   }
   // New order.
   DBuf okeys(c, na * sizeof(uint64_t));
-  k_order_keys<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(alive, na, deg, okeys.as<uint64_t>());
+  k_order_keys<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(alive, na, deg, group_of,
+                                                                             okeys.as<uint64_t>());
   KT_LAUNCHED(c);
   radix_sort_u64(c, okeys.as<uint64_t>(), nullptr, na, 64);
   DBuf newid(c, (g.n ? g.n : 1) * sizeof(uint32_t));
@@ -158,6 +183,24 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
       okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>(), idmap);
   KT_LAUNCHED(c);
   okeys.release();
+  if (group_of) {
+    // orig holds ids of g here (mapped below); group them.
+    s.vgid.alloc(c, na * sizeof(uint32_t));
+    s.vbase.alloc(c, na * sizeof(uint32_t));
+    DBuf gstart(c, (uint64_t)ngroups * sizeof(uint32_t)), gsize(c, (uint64_t)ngroups * sizeof(uint32_t));
+    zero(c, gsize.get(), gsize.bytes());
+    k_group_meta<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.orig.as<uint32_t>(), na, group_of, s.vgid.as<uint32_t>(), gstart.as<uint32_t>(), gsize.as<uint32_t>());
+    KT_LAUNCHED(c);
+    k_group_base<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(s.vgid.as<uint32_t>(), na,
+                                                                              gstart.as<uint32_t>(),
+                                                                              s.vbase.as<uint32_t>());
+    KT_LAUNCHED(c);
+    std::vector<uint32_t> sizes(ngroups);
+    copy_d2h(c, sizes.data(), gsize.get(), ngroups * sizeof(uint32_t));
+    s.max_group = 0;
+    for (uint32_t x : sizes) s.max_group = std::max(s.max_group, x);
+  }
   scan_u32_to_u64(c, sdeg.as<uint32_t>(), s.off.as<uint64_t>(), na + 1);
   const uint64_t n2 = read_word<uint64_t>(c, s.off.as<uint64_t>() + na);
   if (n2 & 1) throw Error(KT_ERR_CUDA, "subgraph: odd adjacency size (inconsistent degrees)");
@@ -211,6 +254,13 @@ void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s) {
   (void)g;
   build_from_list(c, kc.cur(), kc.alive.as<uint32_t>(), kc.n_alive, kc.deg.as<uint32_t>(), kc.rem.as<uint32_t>(),
                   kc.map(), s);
+}
+
+void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
+                       const uint32_t* rem, const uint32_t* group_of, uint32_t ngroups, Sub& s) {
+  if (g.n >= (1ull << 28)) throw Error(KT_ERR_LIMIT, "batched union: more than 2^28 vertices in a wave");
+  if (ngroups > 65536) throw Error(KT_ERR_LIMIT, "batched union: more than 65536 graphs in a wave");
+  build_from_list(c, g, alive, na, deg, rem, nullptr, s, group_of, ngroups);
 }
 
 void build_sub_all(Ctx* c, const Graph& g, Sub& s) {

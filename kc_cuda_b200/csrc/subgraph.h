@@ -24,12 +24,31 @@ struct Sub {
   // whose bitsets fit in L2 together.
   DBuf order;
   uint32_t tile_bits = 0;
+  // Batched unions of many graphs: vertices are grouped by graph (new ids of
+  // one graph are contiguous), vgid[v] = its graph, vbase[v] = first new id
+  // of its graph, max_group = most vertices of one graph.
+  DBuf vgid, vbase;
+  uint32_t max_group = 0;
 };
 
 // Builds the subgraph induced by the k-core state's alive vertices.
 void build_sub(Ctx* c, const Graph& g, const KCore& kc, Sub& s);
 // Builds the whole graph as a subgraph (every vertex of degree > 0).
 void build_sub_all(Ctx* c, const Graph& g, Sub& s);
+// Subgraph of a list of alive vertices of a disjoint union of graphs,
+// grouped by graph: group_of[v] (< 65536) is the graph of vertex v of g
+// (g.n < 2^28); within a graph, ascending (degree, id).
+void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
+                       const uint32_t* rem, const uint32_t* group_of, uint32_t ngroups, Sub& s);
+
+// Per-graph bookkeeping of a batched peel: after every level, each graph
+// with alive edges records (its minimum support + 2, its alive edges).
+struct GraphTrack {
+  const uint32_t* vgid;  // graph of each vertex of the working graph
+  uint32_t ngroups;
+  uint32_t* kmax;        // device [ngroups], last recorded level (0 = none)
+  uint64_t* count;       // device [ngroups]
+};
 
 // support.cu: sup[e] = triangles through edge e (all edges of s).  Uses the
 // bitsets when they are built.  cap > 0 (dense mode only): an edge whose
@@ -56,6 +75,6 @@ void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub
 // guess (> t0, 0 = none): first level to try, undone and halved toward t0 if
 // it empties the graph (only without truss output).
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
-                      uint32_t guess = 0);
+                      uint32_t guess = 0, const GraphTrack* track = nullptr);
 
 }  // namespace kt

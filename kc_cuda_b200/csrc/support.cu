@@ -24,15 +24,19 @@ namespace {
 
 constexpr unsigned kSupThreads = 256;
 
+// Batched unions: the bitmap covers only v's own graph, bits indexed from
+// vbase[v] (graphs are contiguous and no edge crosses graphs); `range` =
+// most vertices of one graph.
 __global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, const uint64_t* __restrict__ off,
                                                                 const uint32_t* __restrict__ adj,
                                                                 const uint32_t* __restrict__ eid,
                                                                 const uint64_t* __restrict__ up,
                                                                 uint32_t* __restrict__ sup,
-                                                                unsigned long long* cursor) {
+                                                                unsigned long long* cursor,
+                                                                const uint32_t* __restrict__ vbase, uint32_t range) {
   extern __shared__ uint32_t bits[];
   __shared__ uint32_t s_v;
-  const uint32_t words = (n + 31) / 32;
+  const uint32_t words = (range + 31) / 32;
   for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0;
   __syncthreads();
   while (true) {
@@ -43,9 +47,10 @@ __global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, cons
     __syncthreads();
     const uint32_t v = s_v;
     if (v == 0xffffffffu) break;
+    const uint32_t base = vbase ? vbase[v] : 0u;
     const uint64_t vb = off[v], ve = off[v + 1], vu = up[v];
     for (uint64_t j = vb + threadIdx.x; j < ve; j += blockDim.x) {
-      const uint32_t w = adj[j];
+      const uint32_t w = adj[j] - base;
       atomicOr(&bits[w >> 5], 1u << (w & 31));
     }
     __syncthreads();
@@ -55,7 +60,7 @@ __global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, cons
       const uint64_t ub = off[u], ue = off[u + 1];
       uint32_t cnt = 0;
       for (uint64_t q = ub + lane_id(); q < ue; q += 32) {
-        const uint32_t w = adj[q];
+        const uint32_t w = adj[q] - base;
         cnt += (bits[w >> 5] >> (w & 31)) & 1u;
       }
       cnt = warp_sum(cnt);
@@ -63,7 +68,7 @@ __global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, cons
     }
     __syncthreads();
     for (uint64_t j = vb + threadIdx.x; j < ve; j += blockDim.x) {
-      const uint32_t w = adj[j];
+      const uint32_t w = adj[j] - base;
       bits[w >> 5] = 0;
     }
     __syncthreads();
@@ -211,8 +216,9 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
       launch_dense_support<true>(c, s, sup, cap);
     else
       launch_dense_support<false>(c, s, sup, 0);
-  } else if ((int64_t)s.n <= c->opt.support_bitmap_max_n) {
-    const size_t smem = ((s.n + 31) / 32) * sizeof(uint32_t);
+  } else if ((int64_t)(s.vbase.get() ? s.max_group : s.n) <= c->opt.support_bitmap_max_n) {
+    const uint32_t range = s.vbase.get() ? s.max_group : s.n;
+    const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
       KT_CUDA(cudaFuncSetAttribute(k_support_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -223,7 +229,9 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
     const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * c->num_sms, s.n);
     k_support_bitmap<<<grid, kSupThreads, smem, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
                                                              s.eid.as<uint32_t>(), s.up.as<uint64_t>(), sup,
-                                                             cur.as<unsigned long long>());
+                                                             cur.as<unsigned long long>(),
+                                                             s.vbase.get() ? s.vbase.as<uint32_t>() : nullptr,
+                                                             range);
     KT_LAUNCHED(c);
   } else {
     k_support_search<<<grid_for(s.m * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(

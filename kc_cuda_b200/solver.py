@@ -49,6 +49,7 @@ class Stats(ctypes.Structure):
         ("device_bytes_peak", ctypes.c_uint64),
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("peel_decrements", ctypes.c_uint64),
+        ("batch_waves", ctypes.c_uint32), ("batch_graphs", ctypes.c_uint32),
     ]
 
     def as_dict(self):
@@ -78,6 +79,14 @@ SIGNATURES = [
     ("kt_tsv_stage", ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     ("kt_solve_staged", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
     ("kt_tsv_free", None, [_P, _P]),
+    ("kt_batch_create", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
+    ("kt_batch_add_pairs", ctypes.c_int, [_P, _U64P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]),
+    ("kt_batch_add_mix", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    ("kt_batch_size", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    ("kt_batch_run", ctypes.c_int, [_P]),
+    ("kt_batch_results", ctypes.c_int, [_P, _U32P, _U64P]),
+    ("kt_batch_free", None, [_P]),
+    ("kt_load_mix_graph", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     ("kt_kcore", ctypes.c_int, [_P, _P, ctypes.c_uint32, _U8P, ctypes.POINTER(ctypes.c_uint32)]),
     ("kt_kcore_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_void_p, ctypes.c_void_p]),
@@ -195,6 +204,14 @@ class Context:
         self.check(self._L.kt_tsv_stage(self._h, p, n, ctypes.byref(t)))
         return StagedTsv(self, t, n)
 
+    def load_mix_graph(self, index: int, base_seed: int = 0x4B54) -> "Graph":
+        g = ctypes.c_void_p()
+        self.check(self._L.kt_load_mix_graph(self._h, index, base_seed, ctypes.byref(g)))
+        return Graph(self, g)
+
+    def batch(self) -> "Batch":
+        return Batch(self)
+
     # ---- one-call solve
     def solve_tsv(self, data) -> Tuple[int, int]:
         p, n, keep = _buf(data)
@@ -202,6 +219,54 @@ class Context:
         e = ctypes.c_uint64()
         self.check(self._L.kt_solve_tsv(self._h, p, n, ctypes.byref(k), ctypes.byref(e)))
         return k.value, e.value
+
+
+class Batch:
+    """Many graphs solved together (waves of disjoint unions)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx.check(ctx._L.kt_batch_create(ctx._h, ctypes.byref(h)))
+        self._h = h
+
+    def free(self):
+        if getattr(self, "_h", None):
+            self.ctx._L.kt_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.free()
+
+    def add_pairs(self, xy: np.ndarray) -> int:
+        xy = np.ascontiguousarray(xy, dtype=np.uint64)
+        gid = ctypes.c_uint32()
+        self.ctx.check(self.ctx._L.kt_batch_add_pairs(self._h, xy.ctypes.data if xy.size else None, xy.size,
+                                                      ctypes.byref(gid)))
+        return gid.value
+
+    def add_edges(self, pairs: np.ndarray) -> int:
+        p = np.asarray(pairs, dtype=np.uint64).reshape(-1, 2)
+        return self.add_pairs((p[:, 0] << np.uint64(32)) | p[:, 1])
+
+    def add_mix(self, first: int, count: int, base_seed: int = 0x4B54):
+        self.ctx.check(self.ctx._L.kt_batch_add_mix(self._h, first, count, base_seed))
+
+    def size(self) -> Tuple[int, int]:
+        g = ctypes.c_uint64()
+        r = ctypes.c_uint64()
+        self.ctx.check(self.ctx._L.kt_batch_size(self._h, ctypes.byref(g), ctypes.byref(r)))
+        return g.value, r.value
+
+    def run(self):
+        self.ctx.check(self.ctx._L.kt_batch_run(self._h))
+
+    def results(self) -> Tuple[np.ndarray, np.ndarray]:
+        n = self.size()[0]
+        k = np.zeros(max(n, 1), dtype=np.uint32)
+        e = np.zeros(max(n, 1), dtype=np.uint64)
+        self.ctx.check(self.ctx._L.kt_batch_results(self._h, k.ctypes.data, e.ctypes.data))
+        return k[:n], e[:n]
 
 
 class StagedTsv:
