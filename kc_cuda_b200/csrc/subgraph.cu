@@ -52,15 +52,17 @@ __global__ void k_group_base(const uint32_t* __restrict__ vgid, uint64_t na, con
     vbase[i] = gstart[vgid[i]];
 }
 
+// Decodes the sorted order keys: orig[i] = the vertex, newid[v] = i, sdeg[i]
+// = its degree (read from deg when the key holds a saturated copy).
 __global__ void k_order_apply(const uint64_t* __restrict__ keys, uint64_t na, uint32_t* __restrict__ orig,
                               uint32_t* __restrict__ newid, uint32_t* __restrict__ sdeg,
-                              const uint32_t* __restrict__ idmap) {
+                              const uint32_t* __restrict__ deg, bool grouped) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
-    const uint32_t v = (uint32_t)k;
+    const uint32_t v = grouped ? (uint32_t)(k & 0xfffffffULL) : (uint32_t)k;
     orig[i] = v;  // ids of the graph being read; mapped below if it is a compacted copy
     newid[v] = (uint32_t)i;
-    sdeg[i] = (uint32_t)(k >> 32);
+    sdeg[i] = grouped ? deg[v] : (uint32_t)(k >> 32);
   }
 }
 
@@ -180,7 +182,8 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
   DBuf sdeg(c, (na + 1) * sizeof(uint32_t));
   zero(c, sdeg.get(), (na + 1) * sizeof(uint32_t));
   k_order_apply<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>(), idmap);
+      okeys.as<uint64_t>(), na, s.orig.as<uint32_t>(), newid.as<uint32_t>(), sdeg.as<uint32_t>(), deg,
+      group_of != nullptr);
   KT_LAUNCHED(c);
   okeys.release();
   if (group_of) {
