@@ -46,6 +46,7 @@ WORKLOADS = {
     "rmat24": (24, 32, 2, [80, 120, 200]),
     "rmat21": (21, 32, 2, [80, 120, 200]),
     "rmat16": (16, 16, 1, [30]),
+    "mix4096": None,  # batched: the 4,096-graph mix (see run_mix)
 }
 # CPU sample of the same family for the reference solver (about 10-30 s).
 CPU_SAMPLE = (20, 32, 2, [80, 120, 200])
@@ -198,6 +199,70 @@ def cpu_baseline_run(steps: int, warmup: int, threads: int):
     return m / med, desc, times
 
 
+def run_mix(args, world, rank, local, pg):
+    """Batched workload: graphs 0..G-1 of the mix (n log-uniform over
+    [1e3, 1e6], R-MAT or Erdos-Renyi, edge factor 4..64, one clique of 5..60),
+    generated on the device.  value = graphs/s of kt_batch_run with the input
+    generation excluded; the per-graph path (kt_load_mix_graph + kt_solve,
+    one graph at a time) is timed on every `sample_every`-th graph."""
+    import numpy as np
+
+    import kc_cuda_b200 as K
+    G = args.mix_graphs
+    first = rank * G  # each rank its own slice of the mix (independent graphs)
+    ctx = K.Context(local)
+    # Per-graph path on a uniform sample.
+    lat = []
+    sample = list(range(first, first + G, args.sample_every))
+    for i in sample[: min(3, len(sample))]:  # warm-up
+        g = ctx.load_mix_graph(i)
+        g.kmax_truss()
+        g.free()
+    answers_alone = {}
+    for i in sample:
+        g = ctx.load_mix_graph(i)
+        answers_alone[i] = g.kmax_truss()
+        lat.append(ctx.stats()["ms_total"])
+        g.free()
+    per_graph_gps = len(lat) / (sum(lat) / 1000.0)
+    # Batched.
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        b = ctx.batch()
+        b.add_mix(first, min(G, 64))
+        b.run()
+        b.free()
+    barrier(pg)
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            b = ctx.batch()
+            b.add_mix(first, G)
+            b.run()
+            st = ctx.stats()
+            times.append(st["ms_total"] - st["ms_parse"])
+            k, c = b.results()
+            b.free()
+    for i in sample:
+        assert (int(k[i - first]), int(c[i - first])) == answers_alone[i], i
+    step_ms = max_over_ranks(pg, sum(times) / len(times))
+    total = sum_over_ranks(pg, float(G))
+    value = total / (step_ms / 1000.0)
+    if rank == 0:
+        lat_np = np.array(lat)
+        print(json.dumps({
+            "metric": "batched kmax-truss graphs/s (mix of graphs 0..G-1)", "value": value, "unit": "graphs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"mix{G}", "graphs": G, "waves": st["batch_waves"],
+                       "edge_records": int(b.size()[1]) if False else None},
+            "per_graph": {"graphs_per_s": per_graph_gps, "sample": len(lat), "every": args.sample_every,
+                          "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
+            "batched_vs_per_graph": value / per_graph_gps,
+            "clocks": clk.summary(),
+        }))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,8 +271,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mix-graphs", type=int, default=4096)
+    ap.add_argument("--sample-every", type=int, default=32)
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
+    if args.workload == "mix4096" and args.impl == "ours":
+        run_mix(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     threads = os.cpu_count() or 1
     metric = "kmax-truss solve edges/s per graph"
 

@@ -110,7 +110,9 @@ kt_status kt_batch_add_pairs(kt_batch* b, const uint64_t* xy, uint64_t count, ui
  * (generated on the device at run time from their seeds). */
 kt_status kt_batch_add_mix(kt_batch* b, uint64_t first_index, uint64_t count, uint64_t base_seed);
 kt_status kt_batch_size(const kt_batch* b, uint64_t* graphs, uint64_t* edge_records);
-/* Solves every graph of the batch; ms_total / batch_waves in kt_get_stats. */
+/* Solves every graph of the batch; kt_get_stats: ms_total = the whole run,
+ * ms_parse = the part spent generating / uploading the graphs' edges,
+ * batch_waves = waves used. */
 kt_status kt_batch_run(kt_batch* b);
 /* kmax and kmax-truss edge count of every graph, in graph-id order. */
 kt_status kt_batch_results(const kt_batch* b, uint32_t* kmax, uint64_t* edges);

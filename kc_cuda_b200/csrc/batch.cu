@@ -280,7 +280,11 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   DBuf keys;
   uint64_t nkeys = 0;
   std::vector<uint64_t> vbase;
+  // Input: generation (or upload) of the wave's edge keys, timed apart.
+  KT_CUDA(cudaEventRecord(c->ev[4], c->stream));
   const uint64_t nv = wave_keys(c, items, keys, nkeys, vbase);
+  KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
+  st.ms_parse += event_ms(c->ev[4], c->ev[5]);
   Graph U;
   build_graph(c, keys.as<uint64_t>(), nkeys, nv, U);
   keys.release();
