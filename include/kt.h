@@ -49,8 +49,19 @@ void kt_destroy(kt_ctx* ctx);
 const char* kt_last_error(const kt_ctx* ctx);
 const char* kt_status_string(kt_status s);
 
-/* Tunables by name (see DESIGN and kt_option_names): returns KT_ERR_INVALID
- * for an unknown name. */
+/* Tunables by name; KT_ERR_INVALID for an unknown name.
+ *   predict (1)                 prediction phase (truss of the maximum core)
+ *   persistent (1)              peel / k-core rounds in one cooperative launch
+ *   support_bitmap_max_n (2^20) vertex-bitmap support up to this many vertices
+ *   dense_max_n (65536)         adjacency bitsets up to this many vertices
+ *   dense_min_fill (32)         bitsets when avg degree * this >= words per row
+ *   recount_gamma (16)          recount round when frontier * thr * gamma > alive * words
+ *   capped_support (1)          search phase: abandon supports below the threshold
+ *   timeout_ms (20000)          bound on every device-side wait
+ *   parse_pipeline_mb (256)     host->device chunk of file ingest
+ *   record_kernel_times (0)     events around support / peel kernels
+ *   debug_checks (0)            extra host-side consistency checks
+ *   verbose (0)                 stage decisions on stderr */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 

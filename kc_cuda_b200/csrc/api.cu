@@ -315,7 +315,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"timeout_ms", &o.timeout_ms},
              {"parse_pipeline_mb", &o.parse_pipeline_mb},
              {"record_kernel_times", &o.record_kernel_times},
-             {"debug_checks", &o.debug_checks}};
+             {"debug_checks", &o.debug_checks},
+             {"verbose", &o.verbose}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

@@ -235,10 +235,15 @@ static uint64_t wave_keys(Ctx* c, const std::vector<BatchItem*>& items, DBuf& ke
 }
 
 // One union stage: the subgraph of vertices whose core reaches need[graph],
-// its support and its tracked peel; kmax/count receive the per-graph records.
+// its support and its tracked peel, graph g from level t0[g] (empty: 3) with
+// early stop at stop[g] edges (empty: none); kmax/count receive the
+// per-graph records.
 static void union_truss(Ctx* c, const Graph& U, const uint32_t* dcore, const uint32_t* dgid, uint32_t G,
-                        const std::vector<uint32_t>& need, std::vector<uint32_t>& kmax, std::vector<uint64_t>& count,
+                        const std::vector<uint32_t>& need, const std::vector<uint32_t>& t0,
+                        const std::vector<uint64_t>& stop, std::vector<uint32_t>& kmax, std::vector<uint64_t>& count,
                         kt_stats& st) {
+  Timer tm(c);
+  tm.start();
   DBuf dneed(c, G * sizeof(uint32_t));
   copy_h2d(c, dneed.get(), need.data(), G * sizeof(uint32_t));
   DBuf list(c, (U.n ? U.n : 1) * sizeof(uint32_t));
@@ -260,18 +265,34 @@ static void union_truss(Ctx* c, const Graph& U, const uint32_t* dcore, const uin
   deg.release();
   st.core_vertices += s.n;
   st.core_edges += s.m;
+  st.ms_subgraph += tm.stop();
   if (s.m == 0) return;
+  tm.start();
   DBuf sup(c, s.m * sizeof(uint32_t));
   edge_support(c, s, sup.as<uint32_t>());
+  st.ms_support += tm.stop();
+  tm.start();
   DBuf dk(c, G * sizeof(uint32_t)), dc(c, G * sizeof(uint64_t));
   zero(c, dk.get(), dk.bytes());
   zero(c, dc.get(), dc.bytes());
   GraphTrack tr{s.vgid.as<uint32_t>(), G, dk.as<uint32_t>(), dc.as<uint64_t>()};
+  DBuf dt0, dstop;
+  if (!t0.empty()) {
+    dt0.alloc(c, G * sizeof(uint32_t));
+    copy_h2d(c, dt0.get(), t0.data(), G * sizeof(uint32_t));
+    tr.t0 = dt0.as<uint32_t>();
+  }
+  if (!stop.empty()) {
+    dstop.alloc(c, G * sizeof(uint64_t));
+    copy_h2d(c, dstop.get(), stop.data(), G * sizeof(uint64_t));
+    tr.stop = dstop.as<uint64_t>();
+  }
   const PeelResult pr = truss_peel(c, s, sup.as<uint32_t>(), 3, 0, nullptr, 0, &tr);
   st.levels += pr.levels;
   st.rounds += (uint32_t)pr.rounds;
   copy_d2h(c, kmax.data(), dk.get(), G * sizeof(uint32_t));
   copy_d2h(c, count.data(), dc.get(), G * sizeof(uint64_t));
+  st.ms_peel += tm.stop();
 }
 
 void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
@@ -285,10 +306,14 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   const uint64_t nv = wave_keys(c, items, keys, nkeys, vbase);
   KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
   st.ms_parse += event_ms(c->ev[4], c->ev[5]);
+  Timer tm(c);
+  tm.start();
   Graph U;
   build_graph(c, keys.as<uint64_t>(), nkeys, nv, U);
   keys.release();
+  st.ms_csr += tm.stop();
   // Core numbers of the union and each graph's maximum core.
+  tm.start();
   DBuf dcore(c, (nv ? nv : 1) * sizeof(uint32_t));
   {
     KCore kc;
@@ -308,14 +333,18 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   }
   std::vector<uint32_t> cmax(G);
   copy_d2h(c, cmax.data(), dcm.get(), G * sizeof(uint32_t));
+  st.ms_kcore += tm.stop();
   // Phase 1: the maximum core of every graph that can hold a triangle.
   std::vector<uint32_t> need(G, 0);
   for (uint32_t g = 0; g < G; ++g) need[g] = cmax[g] >= 2 ? cmax[g] : 0;
   std::vector<uint32_t> k1;
   std::vector<uint64_t> c1;
-  union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, k1, c1, st);
-  // Phase 2: the (L-1)-core of every graph whose bound is not met.
+  union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, {}, {}, k1, c1, st);
+  // Phase 2: the (L-1)-core of every graph whose bound is not met, peeled
+  // from level L with early stop at phase 1's count.
   bool any = false;
+  std::vector<uint32_t> t0(G, 3);
+  std::vector<uint64_t> stop(G, 0);
   for (uint32_t g = 0; g < G; ++g) {
     items[g]->kmax = 0;
     items[g]->count = 0;
@@ -328,12 +357,16 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
       continue;
     }
     need[g] = L ? L - 1 : 2;
+    if (L) {
+      t0[g] = L;
+      stop[g] = c1[g];
+    }
     any = true;
   }
   if (any) {
     std::vector<uint32_t> k2;
     std::vector<uint64_t> c2;
-    union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, k2, c2, st);
+    union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, t0, stop, k2, c2, st);
     for (uint32_t g = 0; g < G; ++g) {
       if (!need[g]) continue;
       items[g]->kmax = k2[g] >= 3 ? k2[g] : 0;

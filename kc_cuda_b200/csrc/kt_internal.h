@@ -2,6 +2,7 @@
 // device buffers charged to the context's HBM budget, error propagation and
 // launch accounting.
 #pragma once
+#include <cstdio>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -51,7 +52,14 @@ struct Options {
   int64_t parse_pipeline_mb = 256;  // host->device chunk for file ingest
   int64_t record_kernel_times = 0;  // events around support / peel kernels
   int64_t debug_checks = 0;       // extra host-side consistency checks
+  int64_t verbose = 0;            // stage decisions on stderr
 };
+
+// Stage decisions on stderr when the context's verbose option is set.
+#define KT_LOG(c, ...)                                  \
+  do {                                                  \
+    if ((c)->opt.verbose) std::fprintf(stderr, __VA_ARGS__); \
+  } while (0)
 
 struct Ctx;
 

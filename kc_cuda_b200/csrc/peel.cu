@@ -66,7 +66,15 @@ struct PeelArgs {
   unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements, [2] recounted edges
   DevWords* words;
   unsigned long long timeout_ns;
+  // Batched unions: per-graph thresholds gthr[egr[e]] replace thr (0 = the
+  // graph is finished and its edges are never frontier edges).
+  const uint32_t* gthr;
+  const uint32_t* egr;
 };
+
+__device__ __forceinline__ uint32_t edge_thr(const PeelArgs& A, uint32_t e) {
+  return A.gthr ? A.gthr[A.egr[e]] : A.thr;
+}
 
 __device__ __forceinline__ void push_warp_full(bool want, uint32_t item, uint32_t* list, unsigned long long* cnt,
                                                uint64_t cap, uint32_t* err) {
@@ -100,12 +108,12 @@ __device__ __forceinline__ uint64_t find_sorted(const uint32_t* a, uint64_t lo, 
 // Triangle {e, a, b} seen from frontier edge e in round r; returns which of
 // a, b crossed below the threshold (to be pushed).
 __device__ __forceinline__ void close_triangle(const PeelArgs& A, uint32_t e, uint32_t a, uint32_t b, uint32_t r,
-                                               bool& pa, bool& pb, uint32_t& ndec) {
+                                               uint32_t thr, bool& pa, bool& pb, uint32_t& ndec) {
   const uint32_t sa = A.state[a], sb = A.state[b];
   if (sa < r || sb < r) return;  // broken in an earlier round
   if (sa > r && !(sb == r && b < e)) {
     ++ndec;
-    if (atomicSub(&A.sup[a], 1u) == A.thr) {
+    if (atomicSub(&A.sup[a], 1u) == thr) {
       A.state[a] = r + 1;
       if (A.truss) A.truss[a] = A.tval;
       pa = true;
@@ -113,7 +121,7 @@ __device__ __forceinline__ void close_triangle(const PeelArgs& A, uint32_t e, ui
   }
   if (sb > r && !(sa == r && a < e)) {
     ++ndec;
-    if (atomicSub(&A.sup[b], 1u) == A.thr) {
+    if (atomicSub(&A.sup[b], 1u) == thr) {
       A.state[b] = r + 1;
       if (A.truss) A.truss[b] = A.tval;
       pb = true;
@@ -128,6 +136,7 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
   const uint64_t k = A.ends[e];
   uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
   if (lane_id() == 0) tdeg += (uint64_t)atomicSub(&A.adeg[x], 1u) + atomicSub(&A.adeg[y], 1u);
+  const uint32_t thr = edge_thr(A, e);  // the triangle's edges share e's graph
   uint32_t ndec = 0;
   uint64_t xb = A.off[x], xe = A.off[x + 1], yb = A.off[y], ye = A.off[y + 1];
   if (xe - xb > ye - yb) {
@@ -151,7 +160,7 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
         if (p != ye) {
           a = A.eid[q];
           b = A.eid[p];
-          close_triangle(A, e, a, b, r, pa, pb, ndec);
+          close_triangle(A, e, a, b, r, thr, pa, pb, ndec);
         }
       }
       push_warp_full(pa, a, next, ncnt, A.cap, err);
@@ -181,7 +190,7 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
     if (lane < ta && q < tb && hit == av) {
       a = A.eid[xb + i + lane];
       b = A.eid[yb + j + q];
-      close_triangle(A, e, a, b, r, pa, pb, ndec);
+      close_triangle(A, e, a, b, r, thr, pa, pb, ndec);
     }
     push_warp_full(pa, a, next, ncnt, A.cap, err);
     push_warp_full(pb, b, next, ncnt, A.cap, err);
@@ -207,7 +216,7 @@ __device__ __forceinline__ void level_frontier(const PeelArgs& A, uint32_t r, ui
     uint32_t e = 0;
     if (i < A.na) {
       e = A.alive[i];
-      if (A.state[e] == kAlive && A.sup[e] < A.thr) {
+      if (A.state[e] == kAlive && A.sup[e] < edge_thr(A, e)) {
         A.state[e] = r;
         if (A.truss) A.truss[e] = A.tval;
         want = true;
@@ -250,7 +259,7 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
     bool want = false;
     if (ok) {
       A.sup[e] = sc;
-      if (sc < A.thr) {
+      if (sc < edge_thr(A, e)) {
         A.state[e] = r + 1;
         if (A.truss) A.truss[e] = A.tval;
         want = true;
@@ -375,22 +384,47 @@ __global__ void k_track(const uint32_t* __restrict__ alive, uint64_t na, const u
   }
 }
 
+// Records every running graph's level and sets its next threshold (its
+// minimum support + 1, i.e. level min + 3); a graph with no alive edge, or
+// whose first level kept exactly stop[g] edges, is finished (threshold 0).
 __global__ void k_track_record(uint32_t ngroups, unsigned long long* __restrict__ gcnt, uint32_t* __restrict__ gmin,
-                               uint32_t* __restrict__ kmax, uint64_t* __restrict__ count) {
+                               uint32_t* __restrict__ kmax, uint64_t* __restrict__ count,
+                               uint32_t* __restrict__ gthr, const uint64_t* __restrict__ stop, bool first) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
-    if (gcnt[g]) {
-      kmax[g] = gmin[g] + 2;
-      count[g] = gcnt[g];
+    if (gthr[g]) {
+      if (gcnt[g]) {
+        kmax[g] = gmin[g] + 2;
+        count[g] = gcnt[g];
+        gthr[g] = first && stop && stop[g] && gcnt[g] == stop[g] ? 0u : gmin[g] + 1;
+      } else {
+        gthr[g] = 0;
+      }
     }
     gcnt[g] = 0;
     gmin[g] = 0xffffffffu;
   }
 }
 
+__global__ void k_track_init(uint64_t m, const uint64_t* __restrict__ ends, const uint32_t* __restrict__ vgid,
+                             uint32_t* __restrict__ egr, uint32_t ngroups, const uint32_t* __restrict__ t0,
+                             uint32_t tdef, uint32_t* __restrict__ gthr) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x)
+    egr[e] = vgid[(uint32_t)(ends[e] >> 32)];
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    const uint32_t t = t0 && t0[g] > 3 ? t0[g] : (tdef > 3 ? tdef : 3);
+    gthr[g] = t - 2;
+  }
+}
+
 struct StillAlive {
   const uint32_t* list;
   const uint32_t* state;
-  __device__ bool keep(uint64_t i) const { return state[list[i]] == kAlive; }
+  const uint32_t* gthr;  // batched: drop the edges of finished graphs
+  const uint32_t* egr;
+  __device__ bool keep(uint64_t i) const {
+    const uint32_t e = list[i];
+    return state[e] == kAlive && (!gthr || gthr[egr[e]] != 0);
+  }
   __device__ uint32_t value(uint64_t i) const { return list[i]; }
 };
 
@@ -478,6 +512,8 @@ struct Peeler {
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
+    A.gthr = track ? gthr.as<uint32_t>() : nullptr;
+    A.egr = track ? egr.as<uint32_t>() : nullptr;
     return A;
   }
 
@@ -510,10 +546,14 @@ struct Peeler {
     c->timer.end(c->stream, e0, &c->stats.ms_peel_kernel);
     c->stats.peel_launches++;
     check_words(c, "truss peel");
+    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds\n", t,
+           (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds);
     r += (uint32_t)rounds + 1;
     res->rounds += rounds;
     res->levels++;
-    na = compact(c, na, StillAlive{alive[ai].as<uint32_t>(), state.as<uint32_t>()}, alive[ai ^ 1].as<uint32_t>());
+    na = compact(c, na,
+                 StillAlive{alive[ai].as<uint32_t>(), state.as<uint32_t>(), A.gthr, A.egr},
+                 alive[ai ^ 1].as<uint32_t>());
     ai ^= 1;
     return na;
   }
@@ -529,17 +569,23 @@ struct Peeler {
     c->stats.peel_decrements += h[1];
   }
 
-  // Batched unions: per-graph records after a level.
+  // Batched unions: per-graph thresholds and records after a level.
   const GraphTrack* track = nullptr;
-  DBuf tcnt, tmin;
-  void record_groups() {
-    if (!track || track->ngroups == 0) return;
-    if (!tcnt.get()) {
-      tcnt = DBuf(c, (uint64_t)track->ngroups * 8);
-      tmin = DBuf(c, (uint64_t)track->ngroups * 4);
-      zero(c, tcnt.get(), tcnt.bytes());
-      KT_CUDA(cudaMemsetAsync(tmin.get(), 0xff, tmin.bytes(), c->stream));
-    }
+  DBuf tcnt, tmin, gthr, egr;
+  void init_track(uint32_t t0) {
+    const uint32_t G = std::max<uint32_t>(track->ngroups, 1);
+    tcnt = DBuf(c, (uint64_t)G * 8);
+    tmin = DBuf(c, (uint64_t)G * 4);
+    gthr = DBuf(c, (uint64_t)G * 4);
+    egr = DBuf(c, s->m * 4);
+    zero(c, tcnt.get(), tcnt.bytes());
+    KT_CUDA(cudaMemsetAsync(tmin.get(), 0xff, tmin.bytes(), c->stream));
+    k_track_init<<<grid_for(std::max<uint64_t>(s->m, G), 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s->m, s->ends.as<uint64_t>(), track->vgid, egr.as<uint32_t>(), track->ngroups, track->t0, t0,
+        gthr.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
+  void record_groups(bool first) {
     if (na) {
       k_track<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(
           alive[ai].as<uint32_t>(), na, s->ends.as<uint64_t>(), sup, track->vgid, tcnt.as<unsigned long long>(),
@@ -547,7 +593,8 @@ struct Peeler {
       KT_LAUNCHED(c);
     }
     k_track_record<<<grid_for(track->ngroups, 256, c->num_sms * 4), 256, 0, c->stream>>>(
-        track->ngroups, tcnt.as<unsigned long long>(), tmin.as<uint32_t>(), track->kmax, track->count);
+        track->ngroups, tcnt.as<unsigned long long>(), tmin.as<uint32_t>(), track->kmax, track->count,
+        gthr.as<uint32_t>(), track->stop, first);
     KT_LAUNCHED(c);
   }
 
@@ -612,9 +659,16 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
   P.init();
   uint32_t t = t0;
   if (track) {
-    // Batched: every graph is tracked, so no early stop and no jump.
-    stop_count = 0;
-    guess = 0;
+    // Batched: every graph climbs its own levels (min-support jumps, its own
+    // first level and early stop); a cascade runs all of them at once.
+    if (track->ngroups == 0) return res;
+    P.init_track(t0);
+    for (bool first = true; P.na; first = false) {
+      P.cascade(t);
+      P.record_groups(first);
+    }
+    P.account();
+    return res;
   }
   // Jump phase: try `guess` (> t0) from a snapshot; halve toward t0 on failure.
   if (!truss && guess > t0) {
@@ -661,7 +715,6 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
   bool first = true;
   while (true) {
     const uint64_t left = P.cascade(t);
-    P.record_groups();
     if (left == 0) break;
     if (first && stop_count && left == stop_count) {
       res.kmax = t;

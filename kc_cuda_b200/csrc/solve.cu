@@ -53,26 +53,6 @@ struct AtLeast {
   __device__ uint64_t value(uint64_t e) const { return ends[e]; }
 };
 
-struct Timer {
-  Ctx* c;
-  cudaEvent_t a, b;
-  explicit Timer(Ctx* cx) : c(cx) {
-    KT_CUDA(cudaEventCreate(&a));
-    KT_CUDA(cudaEventCreate(&b));
-  }
-  ~Timer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-  void start() { KT_CUDA(cudaEventRecord(a, c->stream)); }
-  double stop() {
-    KT_CUDA(cudaEventRecord(b, c->stream));
-    KT_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    KT_CUDA(cudaEventElapsedTime(&ms, a, b));
-    return ms;
-  }
-};
 
 }  // namespace
 
@@ -96,6 +76,50 @@ void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
     }
   } resolve{c};
   solve_graph_inner(c, g, kmax, count);
+}
+
+// kmax-truss of the maximum core s1 (exact supports sup1, core number
+// cmax).  Levels g are tried from the support bound down, halving toward 3:
+// the g-truss lies within the edges of support >= g-2, so while those are
+// few, the g-truss and everything above it are found on a graph rebuilt from
+// them alone.  When they are not few, the whole core is peeled, first
+// trying level min(g, (cmax+1)/2) from a snapshot.
+PeelResult predict_peel(Ctx* c, const Sub& s1, uint32_t* sup1, uint32_t cmax) {
+  uint32_t g = support_bound(c, sup1, s1.m, cmax + 1);
+  KT_LOG(c, "kt: predict on %u vertices, %llu edges, cmax %u: support bound %u\n", s1.n, (unsigned long long)s1.m,
+         cmax, g);
+  if (g < 3) return PeelResult{};  // no truss level 3: no triangle
+  const uint32_t half = (cmax + 1) / 2;
+  uint32_t levels = 0;
+  uint64_t rounds = 0;
+  for (bool tried = false; g > 3; tried = true, g = 3 + (g - 3) / 2) {
+    DBuf keys(c, s1.m * sizeof(uint64_t));
+    const uint64_t k = compact(c, s1.m, AtLeast{sup1, s1.ends.as<uint64_t>(), g - 2}, keys.as<uint64_t>());
+    KT_LOG(c, "kt: predict level %u: %llu of %llu edges have support >= %u\n", g, (unsigned long long)k,
+           (unsigned long long)s1.m, g - 2);
+    if (k * 2 > s1.m) {
+      if (!tried) g = std::min(g, half);
+      break;
+    }
+    Sub s;
+    build_sub_from_keys(c, keys.as<uint64_t>(), k, s1.n, s);
+    keys.release();
+    DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
+    edge_support(c, s, sup.as<uint32_t>());
+    PeelResult p = truss_peel(c, s, sup.as<uint32_t>(), g, 0, nullptr);
+    levels += p.levels;
+    rounds += p.rounds;
+    if (p.kmax >= g) {
+      p.levels = levels;
+      p.rounds = rounds;
+      return p;
+    }
+  }
+  KT_LOG(c, "kt: predict peels the whole core, first level %u\n", g);
+  PeelResult p = truss_peel(c, s1, sup1, 3, 0, nullptr, g);
+  p.levels += levels;
+  p.rounds += rounds;
+  return p;
 }
 
 void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) {
@@ -126,8 +150,7 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     edge_support(c, s1, sup1.as<uint32_t>());
     st.ms_support += tm.stop();
     tm.start();
-    // First try half the core number: one cascade removes everything below it.
-    const PeelResult p1 = truss_peel(c, s1, sup1.as<uint32_t>(), 3, 0, nullptr, (cmax + 1) / 2);
+    const PeelResult p1 = predict_peel(c, s1, sup1.as<uint32_t>(), cmax);
     st.ms_peel += tm.stop();
     st.levels += p1.levels;
     st.rounds += (uint32_t)p1.rounds;
@@ -165,17 +188,19 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   DBuf sup3;
   const Sub* sp = &s2;
   uint32_t* supp = sup2.as<uint32_t>();
-  if (capped) {
-    DBuf keys(c, (s2.m ? s2.m : 1) * sizeof(uint64_t));
+  if (t2 > 3 && s2.m) {
+    DBuf keys(c, s2.m * sizeof(uint64_t));
     const uint64_t k = compact(c, s2.m, AtLeast{sup2.as<uint32_t>(), s2.ends.as<uint64_t>(), t2 - 2},
                                keys.as<uint64_t>());
+    KT_LOG(c, "kt: search level %u: %llu of %llu edges have support >= %u\n", t2, (unsigned long long)k,
+           (unsigned long long)s2.m, t2 - 2);
     if (k * 2 < s2.m) {
       build_sub_from_keys(c, keys.as<uint64_t>(), k, s2.n, s3);
       sup3 = DBuf(c, (s3.m ? s3.m : 1) * sizeof(uint32_t));
       edge_support(c, s3, sup3.as<uint32_t>());
       sp = &s3;
       supp = sup3.as<uint32_t>();
-    } else {
+    } else if (capped) {
       edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
     }
   }

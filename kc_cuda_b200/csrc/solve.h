@@ -4,6 +4,28 @@
 
 namespace kt {
 
+// Stream-ordered stage timer: stop() waits for the stage and returns its ms.
+struct Timer {
+  Ctx* c;
+  cudaEvent_t a, b;
+  explicit Timer(Ctx* cx) : c(cx) {
+    KT_CUDA(cudaEventCreate(&a));
+    KT_CUDA(cudaEventCreate(&b));
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { KT_CUDA(cudaEventRecord(a, c->stream)); }
+  double stop() {
+    KT_CUDA(cudaEventRecord(b, c->stream));
+    KT_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    KT_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+};
+
 // Clears the per-solve statistics.
 void begin_solve_stats(Ctx* c);
 void solve_graph(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count);

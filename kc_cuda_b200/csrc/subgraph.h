@@ -41,13 +41,16 @@ void build_sub_all(Ctx* c, const Graph& g, Sub& s);
 void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
                        const uint32_t* rem, const uint32_t* group_of, uint32_t ngroups, Sub& s);
 
-// Per-graph bookkeeping of a batched peel: after every level, each graph
-// with alive edges records (its minimum support + 2, its alive edges).
+// Per-graph bookkeeping of a batched peel: every graph climbs its own
+// levels; after each of its levels a graph with alive edges records (its
+// minimum support + 2, its alive edges).
 struct GraphTrack {
   const uint32_t* vgid;  // graph of each vertex of the working graph
   uint32_t ngroups;
   uint32_t* kmax;        // device [ngroups], last recorded level (0 = none)
   uint64_t* count;       // device [ngroups]
+  const uint32_t* t0 = nullptr;    // device [ngroups]: first level (null/0: the peel's t0)
+  const uint64_t* stop = nullptr;  // device [ngroups]: early-stop edge count (null/0: none)
 };
 
 // support.cu: sup[e] = triangles through edge e (all edges of s).  Uses the
@@ -55,6 +58,11 @@ struct GraphTrack {
 // support is below cap may get any value below cap -- enough for a peel whose
 // first level removes everything below cap.
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap = 0);
+// Upper bound on the largest non-empty truss level, from exact supports: the
+// largest t <= cap with at least t(t-1)/2 edges of support >= t-2 (a
+// non-empty t-truss has t or more vertices, each of degree >= t-1 in it, and
+// each of its edges has support >= t-2).  0 when no t >= 3 qualifies.
+uint32_t support_bound(Ctx* c, const uint32_t* sup, uint64_t m, uint32_t cap);
 // Builds s.bits when the subgraph qualifies for dense mode; returns whether.
 bool build_bits(Ctx* c, Sub& s);
 

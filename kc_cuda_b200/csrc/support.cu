@@ -16,6 +16,8 @@
 // warp per edge, lanes binary-search the shorter row in the longer one.
 #include <algorithm>
 
+#include <vector>
+
 #include "dense.cuh"
 #include "subgraph.h"
 
@@ -176,7 +178,37 @@ __global__ void k_support_alg(uint64_t m, const uint64_t* __restrict__ ends, con
   if (lane_id() == 0 && s) atomicAdd(out, (unsigned long long)s);
 }
 
+// hist[min(sup, cap)] += 1, warp-aggregated over equal bins.
+__global__ void k_sup_hist(const uint32_t* __restrict__ sup, uint64_t m, uint32_t cap,
+                           unsigned long long* __restrict__ hist) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((m + 31) & ~31ULL);
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ok = i < m;
+    const uint32_t b = ok ? min(sup[i], cap) : 0xffffffffu;
+    const unsigned peers = __match_any_sync(kFull, b);
+    if (ok && lane_id() == (unsigned)(__ffs(peers) - 1)) atomicAdd(&hist[b], (unsigned long long)__popc(peers));
+  }
+}
+
 }  // namespace
+
+uint32_t support_bound(Ctx* c, const uint32_t* sup, uint64_t m, uint32_t cap) {
+  if (m == 0 || cap < 3) return 0;
+  DBuf hist(c, ((uint64_t)cap + 1) * 8);
+  zero(c, hist.get(), hist.bytes());
+  k_sup_hist<<<grid_for(m, 256, c->num_sms * 16), 256, 0, c->stream>>>(sup, m, cap,
+                                                                       hist.as<unsigned long long>());
+  KT_LAUNCHED(c);
+  std::vector<unsigned long long> h(cap + 1);
+  copy_d2h(c, h.data(), hist.get(), h.size() * sizeof(unsigned long long));
+  // at_least = edges with support >= t-2, accumulated while t descends.
+  unsigned long long at_least = h[cap] + h[cap - 1];
+  for (uint32_t t = cap; t >= 3; --t) {
+    at_least += h[t - 2];
+    if (at_least >= (unsigned long long)t * (t - 1) / 2) return t;
+  }
+  return 0;
+}
 
 bool build_bits(Ctx* c, Sub& s) {
   s.W = 0;
