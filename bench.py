@@ -1,7 +1,7 @@
 """Benchmark: kmax-truss solve of one large graph per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rmat24|rmat21|rmat16]
+                    [--workload rmat24|rmat21|rmat16|mix4096|serve]
 
 Workload (default rmat24): undirected R-MAT, scale 24 (16.7M vertex ids), edge
 factor 32 (536.9M draws), a/b/c/d = .57/.19/.19/.05, seed 2, cliques of 80,
@@ -21,6 +21,12 @@ The TSV (16 GB) is larger than L2, so no flush is needed between steps.
 Under torchrun each rank solves its own replica on its own GPU (graphs are
 independent units: no data-path collective); the step time is the max over
 ranks and value counts the edges of all ranks.
+
+--workload mix4096: graphs/s of the batched path over graphs 0..4095 of the
+batched mix, beside the one-graph-per-launch path on a sample (run_mix).
+--workload serve: the serving loop under Poisson arrivals of mix graphs at
+0.8 x the batched graphs/s measured in the same run; p50/p99 latency and
+served graphs/s (run_serve).
 
 --impl reference runs the reference's own CPU solver (kc_cpu, built from the
 reference sources into oracle/_ref/) on a bounded sample of the same
@@ -47,6 +53,7 @@ WORKLOADS = {
     "rmat21": (21, 32, 2, [80, 120, 200]),
     "rmat16": (16, 16, 1, [30]),
     "mix4096": None,  # batched: the 4,096-graph mix (see run_mix)
+    "serve": None,    # serving loop under Poisson arrivals (see run_serve)
 }
 # CPU sample of the same family for the reference solver (about 10-30 s).
 CPU_SAMPLE = (20, 32, 2, [80, 120, 200])
@@ -221,8 +228,9 @@ def run_mix(args, world, rank, local, pg):
     answers_alone = {}
     for i in sample:
         g = ctx.load_mix_graph(i)
+        csr_ms = ctx.stats()["ms_csr"]  # the CSR build counts, the generation does not
         answers_alone[i] = g.kmax_truss()
-        lat.append(ctx.stats()["ms_total"])
+        lat.append(csr_ms + ctx.stats()["ms_total"])
         g.free()
     per_graph_gps = len(lat) / (sum(lat) / 1000.0)
     # Batched.
@@ -263,6 +271,71 @@ def run_mix(args, world, rank, local, pg):
     ctx.close()
 
 
+def run_serve(args, world, rank, local, pg):
+    """Serving workload: R requests, request i = graph (offset + i) of the
+    batched mix, Poisson arrivals (fixed seed) at 0.8 x the batched graphs/s
+    measured first on a calibration batch of other mix graphs.  The server
+    admits arrivals into waves as the device frees (kt_server_*).  value =
+    served graphs/s (completed / first submission -> last result); p50/p99
+    latency = submission -> result, measured by the library."""
+    import numpy as np
+
+    import kc_cuda_b200 as K
+    from kc_cuda_b200 import serving
+    R = args.serve_requests
+    base = 1_000_000 + rank * (R + args.calib_graphs)  # away from the graphs of the batched workload
+    calib_first, first = base, base + args.calib_graphs
+    ctx = K.Context(local)
+    # Calibration: batched graphs/s of this device on other mix graphs.
+    b = ctx.batch()
+    b.add_mix(calib_first, min(64, args.calib_graphs))
+    b.run()
+    b.free()
+    b = ctx.batch()
+    b.add_mix(calib_first, args.calib_graphs)
+    b.run()
+    st = ctx.stats()
+    b.free()
+    calib_gps = args.calib_graphs / ((st["ms_total"] - st["ms_parse"]) / 1000.0)
+    rate = args.serve_rate if args.serve_rate > 0 else 0.8 * calib_gps
+    arrivals = serving.poisson_arrivals(R, rate, seed=55 + rank)
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        srv = ctx.server()
+        submitted = serving.drive(arrivals, lambda i: srv.submit_mix(first + i))
+        results = [srv.wait(rid) for rid, _ in submitted]
+        sst = srv.stats()
+        srv.close()
+    assert all(r["status"] == 0 for r in results)
+    summ = serving.summarize(submitted, results)
+    # Alone vs served on a sample of the requests.
+    mism = 0
+    for j in range(0, R, max(1, R // 16)):
+        g = ctx.load_mix_graph(first + j)
+        if g.kmax_truss() != (results[j]["kmax"], results[j]["edges"]):
+            mism += 1
+        g.free()
+    span = max_over_ranks(pg, summ["span_s"])
+    total = sum_over_ranks(pg, float(R))
+    p99 = max_over_ranks(pg, summ["p99_ms"])
+    if rank == 0:
+        print(json.dumps({
+            "metric": "served kmax-truss graphs/s with p50/p99 latency (Poisson arrivals of mix graphs)",
+            "value": total / span, "unit": "graphs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": span * 1000.0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"serve{R}", "requests": R, "first_graph": first,
+                       "arrival_rate_per_s": rate, "calibration_graphs_per_s": calib_gps,
+                       "calibration_graphs": args.calib_graphs, "arrival_seed": 55 + rank},
+            "latency": {"p50_ms": summ["p50_ms"], "p99_ms": p99, "mean_ms": summ["mean_ms"],
+                        "max_ms": summ["max_ms"], "wait_p50_ms": summ["wait_p50_ms"]},
+            "waves": sst["waves"], "mean_wave_graphs": summ["mean_wave_graphs"],
+            "max_wave_graphs": sst["max_wave_graphs"], "device_bytes_peak": sst["device_bytes_peak"],
+            "alone_vs_served_mismatches": mism, "clocks": clk.summary(),
+        }))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -273,10 +346,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mix-graphs", type=int, default=4096)
     ap.add_argument("--sample-every", type=int, default=32)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="requests/s (0: 0.8 x calibrated batched)")
+    ap.add_argument("--calib-graphs", type=int, default=512)
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
-    if args.workload == "mix4096" and args.impl == "ours":
-        run_mix(args, world, rank, local, pg)
+    if args.workload in ("mix4096", "serve") and args.impl == "ours":
+        (run_mix if args.workload == "mix4096" else run_serve)(args, world, rank, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -129,8 +129,47 @@ kt_status kt_batch_run(kt_batch* b);
 kt_status kt_batch_results(const kt_batch* b, uint32_t* kmax, uint64_t* edges);
 void kt_batch_free(kt_batch* b);
 /* Graph `index` of the batched mix, generated on the device (the per-graph
- * path's input, identical to the batch's). */
+ * path's input, identical to the batch's); kt_get_stats: ms_parse = the
+ * generation, ms_csr = the CSR build. */
 kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_graph** out);
+
+/* ----------------------------------------------------------------- serve */
+
+/* A continuous-batching serving loop (no counterpart in the reference).
+ * Requests are submitted from any thread at any time and queue in arrival
+ * order; a worker thread, which owns the context while the server lives,
+ * admits queued requests oldest first while their estimated device footprint
+ * fits half of the context's free budget (and at most max_wave_graphs of
+ * them, 0 = 65535) and solves them as one wave of the batch path; requests
+ * that arrive meanwhile join the next wave.  A request's answer is the same
+ * alone and in any mix.  Other calls on the context block while a wave runs. */
+typedef struct kt_server kt_server;
+typedef struct kt_request_result {
+  kt_status status;      /* KT_OK, or the error of the wave that held it */
+  uint32_t kmax;
+  uint64_t edges;        /* kmax-truss edge count */
+  double ms_wait;        /* submission -> admission into a wave (host clock) */
+  double ms_latency;     /* submission -> result available */
+  uint32_t wave;         /* the wave that solved it (0, 1, ...) */
+  uint32_t wave_graphs;  /* requests solved in that wave */
+} kt_request_result;
+typedef struct kt_server_stats {
+  uint64_t submitted, completed, pending, waves, max_wave_graphs;
+  double ms_busy;              /* worker time inside waves */
+  uint64_t device_bytes_peak;  /* the context's peak device memory */
+} kt_server_stats;
+kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** out);
+/* Queues a graph given as records x << 32 | y (copied).  KT_ERR_LIMIT if its
+ * footprint alone exceeds what a wave may hold. */
+kt_status kt_server_submit_pairs(kt_server* s, const uint64_t* xy, uint64_t count, uint64_t* request_id);
+/* Queues graph `index` of the batched mix (generated on the device). */
+kt_status kt_server_submit_mix(kt_server* s, uint64_t index, uint64_t base_seed, uint64_t* request_id);
+/* A request's result; waits up to timeout_ms (0 = do not wait) and returns
+ * KT_ERR_TIMEOUT while it is still pending. */
+kt_status kt_server_wait(kt_server* s, uint64_t request_id, uint32_t timeout_ms, kt_request_result* out);
+kt_status kt_server_get_stats(kt_server* s, kt_server_stats* out);
+/* Finishes every queued request, stops the worker and frees the server. */
+void kt_server_destroy(kt_server* s);
 
 /* ------------------------------------------------------- stage outputs */
 

@@ -12,24 +12,9 @@
 #include <cstring>
 #include <new>
 
-#include "kt.h"
-#include "batch.h"
+#include "handles.h"
 #include "solve.h"
 
-struct kt_ctx {
-  kt::Ctx c;
-};
-struct kt_graph {
-  kt::Graph g;
-};
-struct kt_tsv {
-  kt::DBuf bytes;
-  uint64_t len = 0;
-};
-struct kt_batch {
-  kt_ctx* ctx = nullptr;
-  std::vector<kt::BatchItem> items;
-};
 
 namespace kt {
 
@@ -205,27 +190,6 @@ static void load_tsv_file(Ctx* c, const char* path, Graph& g) {
 }  // namespace kt
 
 using kt::Error;
-
-#define KT_API_BEGIN(ctx)                            \
-  if (!(ctx)) return KT_ERR_INVALID;                 \
-  std::lock_guard<std::recursive_mutex> lk_((ctx)->c.mu); \
-  try {                                              \
-    KT_CUDA(cudaSetDevice((ctx)->c.device));
-#define KT_API_END(ctx)                              \
-  return KT_OK;                                      \
-  }                                                  \
-  catch (const Error& e) {                           \
-    (ctx)->c.last_error = e.what();                  \
-    return e.status;                                 \
-  }                                                  \
-  catch (const std::bad_alloc&) {                    \
-    (ctx)->c.last_error = "host allocation failed";  \
-    return KT_ERR_NOMEM;                             \
-  }                                                  \
-  catch (const std::exception& e) {                  \
-    (ctx)->c.last_error = e.what();                  \
-    return KT_ERR_CUDA;                              \
-  }
 
 extern "C" {
 

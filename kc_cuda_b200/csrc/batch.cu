@@ -234,67 +234,144 @@ static uint64_t wave_keys(Ctx* c, const std::vector<BatchItem*>& items, DBuf& ke
   return vbase[G];
 }
 
-// One union stage: the subgraph of vertices whose core reaches need[graph],
-// its support and its tracked peel, graph g from level t0[g] (empty: 3) with
-// early stop at stop[g] edges (empty: none); kmax/count receive the
-// per-graph records.
-static void union_truss(Ctx* c, const Graph& U, const uint32_t* dcore, const uint32_t* dgid, uint32_t G,
-                        const std::vector<uint32_t>& need, const std::vector<uint32_t>& t0,
-                        const std::vector<uint64_t>& stop, std::vector<uint32_t>& kmax, std::vector<uint64_t>& count,
-                        kt_stats& st) {
-  Timer tm(c);
-  tm.start();
+// Union working graph: the vertices of graph g whose core number reaches
+// need[g] (0 = none of g), grouped by graph.
+static void union_sub(Ctx* c, const Graph& U, const uint32_t* dcore, const uint32_t* dgid, uint32_t G,
+                      const std::vector<uint32_t>& need, Sub& s) {
   DBuf dneed(c, G * sizeof(uint32_t));
   copy_h2d(c, dneed.get(), need.data(), G * sizeof(uint32_t));
   DBuf list(c, (U.n ? U.n : 1) * sizeof(uint32_t));
   const uint64_t na = compact(c, U.n, CoreAtLeast{dcore, dgid, dneed.as<uint32_t>()}, list.as<uint32_t>());
-  kmax.assign(G, 0);
-  count.assign(G, 0);
-  if (na == 0) return;
-  DBuf rem(c, U.n * sizeof(uint32_t)), deg(c, U.n * sizeof(uint32_t));
+  DBuf rem(c, (U.n ? U.n : 1) * sizeof(uint32_t)), deg(c, (U.n ? U.n : 1) * sizeof(uint32_t));
   zero(c, rem.get(), rem.bytes());
-  k_mark<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(list.as<uint32_t>(), na, rem.as<uint32_t>());
-  KT_LAUNCHED(c);
-  k_alive_degree<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      list.as<uint32_t>(), na, U.off.as<uint64_t>(), U.adj.as<uint32_t>(), rem.as<uint32_t>(), deg.as<uint32_t>());
-  KT_LAUNCHED(c);
-  Sub s;
+  if (na) {
+    k_mark<<<grid_for(na, 256, c->num_sms * 16), 256, 0, c->stream>>>(list.as<uint32_t>(), na, rem.as<uint32_t>());
+    KT_LAUNCHED(c);
+    k_alive_degree<<<grid_for(na * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        list.as<uint32_t>(), na, U.off.as<uint64_t>(), U.adj.as<uint32_t>(), rem.as<uint32_t>(),
+        deg.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
   build_sub_grouped(c, U, list.as<uint32_t>(), na, deg.as<uint32_t>(), rem.as<uint32_t>(), dgid, G, s);
-  list.release();
-  rem.release();
-  deg.release();
-  st.core_vertices += s.n;
-  st.core_edges += s.m;
-  st.ms_subgraph += tm.stop();
-  if (s.m == 0) return;
-  tm.start();
-  DBuf sup(c, s.m * sizeof(uint32_t));
-  edge_support(c, s, sup.as<uint32_t>());
-  st.ms_support += tm.stop();
-  tm.start();
-  DBuf dk(c, G * sizeof(uint32_t)), dc(c, G * sizeof(uint64_t));
-  zero(c, dk.get(), dk.bytes());
-  zero(c, dc.get(), dc.bytes());
-  GraphTrack tr{s.vgid.as<uint32_t>(), G, dk.as<uint32_t>(), dc.as<uint64_t>()};
-  DBuf dt0, dstop;
-  if (!t0.empty()) {
-    dt0.alloc(c, G * sizeof(uint32_t));
-    copy_h2d(c, dt0.get(), t0.data(), G * sizeof(uint32_t));
-    tr.t0 = dt0.as<uint32_t>();
-  }
-  if (!stop.empty()) {
-    dstop.alloc(c, G * sizeof(uint64_t));
-    copy_h2d(c, dstop.get(), stop.data(), G * sizeof(uint64_t));
-    tr.stop = dstop.as<uint64_t>();
-  }
-  const PeelResult pr = truss_peel(c, s, sup.as<uint32_t>(), 3, 0, nullptr, 0, &tr);
-  st.levels += pr.levels;
-  st.rounds += (uint32_t)pr.rounds;
-  copy_d2h(c, kmax.data(), dk.get(), G * sizeof(uint32_t));
-  copy_d2h(c, count.data(), dc.get(), G * sizeof(uint64_t));
-  st.ms_peel += tm.stop();
 }
 
+// Edges of graph thr's group with support >= thr[group] (thr 0: none).
+struct GroupAtLeast {
+  const uint32_t* sup;
+  const uint64_t* ends;
+  const uint32_t* vgid;
+  const uint32_t* thr;
+  __device__ bool keep(uint64_t e) const {
+    const uint32_t t = thr[vgid[(uint32_t)(ends[e] >> 32)]];
+    return t && sup[e] >= t;
+  }
+  __device__ uint64_t value(uint64_t e) const { return ends[e]; }
+};
+
+// Per-graph support histograms: hist[hoff[g] + min(sup, cap[g])] += 1.
+__global__ void k_group_hist(const uint32_t* __restrict__ sup, const uint64_t* __restrict__ ends, uint64_t m,
+                             const uint32_t* __restrict__ vgid, const uint32_t* __restrict__ hoff,
+                             const uint32_t* __restrict__ cap, unsigned long long* __restrict__ hist) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ((m + 31) & ~31ULL);
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ok = e < m;
+    uint32_t b = 0xffffffffu;
+    if (ok) {
+      const uint32_t g = vgid[(uint32_t)(ends[e] >> 32)];
+      b = hoff[g] + min(sup[e], cap[g]);
+    }
+    const unsigned peers = __match_any_sync(kFull, b);
+    if (ok && lane_id() == (unsigned)(__ffs(peers) - 1)) atomicAdd(&hist[b], (unsigned long long)__popc(peers));
+  }
+}
+
+// Per-graph support bounds (the single-graph rule: largest t <= cap[g] with
+// t(t-1)/2 edges of support >= t-2; 0 if none) over a grouped union.
+static std::vector<uint32_t> group_bounds(Ctx* c, const Sub& s, const uint32_t* sup, const std::vector<uint32_t>& cap) {
+  const uint32_t G = (uint32_t)cap.size();
+  std::vector<uint32_t> hoff(G + 1, 0), out(G, 0);
+  for (uint32_t g = 0; g < G; ++g) hoff[g + 1] = hoff[g] + cap[g] + 1;
+  if (s.m == 0) return out;
+  DBuf dh(c, (uint64_t)hoff[G] * 8), doff(c, G * 4ull), dcap(c, G * 4ull);
+  zero(c, dh.get(), dh.bytes());
+  copy_h2d(c, doff.get(), hoff.data(), G * 4ull);
+  copy_h2d(c, dcap.get(), cap.data(), G * 4ull);
+  k_group_hist<<<grid_for(s.m, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      sup, s.ends.as<uint64_t>(), s.m, s.vgid.as<uint32_t>(), doff.as<uint32_t>(), dcap.as<uint32_t>(),
+      dh.as<unsigned long long>());
+  KT_LAUNCHED(c);
+  std::vector<unsigned long long> h(hoff[G]);
+  copy_d2h(c, h.data(), dh.get(), h.size() * 8);
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint32_t cp = cap[g];
+    if (cp < 3) continue;
+    const unsigned long long* hg = h.data() + hoff[g];
+    unsigned long long at_least = hg[cp] + hg[cp - 1];
+    for (uint32_t t = cp; t >= 3; --t) {
+      at_least += hg[t - 2];
+      if (at_least >= (unsigned long long)t * (t - 1) / 2) {
+        out[g] = t;
+        break;
+      }
+    }
+  }
+  return out;
+}
+
+// Survivors: the union of each graph's edges with support >= thr[g],
+// rebuilt as a grouped working graph with exact supports.  When `only_if_few`
+// and they are not fewer than half the edges, nothing is built (false).
+static bool survivors(Ctx* c, const Sub& s, const uint32_t* sup, const std::vector<uint32_t>& thr, bool only_if_few,
+                      Sub& out, DBuf& out_sup) {
+  const uint32_t G = (uint32_t)thr.size();
+  DBuf dthr(c, G * 4ull);
+  copy_h2d(c, dthr.get(), thr.data(), G * 4ull);
+  DBuf keys(c, (s.m ? s.m : 1) * sizeof(uint64_t));
+  const uint64_t k = compact(c, s.m, GroupAtLeast{sup, s.ends.as<uint64_t>(), s.vgid.as<uint32_t>(),
+                                                  dthr.as<uint32_t>()},
+                             keys.as<uint64_t>());
+  KT_LOG(c, "kt: batch survivors: %llu of %llu edges\n", (unsigned long long)k, (unsigned long long)s.m);
+  if (only_if_few && k * 2 >= s.m) return false;
+  build_sub_grouped_from_keys(c, keys.as<uint64_t>(), k, s.n, s.vgid.as<uint32_t>(), G, out);
+  keys.release();
+  out_sup = DBuf(c, (out.m ? out.m : 1) * sizeof(uint32_t));
+  edge_support(c, out, out_sup.as<uint32_t>());
+  return true;
+}
+
+// Tracked peel of a grouped union: graph g from level t0[g] with early stop
+// at stop[g] edges (0: none); returns each graph's last recorded level and
+// its edge count.
+static void tracked_peel(Ctx* c, const Sub& s, uint32_t* sup, const std::vector<uint32_t>& t0,
+                         const std::vector<uint64_t>& stop, std::vector<uint32_t>& kmax,
+                         std::vector<uint64_t>& count) {
+  const uint32_t G = (uint32_t)t0.size();
+  kmax.assign(G, 0);
+  count.assign(G, 0);
+  if (s.m == 0) return;
+  DBuf dk(c, G * sizeof(uint32_t)), dc(c, G * sizeof(uint64_t)), dt0(c, G * sizeof(uint32_t)),
+      dstop(c, G * sizeof(uint64_t));
+  zero(c, dk.get(), dk.bytes());
+  zero(c, dc.get(), dc.bytes());
+  copy_h2d(c, dt0.get(), t0.data(), G * sizeof(uint32_t));
+  copy_h2d(c, dstop.get(), stop.data(), G * sizeof(uint64_t));
+  GraphTrack tr{s.vgid.as<uint32_t>(), G, dk.as<uint32_t>(), dc.as<uint64_t>(), dt0.as<uint32_t>(),
+                dstop.as<uint64_t>()};
+  const PeelResult pr = truss_peel(c, s, sup, 3, 0, nullptr, 0, &tr);
+  c->stats.levels += pr.levels;
+  c->stats.rounds += (uint32_t)pr.rounds;
+  copy_d2h(c, kmax.data(), dk.get(), G * sizeof(uint32_t));
+  copy_d2h(c, count.data(), dc.get(), G * sizeof(uint64_t));
+}
+
+// One wave: the two phases of the single-graph driver, each graph on its own
+// levels, all graphs of the wave in each launch.
+//   1. On the union of maximum cores: per-graph support bounds; graph g tries
+//      level min(bound, (cmax+1)/2) on its edges of support >= level-2
+//      (rebuilt), halving toward 3 while that truss is empty.
+//   2. On the union of (L-1)-cores of the graphs whose bound L = cmax + 1 is
+//      not met: edges of support >= L-2, peeled from L with early stop at
+//      phase 1's count.
 void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   const uint32_t G = (uint32_t)items.size();
   kt_stats& st = c->stats;
@@ -334,44 +411,112 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   std::vector<uint32_t> cmax(G);
   copy_d2h(c, cmax.data(), dcm.get(), G * sizeof(uint32_t));
   st.ms_kcore += tm.stop();
-  // Phase 1: the maximum core of every graph that can hold a triangle.
-  std::vector<uint32_t> need(G, 0);
-  for (uint32_t g = 0; g < G; ++g) need[g] = cmax[g] >= 2 ? cmax[g] : 0;
-  std::vector<uint32_t> k1;
-  std::vector<uint64_t> c1;
-  union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, {}, {}, k1, c1, st);
-  // Phase 2: the (L-1)-core of every graph whose bound is not met, peeled
-  // from level L with early stop at phase 1's count.
-  bool any = false;
-  std::vector<uint32_t> t0(G, 3);
+
+  // Phase 1.
+  std::vector<uint32_t> L(G, 0);
+  std::vector<uint64_t> C(G, 0);
+  {
+    tm.start();
+    std::vector<uint32_t> need(G, 0), cap(G, 0);
+    for (uint32_t g = 0; g < G; ++g)
+      if (cmax[g] >= 2) {
+        need[g] = cmax[g];
+        cap[g] = cmax[g] + 1;
+      }
+    Sub s1;
+    union_sub(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, s1);
+    st.predict_vertices += s1.n;
+    st.predict_edges += s1.m;
+    st.ms_subgraph += tm.stop();
+    tm.start();
+    DBuf sup1(c, (s1.m ? s1.m : 1) * sizeof(uint32_t));
+    edge_support(c, s1, sup1.as<uint32_t>());
+    const std::vector<uint32_t> ub = group_bounds(c, s1, sup1.as<uint32_t>(), cap);
+    st.ms_support += tm.stop();
+    tm.start();
+    std::vector<uint32_t> level(G, 0);
+    bool pending = false;
+    for (uint32_t g = 0; g < G; ++g)
+      if (ub[g] >= 3) {
+        level[g] = std::max<uint32_t>(3, std::min<uint32_t>(ub[g], (cmax[g] + 1) / 2));
+        pending = true;
+      }
+    const std::vector<uint64_t> nostop(G, 0);
+    while (pending) {
+      std::vector<uint32_t> thr(G, 0);
+      for (uint32_t g = 0; g < G; ++g) thr[g] = level[g] ? level[g] - 2 : 0;
+      Sub s;
+      DBuf sup;
+      survivors(c, s1, sup1.as<uint32_t>(), thr, false, s, sup);
+      std::vector<uint32_t> km;
+      std::vector<uint64_t> cn;
+      tracked_peel(c, s, sup.as<uint32_t>(), level, nostop, km, cn);
+      pending = false;
+      for (uint32_t g = 0; g < G; ++g) {
+        if (!level[g]) continue;
+        if (km[g] >= level[g]) {
+          L[g] = km[g];
+          C[g] = cn[g];
+          level[g] = 0;
+        } else if (level[g] == 3) {
+          level[g] = 0;
+        } else {
+          level[g] = 3 + (level[g] - 3) / 2;
+          pending = true;
+        }
+      }
+    }
+    st.ms_peel += tm.stop();
+  }
+
+  // Phase 2.
+  std::vector<uint32_t> need(G, 0), t0(G, 3);
   std::vector<uint64_t> stop(G, 0);
+  bool any = false;
   for (uint32_t g = 0; g < G; ++g) {
     items[g]->kmax = 0;
     items[g]->count = 0;
-    need[g] = 0;
     if (cmax[g] < 2) continue;
-    const uint32_t L = k1[g] >= 3 ? k1[g] : 0;
-    if (L && L == cmax[g] + 1) {
-      items[g]->kmax = L;
-      items[g]->count = c1[g];
+    if (L[g] >= 3 && L[g] == cmax[g] + 1) {
+      items[g]->kmax = L[g];
+      items[g]->count = C[g];
       continue;
     }
-    need[g] = L ? L - 1 : 2;
-    if (L) {
-      t0[g] = L;
-      stop[g] = c1[g];
+    need[g] = L[g] >= 3 ? L[g] - 1 : 2;
+    if (L[g] >= 3) {
+      t0[g] = L[g];
+      stop[g] = C[g];
     }
     any = true;
   }
-  if (any) {
-    std::vector<uint32_t> k2;
-    std::vector<uint64_t> c2;
-    union_truss(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, t0, stop, k2, c2, st);
-    for (uint32_t g = 0; g < G; ++g) {
-      if (!need[g]) continue;
-      items[g]->kmax = k2[g] >= 3 ? k2[g] : 0;
-      items[g]->count = k2[g] >= 3 ? c2[g] : 0;
-    }
+  if (!any) return;
+  tm.start();
+  Sub s2;
+  union_sub(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, s2);
+  st.core_vertices += s2.n;
+  st.core_edges += s2.m;
+  st.ms_subgraph += tm.stop();
+  tm.start();
+  DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
+  edge_support(c, s2, sup2.as<uint32_t>());
+  std::vector<uint32_t> thr(G, 0);
+  for (uint32_t g = 0; g < G; ++g) thr[g] = need[g] ? t0[g] - 2 : 0;
+  Sub s3;
+  DBuf sup3;
+  const bool rebuilt = survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
+  st.ms_support += tm.stop();
+  tm.start();
+  std::vector<uint32_t> km;
+  std::vector<uint64_t> cn;
+  if (rebuilt)
+    tracked_peel(c, s3, sup3.as<uint32_t>(), t0, stop, km, cn);
+  else
+    tracked_peel(c, s2, sup2.as<uint32_t>(), t0, stop, km, cn);
+  st.ms_peel += tm.stop();
+  for (uint32_t g = 0; g < G; ++g) {
+    if (!need[g]) continue;
+    items[g]->kmax = km[g] >= 3 ? km[g] : 0;
+    items[g]->count = km[g] >= 3 ? cn[g] : 0;
   }
 }
 
@@ -379,18 +524,25 @@ void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
   // Waves: consecutive graphs while the estimated footprint fits half the
   // free budget (keys, sort buffers, CSR, k-core state ~ 48 B per key and
   // 40 B per vertex), the union stays below 2^28 vertices and 65536 graphs.
+  // Graphs are taken in ascending size, so a wave's graphs are alike and its
+  // per-graph structures (support bitmaps) are sized for graphs like them.
   const uint64_t budget = (c->budget > c->in_use ? c->budget - c->in_use : 0) / 2;
+  std::vector<size_t> order(items.size());
+  std::iota(order.begin(), order.end(), size_t(0));
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    return items[a].n != items[b].n ? items[a].n < items[b].n : items[a].nkeys < items[b].nkeys;
+  });
   size_t i = 0;
   out.waves = 0;
   while (i < items.size()) {
     std::vector<BatchItem*> wave;
     uint64_t bytes = 0, verts = 0;
     while (i < items.size()) {
-      const BatchItem& it = items[i];
+      const BatchItem& it = items[order[i]];
       const uint64_t b = 48 * it.nkeys + 40 * it.n;
       if (!wave.empty() && (bytes + b > budget || verts + it.n >= (1ull << 28) || wave.size() >= 65535)) break;
       if (it.n >= (1ull << 28)) throw Error(KT_ERR_LIMIT, "batch: a graph with 2^28 or more vertex ids");
-      wave.push_back(&items[i]);
+      wave.push_back(&items[order[i]]);
       bytes += b;
       verts += it.n;
       ++i;
@@ -407,8 +559,13 @@ void load_mix_graph(Ctx* c, uint64_t index, uint64_t base_seed, Graph& g) {
   DBuf keys;
   uint64_t nkeys = 0;
   std::vector<uint64_t> vbase;
+  KT_CUDA(cudaEventRecord(c->ev[4], c->stream));
   const uint64_t nv = wave_keys(c, one, keys, nkeys, vbase);
+  KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
   build_graph(c, keys.as<uint64_t>(), nkeys, nv, g);
+  KT_CUDA(cudaEventRecord(c->ev[6], c->stream));
+  c->stats.ms_parse = event_ms(c->ev[4], c->ev[5]);
+  c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
 }
 
 }  // namespace kt

@@ -40,6 +40,10 @@ void build_sub_all(Ctx* c, const Graph& g, Sub& s);
 // (g.n < 2^28); within a graph, ascending (degree, id).
 void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na, const uint32_t* deg,
                        const uint32_t* rem, const uint32_t* group_of, uint32_t ngroups, Sub& s);
+// The same from edge keys u << 32 | v (ids below n_ids, group_of indexed by
+// them; keys consumed).
+void build_sub_grouped_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, const uint32_t* group_of,
+                                 uint32_t ngroups, Sub& s);
 
 // Per-graph bookkeeping of a batched peel: every graph climbs its own
 // levels; after each of its levels a graph with alive edges records (its

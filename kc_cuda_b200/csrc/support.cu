@@ -25,11 +25,12 @@ namespace kt {
 namespace {
 
 constexpr unsigned kSupThreads = 256;
+constexpr unsigned kSupThreadsWide = 1024;  // bitmap kernel when its bitmap limits blocks per SM
 
 // Batched unions: the bitmap covers only v's own graph, bits indexed from
 // vbase[v] (graphs are contiguous and no edge crosses graphs); `range` =
 // most vertices of one graph.
-__global__ void __launch_bounds__(kSupThreads) k_support_bitmap(uint32_t n, const uint64_t* __restrict__ off,
+__global__ void __launch_bounds__(kSupThreadsWide) k_support_bitmap(uint32_t n, const uint64_t* __restrict__ off,
                                                                 const uint32_t* __restrict__ adj,
                                                                 const uint32_t* __restrict__ eid,
                                                                 const uint64_t* __restrict__ up,
@@ -253,13 +254,15 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
     const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
       KT_CUDA(cudaFuncSetAttribute(k_support_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // Large bitmaps leave room for few blocks per SM: then wider blocks.
+    const unsigned threads = smem > 24 * 1024 ? kSupThreadsWide : kSupThreads;
     int per_sm = 0;
-    KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_support_bitmap, kSupThreads, smem));
+    KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_support_bitmap, threads, smem));
     if (per_sm < 1) throw Error(KT_ERR_LIMIT, "support: bitmap does not fit in shared memory");
     DBuf cur(c, 8);
     zero(c, cur.get(), 8);
     const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * c->num_sms, s.n);
-    k_support_bitmap<<<grid, kSupThreads, smem, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
+    k_support_bitmap<<<grid, threads, smem, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
                                                              s.eid.as<uint32_t>(), s.up.as<uint64_t>(), sup,
                                                              cur.as<unsigned long long>(),
                                                              s.vbase.get() ? s.vbase.as<uint32_t>() : nullptr,

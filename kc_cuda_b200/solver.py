@@ -56,6 +56,28 @@ class Stats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int), ("kmax", ctypes.c_uint32), ("edges", ctypes.c_uint64),
+        ("ms_wait", ctypes.c_double), ("ms_latency", ctypes.c_double),
+        ("wave", ctypes.c_uint32), ("wave_graphs", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("pending", ctypes.c_uint64),
+        ("waves", ctypes.c_uint64), ("max_wave_graphs", ctypes.c_uint64),
+        ("ms_busy", ctypes.c_double), ("device_bytes_peak", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _LIB = None
 
 # (name, restype, argtypes) of every entry point of include/kt.h.
@@ -93,6 +115,12 @@ SIGNATURES = [
     ("kt_core_numbers", ctypes.c_int, [_P, _P, _U32P]),
     ("kt_edge_support", ctypes.c_int, [_P, _P, _U32P]),
     ("kt_edge_trussness", ctypes.c_int, [_P, _P, _U32P]),
+    ("kt_server_create", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
+    ("kt_server_submit_pairs", ctypes.c_int, [_P, _U64P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("kt_server_submit_mix", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("kt_server_wait", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(RequestResult)]),
+    ("kt_server_get_stats", ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
+    ("kt_server_destroy", None, [_P]),
     ("kt_get_stats", ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
     ("kt_stats_reset", ctypes.c_int, [_P]),
 ]
@@ -212,6 +240,9 @@ class Context:
     def batch(self) -> "Batch":
         return Batch(self)
 
+    def server(self, max_wave_graphs: int = 0) -> "Server":
+        return Server(self, max_wave_graphs)
+
     # ---- one-call solve
     def solve_tsv(self, data) -> Tuple[int, int]:
         p, n, keep = _buf(data)
@@ -267,6 +298,65 @@ class Batch:
         e = np.zeros(max(n, 1), dtype=np.uint64)
         self.ctx.check(self.ctx._L.kt_batch_results(self._h, k.ctypes.data, e.ctypes.data))
         return k[:n], e[:n]
+
+
+class Server:
+    """Continuous-batching serving loop on a context (kt_server_*): submit
+    graphs at any time, collect each result with its latency."""
+
+    def __init__(self, ctx: Context, max_wave_graphs: int = 0):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx.check(ctx._L.kt_server_create(ctx._h, max_wave_graphs, ctypes.byref(h)))
+        self._h = h
+
+    def _check(self, s: int):
+        if s != KT_OK:
+            raise KtError(s, STATUS.get(s, str(s)))
+
+    def submit_pairs(self, xy: np.ndarray) -> int:
+        xy = np.ascontiguousarray(xy, dtype=np.uint64)
+        rid = ctypes.c_uint64()
+        self._check(self.ctx._L.kt_server_submit_pairs(self._h, xy.ctypes.data if xy.size else None, xy.size,
+                                                       ctypes.byref(rid)))
+        return rid.value
+
+    def submit_mix(self, index: int, base_seed: int = 0x4B54) -> int:
+        rid = ctypes.c_uint64()
+        self._check(self.ctx._L.kt_server_submit_mix(self._h, index, base_seed, ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int) -> Optional[dict]:
+        """The request's result, or None while it is pending."""
+        return self.wait(rid, 0)
+
+    def wait(self, rid: int, timeout_ms: int = 600_000) -> Optional[dict]:
+        r = RequestResult()
+        s = self.ctx._L.kt_server_wait(self._h, rid, timeout_ms, ctypes.byref(r))
+        if s == 6:  # KT_ERR_TIMEOUT: still pending
+            return None
+        self._check(s)
+        return r.as_dict()
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._check(self.ctx._L.kt_server_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        """Finishes every queued request and stops the worker."""
+        if getattr(self, "_h", None):
+            self.ctx._L.kt_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class StagedTsv:
