@@ -129,14 +129,16 @@ def have_kc_cpu() -> bool:
     return os.access(kc_cpu_path(), os.X_OK)
 
 
-def run_kc_cpu(path: str, threads: Optional[int] = None, timeout: float = 600) -> Tuple[int, int]:
+def run_kc_cpu(path: str, threads: Optional[int] = None, timeout: float = 600,
+               binary: Optional[str] = None) -> Tuple[int, int]:
     """Runs the reference CPU solver on a TSV file and parses its answer.  A
-    stand-in `vmtouch` (the reference shells out to it) goes first on PATH."""
+    stand-in `vmtouch` (the reference shells out to it) goes first on PATH.
+    binary: another build of it (e.g. oracle/_ref/kc_cpu_large)."""
     env = dict(os.environ)
     env["PATH"] = HERE + os.pathsep + env.get("PATH", "")
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    p = subprocess.run([kc_cpu_path(), "-f", path], capture_output=True, env=env, timeout=timeout)
+    p = subprocess.run([binary or kc_cpu_path(), "-f", path], capture_output=True, env=env, timeout=timeout)
     if p.returncode != 0:
         raise RuntimeError(f"kc_cpu failed ({p.returncode}): {p.stderr[-400:]!r}")
     m = RESULT_RE.search(p.stdout)

@@ -1,0 +1,99 @@
+"""Full-size parity of the single-graph configurations against the
+reference's own CPU solver (run by hand on the GPU host; too large for the
+test suite):
+
+    python tests/large_parity.py [--configs 2 3] [--dir /dev/shm] [--record]
+
+For each configuration: the seeded graph is generated and written as the
+reference's TSV; the drop-in CLI (kc_cuda_b200/kt_solve -f) and kc_cpu (all
+host cores; kc_cpu_large, the build with raised input limits, when the input
+is beyond kc_cpu's own) solve the same file; the answers must be equal.
+--record writes the answers and wall times to tests/golden/large_configs.json,
+which the bench checks its answer against.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import kt_oracle as O  # noqa: E402
+from kc_cuda_b200 import gen  # noqa: E402
+
+CONFIGS = {
+    1: ("rmat16_ef16_seed1_k30", gen.rmat_s16_k30),
+    2: ("rmat24_ef32_seed2_k80_120_200", gen.rmat_s24_ef32_k80_120_200),
+    3: ("chunglu_n50m_g2.1_wmax2m_seed3_block150", gen.chunglu_50m),
+}
+RECORD = os.path.join(ROOT, "tests", "golden", "large_configs.json")
+CLI = os.path.join(ROOT, "kc_cuda_b200", "kt_solve")
+RESULT_RE = re.compile(r"kmax = (\d+), Edges in kmax-truss = (\d+)\.")
+
+
+def run_cli(path: str):
+    t = time.perf_counter()
+    p = subprocess.run([CLI, "-f", path], capture_output=True, text=True, timeout=3600)
+    wall = time.perf_counter() - t
+    if p.returncode != 0:
+        raise RuntimeError(f"kt_solve failed ({p.returncode}): {p.stderr[-400:]}")
+    m = RESULT_RE.search(p.stdout)
+    return (int(m.group(1)), int(m.group(2))), wall
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--configs", type=int, nargs="+", default=[2, 3])
+    ap.add_argument("--dir", default="/dev/shm")
+    ap.add_argument("--record", action="store_true")
+    ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--reference-only", action="store_true", help="no GPU: record kc_cpu's answers only")
+    a = ap.parse_args()
+    rec = json.load(open(RECORD)) if os.path.exists(RECORD) else {}
+    ok = True
+    for cfg in a.configs:
+        name, spec_fn = CONFIGS[cfg]
+        t = time.perf_counter()
+        g = gen.Graph(spec_fn(), threads=a.threads)
+        path = os.path.join(a.dir, f"kt_cfg{cfg}.tsv")
+        g.write_tsv(path, threads=a.threads)
+        n, m, size = g.num_vertices, g.num_edges, os.path.getsize(path)
+        del g
+        t_gen = time.perf_counter() - t
+        ours, wall_ours = (None, None) if a.reference_only else run_cli(path)
+        lines = 2 * m
+        large = lines > 1_700_000_000 or 2 * m >= (1 << 31) - (1 << 24)
+        binary = os.path.join(O.REF, "kc_cpu_large" if large else "kc_cpu")
+        subprocess.run(["cat", path], stdout=subprocess.DEVNULL, check=True)  # page cache, as vmtouch would
+        t = time.perf_counter()
+        ref = O.run_kc_cpu(path, threads=a.threads, timeout=7200, binary=binary)
+        wall_ref = time.perf_counter() - t
+        os.unlink(path)
+        prev = rec.get(name, {})
+        if ours is None and prev.get("ours"):
+            ours, wall_ours = tuple(prev["ours"]), prev.get("ours_cli_wall_s")
+        same = ours == ref if ours is not None else None
+        ok &= same is not False
+        entry = {"config": cfg, "workload": name, "vertices": n, "edges": m, "tsv_bytes": size,
+                 "kmax": ref[0], "kmax_truss_edges": ref[1], "ours": list(ours) if ours else None, "equal": same,
+                 "reference_binary": os.path.basename(binary), "reference_threads": a.threads,
+                 "reference_wall_s": round(wall_ref, 2),
+                 "ours_cli_wall_s": round(wall_ours, 2) if wall_ours else None,
+                 "generate_s": round(t_gen, 1)}
+        print(json.dumps(entry), flush=True)
+        rec[name] = entry
+    if a.record:
+        with open(RECORD, "w") as f:
+            json.dump(rec, f, indent=1, sort_keys=True)
+    sys.exit(0 if ok else 1)
+
+
+if __name__ == "__main__":
+    main()
