@@ -218,6 +218,9 @@ def run_mix(args, world, rank, local, pg):
     G = args.mix_graphs
     first = rank * G  # each rank its own slice of the mix (independent graphs)
     ctx = K.Context(local)
+    # Both paths allocate from a pool grown once to the context's budget, so
+    # graphs of new sizes do not map device memory in the middle of a solve.
+    ctx.set_option("pool_reserve_mb", 1 << 30)
     # Per-graph path on a uniform sample.
     lat = []
     sample = list(range(first, first + G, args.sample_every))
@@ -286,6 +289,7 @@ def run_serve(args, world, rank, local, pg):
     base = 1_000_000 + rank * (R + args.calib_graphs)  # away from the graphs of the batched workload
     calib_first, first = base, base + args.calib_graphs
     ctx = K.Context(local)
+    ctx.set_option("pool_reserve_mb", 1 << 30)
     # Calibration: batched graphs/s of this device on other mix graphs.
     b = ctx.batch()
     b.add_mix(calib_first, min(64, args.calib_graphs))

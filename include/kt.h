@@ -61,7 +61,9 @@ const char* kt_status_string(kt_status s);
  *   parse_pipeline_mb (256)     host->device chunk of file ingest
  *   record_kernel_times (0)     events around support / peel kernels
  *   debug_checks (0)            extra host-side consistency checks
- *   verbose (0)                 stage decisions on stderr */
+ *   verbose (0)                 stage decisions on stderr
+ *   pool_reserve_mb (0)         setting it grows the device memory pool by that
+ *                               much at once (allocations mid-solve then reuse it) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 

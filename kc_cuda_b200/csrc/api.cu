@@ -280,7 +280,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"parse_pipeline_mb", &o.parse_pipeline_mb},
              {"record_kernel_times", &o.record_kernel_times},
              {"debug_checks", &o.debug_checks},
-             {"verbose", &o.verbose}};
+             {"verbose", &o.verbose},
+             {"pool_reserve_mb", &o.pool_reserve_mb}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;
@@ -292,6 +293,20 @@ kt_status kt_set_option(kt_ctx* h, const char* name, int64_t value) {
   int64_t* p = option_slot(h->c.opt, name);
   if (!p) return KT_ERR_INVALID;
   *p = value;
+  if (!std::strcmp(name, "pool_reserve_mb") && value > 0) {
+    // Grow the context's memory pool once, up front: later allocations up to
+    // this size are served from it instead of mapping new memory mid-solve.
+    kt::Ctx* c = &h->c;
+    const uint64_t bytes = std::min<uint64_t>((uint64_t)value << 20, c->budget > c->in_use ? c->budget - c->in_use : 0);
+    void* ptr = nullptr;
+    if (bytes && cudaMallocAsync(&ptr, bytes, c->stream) == cudaSuccess) {
+      cudaFreeAsync(ptr, c->stream);
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return KT_ERR_CUDA;
+    } else if (bytes) {
+      cudaGetLastError();
+      return KT_ERR_NOMEM;
+    }
+  }
   return KT_OK;
 }
 

@@ -99,6 +99,26 @@ __global__ void k_group_max(const uint32_t* __restrict__ val, const uint32_t* __
   }
 }
 
+// Per graph: vertices in its maximum core (core == cmax[g]) and vertices
+// with an edge (core >= 1).
+__global__ void k_group_counts(const uint32_t* __restrict__ core, const uint32_t* __restrict__ gid, uint64_t n,
+                               const uint32_t* __restrict__ cmax, unsigned long long* __restrict__ in_max,
+                               unsigned long long* __restrict__ with_edge) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < ((n + 31) & ~31ULL);
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ok = v < n;
+    const uint32_t g = ok ? gid[v] : 0xffffffffu;
+    const uint32_t k = ok ? core[v] : 0u;
+    const unsigned peers = __match_any_sync(kFull, g);
+    const unsigned a = __popc(__ballot_sync(kFull, ok && k >= 1) & peers);
+    const unsigned b = __popc(__ballot_sync(kFull, ok && k >= 1 && k == cmax[ok ? g : 0]) & peers);
+    if (ok && lane_id() == (unsigned)(__ffs(peers) - 1)) {
+      if (a) atomicAdd(&with_edge[g], (unsigned long long)a);
+      if (b) atomicAdd(&in_max[g], (unsigned long long)b);
+    }
+  }
+}
+
 // Vertices of graph g with core >= need[g] (need 0 = graph not taken).
 struct CoreAtLeast {
   const uint32_t* core;
@@ -253,6 +273,7 @@ static void union_sub(Ctx* c, const Graph& U, const uint32_t* dcore, const uint3
     KT_LAUNCHED(c);
   }
   build_sub_grouped(c, U, list.as<uint32_t>(), na, deg.as<uint32_t>(), rem.as<uint32_t>(), dgid, G, s);
+  build_bits(c, s);
 }
 
 // Edges of graph thr's group with support >= thr[group] (thr 0: none).
@@ -334,6 +355,7 @@ static bool survivors(Ctx* c, const Sub& s, const uint32_t* sup, const std::vect
   if (only_if_few && k * 2 >= s.m) return false;
   build_sub_grouped_from_keys(c, keys.as<uint64_t>(), k, s.n, s.vgid.as<uint32_t>(), G, out);
   keys.release();
+  build_bits(c, out);
   out_sup = DBuf(c, (out.m ? out.m : 1) * sizeof(uint32_t));
   edge_support(c, out, out_sup.as<uint32_t>());
   return true;
@@ -364,9 +386,11 @@ static void tracked_peel(Ctx* c, const Sub& s, uint32_t* sup, const std::vector<
   copy_d2h(c, count.data(), dc.get(), G * sizeof(uint64_t));
 }
 
-// One wave: the two phases of the single-graph driver, each graph on its own
+// One wave: the phases of the single-graph driver, each graph on its own
 // levels, all graphs of the wave in each launch.
-//   1. On the union of maximum cores: per-graph support bounds; graph g tries
+//   1. On the union of maximum cores (2-cores for the graphs whose maximum
+//      core is a large part of them -- their answer is final after this
+//      phase): per-graph support bounds; graph g tries
 //      level min(bound, (cmax+1)/2) on its edges of support >= level-2
 //      (rebuilt), halving toward 3 while that truss is empty.
 //   2. On the union of (L-1)-cores of the graphs whose bound L = cmax + 1 is
@@ -410,6 +434,22 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   }
   std::vector<uint32_t> cmax(G);
   copy_d2h(c, cmax.data(), dcm.get(), G * sizeof(uint32_t));
+  // Graphs whose maximum core is a large part of them take one phase (the
+  // single-graph driver's rule): the truss levels of their 2-core.
+  std::vector<unsigned long long> in_max(G, 0), with_edge(G, 0);
+  if (nv) {
+    DBuf dmx(c, G * 8ull), dwe(c, G * 8ull);
+    zero(c, dmx.get(), dmx.bytes());
+    zero(c, dwe.get(), dwe.bytes());
+    k_group_counts<<<grid_for(nv, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        dcore.as<uint32_t>(), dgid.as<uint32_t>(), nv, dcm.as<uint32_t>(), dmx.as<unsigned long long>(),
+        dwe.as<unsigned long long>());
+    KT_LAUNCHED(c);
+    copy_d2h(c, in_max.data(), dmx.get(), G * 8ull);
+    copy_d2h(c, with_edge.data(), dwe.get(), G * 8ull);
+  }
+  std::vector<char> single(G, 0);
+  for (uint32_t g = 0; g < G; ++g) single[g] = in_max[g] * 4 >= with_edge[g];
   st.ms_kcore += tm.stop();
 
   // Phase 1.
@@ -420,7 +460,7 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     std::vector<uint32_t> need(G, 0), cap(G, 0);
     for (uint32_t g = 0; g < G; ++g)
       if (cmax[g] >= 2) {
-        need[g] = cmax[g];
+        need[g] = single[g] ? 2 : cmax[g];
         cap[g] = cmax[g] + 1;
       }
     Sub s1;
@@ -477,7 +517,7 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     items[g]->kmax = 0;
     items[g]->count = 0;
     if (cmax[g] < 2) continue;
-    if (L[g] >= 3 && L[g] == cmax[g] + 1) {
+    if (single[g] || (L[g] >= 3 && L[g] == cmax[g] + 1)) {
       items[g]->kmax = L[g];
       items[g]->count = C[g];
       continue;

@@ -1,6 +1,11 @@
 // Dense mode: the working graph's alive adjacency as bitsets (row u = W
 // 32-bit words), so |N(u) n N(v)| is a popcount of W word-ANDs.
 //
+// A batched union of graphs keeps one block of bitsets per graph (block
+// diagonal): row u has the words of its own graph's size, starts at word
+// roff[u], and bit j of it is vertex cbase[u] + j.  Two ends of an edge are
+// in the same graph, so their rows have the same length.
+//
 // A warp takes 32 consecutive edges of a list.  Each lane fetches one edge's
 // ends, then the warp walks the 32 edges: row u is copied into the warp's
 // slice of shared memory (W words) and reused while consecutive edges share
@@ -11,15 +16,35 @@
 // results are written or pushed once per group.
 #pragma once
 #include "kt_device.cuh"
+#include "subgraph.h"
 
 namespace kt {
+
+// Row addressing of the bitsets: uniform rows of W words (roff == nullptr),
+// or per-graph rows (roff, rw, cbase per vertex; W = the longest row).
+struct DenseRows {
+  uint32_t* bits;
+  uint32_t W;
+  const uint64_t* roff;
+  const uint32_t* rw;
+  const uint32_t* cbase;
+  __device__ __forceinline__ uint64_t off(uint32_t u) const { return roff ? roff[u] : (uint64_t)u * W; }
+  __device__ __forceinline__ uint32_t words(uint32_t u) const { return roff ? rw[u] : W; }
+  // Bit position of neighbour v in row u.
+  __device__ __forceinline__ uint32_t col(uint32_t u, uint32_t v) const { return roff ? v - cbase[u] : v; }
+};
+
+inline DenseRows dense_rows(const Sub& s) {
+  const bool grouped = s.roff.get() != nullptr;
+  return DenseRows{const_cast<uint32_t*>(s.bits.as<uint32_t>()), s.W,
+                   grouped ? s.roff.as<uint64_t>() : nullptr, grouped ? s.rw.as<uint32_t>() : nullptr,
+                   grouped ? s.vbase.as<uint32_t>() : nullptr};
+}
 
 // Shared memory a block of `threads` needs for rows of W words.
 inline size_t dense_smem_bytes(uint32_t W, unsigned threads) { return (size_t)(threads / 32) * W * 4; }
 
-__device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ bits, uint32_t W, uint32_t u,
-                                               uint32_t* su) {
-  const uint32_t* p = bits + (uint64_t)u * W;
+__device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ p, uint32_t W, uint32_t* su) {
   for (uint32_t i = lane_id(); i < W; i += 32) su[i] = p[i];
   __syncwarp();
 }
@@ -27,9 +52,8 @@ __device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ bits
 // popcount(row u & row v) over words [w0, w1); every lane returns the warp
 // total.  Row v is read 16 strides at a time (16 loads in flight per lane,
 // L2-only caching: each row v is used once per edge).
-__device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ bits, uint32_t W,
-                                                   const uint32_t* su, uint32_t v, uint32_t w0, uint32_t w1) {
-  const uint32_t* p = bits + (uint64_t)v * W;
+__device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
+                                                   uint32_t w1) {
   uint32_t s = 0;
   uint32_t i = w0 + lane_id();
   for (; i + 15 * 32 < w1; i += 16 * 32) {
@@ -55,9 +79,9 @@ __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ 
 // lane j holds (my_e, my_s) of the group's j-th entry, my_ok = counted.
 // su is this warp's W-word slice of shared memory.
 __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
-                                            const uint64_t* __restrict__ ends, const uint32_t* __restrict__ bits,
-                                            uint32_t W, const uint32_t* __restrict__ state, uint32_t* su,
-                                            uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
+                                            const uint64_t* __restrict__ ends, const DenseRows& R,
+                                            const uint32_t* __restrict__ state, uint32_t* su, uint32_t& my_e,
+                                            uint32_t& my_s, bool& my_ok) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -75,17 +99,18 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
   my_ok = ok;
   my_s = 0;
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t cu = 0xffffffffu;
+  uint32_t cu = 0xffffffffu, W = 0;
   while (todo) {
     const int j = __ffs(todo) - 1;
     todo &= todo - 1;
     const uint32_t uj = __shfl_sync(kFull, u, j), vj = __shfl_sync(kFull, v, j);
     if (uj != cu) {
       __syncwarp();
-      dense_load_row(bits, W, uj, su);
+      W = R.words(uj);
+      dense_load_row(R.bits + R.off(uj), W, su);
       cu = uj;
     }
-    const uint32_t s = dense_and_popc(bits, W, su, vj, 0, W);
+    const uint32_t s = dense_and_popc(R.bits + R.off(vj), su, 0, W);
     if (l == (unsigned)j) my_s = s;
   }
   __syncwarp();
@@ -96,9 +121,9 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 // count so far plus the set bits left in row u bounds the result.  An
 // abandoned edge reports a count below thr (not its support).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
-                                                   const uint64_t* __restrict__ ends,
-                                                   const uint32_t* __restrict__ bits, uint32_t W, uint32_t thr,
-                                                   uint32_t* su, uint32_t& my_e, uint32_t& my_s, bool& my_ok) {
+                                                   const uint64_t* __restrict__ ends, const DenseRows& R,
+                                                   uint32_t thr, uint32_t* su, uint32_t& my_e, uint32_t& my_s,
+                                                   bool& my_ok) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -113,21 +138,23 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_e = e;
   my_ok = ok;
   my_s = 0;
-  // Segment bounds: four runs of whole 32-word strides.
-  const uint32_t strides = (W + 31) / 32;
-  const uint32_t c1 = min(W, (strides / 4) * 32), c2 = min(W, (strides / 2) * 32),
-                 c3 = min(W, ((3 * strides) / 4) * 32);
   unsigned todo = __ballot_sync(kFull, ok);
   uint32_t s1 = 0, s2 = 0, s3 = 0;  // set bits of row u in segments 2..4
-  uint32_t cu = 0xffffffffu;
+  uint32_t cu = 0xffffffffu, W = 0, c1 = 0, c2 = 0, c3 = 0;
   while (todo) {
     const int j = __ffs(todo) - 1;
     todo &= todo - 1;
     const uint32_t uj = __shfl_sync(kFull, u, j), vj = __shfl_sync(kFull, v, j);
     if (uj != cu) {
       __syncwarp();
-      dense_load_row(bits, W, uj, su);
+      W = R.words(uj);
+      dense_load_row(R.bits + R.off(uj), W, su);
       cu = uj;
+      // Segment bounds: four runs of whole 32-word strides.
+      const uint32_t strides = (W + 31) / 32;
+      c1 = min(W, (strides / 4) * 32);
+      c2 = min(W, (strides / 2) * 32);
+      c3 = min(W, ((3 * strides) / 4) * 32);
       uint32_t b = 0, c = 0, d = 0;
       for (uint32_t i = c1 + l; i < W; i += 32) {
         const uint32_t pc = __popc(su[i]);
@@ -137,12 +164,13 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       s2 = warp_sum(c);
       s3 = warp_sum(d);
     }
-    uint32_t found = dense_and_popc(bits, W, su, vj, 0, c1);
+    const uint32_t* pv = R.bits + R.off(vj);
+    uint32_t found = dense_and_popc(pv, su, 0, c1);
     if (found + s1 + s2 + s3 >= thr) {
-      found += dense_and_popc(bits, W, su, vj, c1, c2);
+      found += dense_and_popc(pv, su, c1, c2);
       if (found + s2 + s3 >= thr) {
-        found += dense_and_popc(bits, W, su, vj, c2, c3);
-        if (found + s3 >= thr) found += dense_and_popc(bits, W, su, vj, c3, W);
+        found += dense_and_popc(pv, su, c2, c3);
+        if (found + s3 >= thr) found += dense_and_popc(pv, su, c3, W);
       }
     }
     if (l == (unsigned)j) my_s = found;

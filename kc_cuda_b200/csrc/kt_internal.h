@@ -53,6 +53,7 @@ struct Options {
   int64_t record_kernel_times = 0;  // events around support / peel kernels
   int64_t debug_checks = 0;       // extra host-side consistency checks
   int64_t verbose = 0;            // stage decisions on stderr
+  int64_t pool_reserve_mb = 0;    // setting it grows the memory pool by this much at once
 };
 
 // Stage decisions on stderr when the context's verbose option is set.

@@ -60,9 +60,9 @@ struct PeelArgs {
   uint32_t tval;   // trussness recorded for removed edges
   uint32_t r0;     // first round number
   uint32_t* adeg;  // alive degree per vertex (for the byte accounting)
-  uint32_t* bits;  // dense mode: alive adjacency bitsets (null otherwise)
-  uint32_t W;      // words per bitset row
-  uint32_t gamma;  // recount round when nf * thr * gamma > alive * W
+  DenseRows R;     // dense mode: alive adjacency bitsets (R.bits null otherwise)
+  float wavg;      // mean words per bitset row
+  uint32_t gamma;  // recount round when nf * thr * gamma > alive * wavg
   unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements, [2] recounted edges
   DevWords* words;
   unsigned long long timeout_ns;
@@ -70,6 +70,7 @@ struct PeelArgs {
   // graph is finished and its edges are never frontier edges).
   const uint32_t* gthr;
   const uint32_t* egr;
+  const uint32_t* gthr_max;  // batched: the largest running threshold (recount cost model)
 };
 
 __device__ __forceinline__ uint32_t edge_thr(const PeelArgs& A, uint32_t e) {
@@ -229,8 +230,9 @@ __device__ __forceinline__ void level_frontier(const PeelArgs& A, uint32_t r, ui
 __device__ __forceinline__ void clear_edge_bits(const PeelArgs& A, uint32_t e) {
   const uint64_t k = A.ends[e];
   const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
-  atomicAnd(&A.bits[(uint64_t)x * A.W + (y >> 5)], ~(1u << (y & 31)));
-  atomicAnd(&A.bits[(uint64_t)y * A.W + (x >> 5)], ~(1u << (x & 31)));
+  const uint32_t cy = A.R.col(x, y), cx = A.R.col(y, x);
+  atomicAnd(&A.R.bits[A.R.off(x) + (cy >> 5)], ~(1u << (cy & 31)));
+  atomicAnd(&A.R.bits[A.R.off(y) + (cx >> 5)], ~(1u << (cx & 31)));
 }
 
 // Clears the bits of alive-list edges deleted in rounds (lo, hi].
@@ -254,7 +256,7 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
   for (uint64_t g = gwarp; g < groups; g += gwarps) {
     uint32_t e, sc;
     bool ok;
-    dense_group(A.alive, g * 32, A.na, A.ends, A.bits, A.W, A.state, su, e, sc, ok);
+    dense_group(A.alive, g * 32, A.na, A.ends, A.R, A.state, su, e, sc, ok);
     trec += __popc(__ballot_sync(kFull, ok));
     bool want = false;
     if (ok) {
@@ -273,7 +275,7 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
 // shared memory per warp for the recount rounds.
 __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
   extern __shared__ uint32_t dense_smem[];
-  uint32_t* su = dense_smem + warp_id() * A.W;
+  uint32_t* su = dense_smem + warp_id() * A.R.W;
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   level_frontier(A, A.r0, gtid, gthreads);
@@ -291,8 +293,9 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
     uint32_t* fr = A.front[i & 1];
     uint32_t* nx = A.front[(i + 1) & 1];
     unsigned long long* nc = &A.cnt[(i + 1) % 3];
-    const bool recount = A.bits && (double)nf * (double)(A.thr > 0 ? A.thr : 1) * (double)A.gamma >
-                                       (double)alive * (double)A.W;
+    const uint32_t thr = A.gthr_max ? *A.gthr_max : A.thr;
+    const bool recount = A.R.bits && (double)nf * (double)(thr > 0 ? thr : 1) * (double)A.gamma >
+                                         (double)alive * (double)A.wavg;
     if (recount) {
       clear_deleted(A, cleared, r, gtid, gthreads);
       cleared = r;
@@ -313,7 +316,7 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
     ++i;
   }
   // Bring the bitsets up to date with this cascade's remaining deletions.
-  if (ok && A.bits) clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
+  if (ok && A.R.bits) clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
   flush_tallies(A, tdeg, tdec);
   if (lane_id() == 0 && trec) atomicAdd(&A.acct[2], (unsigned long long)trec);
   if (gtid == 0) A.cnt[3] = i;
@@ -403,6 +406,14 @@ __global__ void k_track_record(uint32_t ngroups, unsigned long long* __restrict_
     gcnt[g] = 0;
     gmin[g] = 0xffffffffu;
   }
+}
+
+__global__ void k_max_u32(const uint32_t* __restrict__ a, uint32_t n, uint32_t* out) {
+  uint32_t mx = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31) & ~31u); i += gridDim.x * blockDim.x)
+    mx = max(mx, i < n ? a[i] : 0u);
+  mx = warp_max(mx);
+  if (lane_id() == 0 && mx) atomicMax(out, mx);
 }
 
 __global__ void k_track_init(uint64_t m, const uint64_t* __restrict__ ends, const uint32_t* __restrict__ vgid,
@@ -507,13 +518,14 @@ struct Peeler {
     A.r0 = r;
     A.adeg = adeg.as<uint32_t>();
     A.acct = acct.as<unsigned long long>();
-    A.bits = s->W ? s->bits.as<uint32_t>() : nullptr;
-    A.W = s->W;
+    A.R = s->W ? dense_rows(*s) : DenseRows{nullptr, 0, nullptr, nullptr, nullptr};
+    A.wavg = s->W ? (float)((double)s->bit_words / std::max<uint32_t>(s->n, 1)) : 0.f;
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
     A.gthr = track ? gthr.as<uint32_t>() : nullptr;
     A.egr = track ? egr.as<uint32_t>() : nullptr;
+    A.gthr_max = track ? tmax.as<uint32_t>() : nullptr;
     return A;
   }
 
@@ -565,24 +577,33 @@ struct Peeler {
   void account() {
     uint64_t h[3];
     copy_d2h(c, h, acct.get(), 24);
-    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned + 4ULL * s->W * h[2];
+    const double wavg = s->W ? (double)s->bit_words / std::max<uint32_t>(s->n, 1) : 0.0;
+    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned + (uint64_t)(4.0 * wavg * (double)h[2]);
     c->stats.peel_decrements += h[1];
   }
 
   // Batched unions: per-graph thresholds and records after a level.
   const GraphTrack* track = nullptr;
-  DBuf tcnt, tmin, gthr, egr;
+  DBuf tcnt, tmin, gthr, egr, tmax;
   void init_track(uint32_t t0) {
     const uint32_t G = std::max<uint32_t>(track->ngroups, 1);
     tcnt = DBuf(c, (uint64_t)G * 8);
     tmin = DBuf(c, (uint64_t)G * 4);
     gthr = DBuf(c, (uint64_t)G * 4);
     egr = DBuf(c, s->m * 4);
+    tmax = DBuf(c, 4);
     zero(c, tcnt.get(), tcnt.bytes());
     KT_CUDA(cudaMemsetAsync(tmin.get(), 0xff, tmin.bytes(), c->stream));
     k_track_init<<<grid_for(std::max<uint64_t>(s->m, G), 256, c->num_sms * 16), 256, 0, c->stream>>>(
         s->m, s->ends.as<uint64_t>(), track->vgid, egr.as<uint32_t>(), track->ngroups, track->t0, t0,
         gthr.as<uint32_t>());
+    KT_LAUNCHED(c);
+    update_tmax();
+  }
+  void update_tmax() {
+    zero(c, tmax.get(), 4);
+    k_max_u32<<<grid_for(track->ngroups, 256, c->num_sms * 4), 256, 0, c->stream>>>(
+        gthr.as<uint32_t>(), track->ngroups, tmax.as<uint32_t>());
     KT_LAUNCHED(c);
   }
   void record_groups(bool first) {
@@ -596,6 +617,7 @@ struct Peeler {
         track->ngroups, tcnt.as<unsigned long long>(), tmin.as<uint32_t>(), track->kmax, track->count,
         gthr.as<uint32_t>(), track->stop, first);
     KT_LAUNCHED(c);
+    update_tmax();
   }
 
   // Replaces the working graph by its alive part (renumbered, with its own

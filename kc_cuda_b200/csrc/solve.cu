@@ -130,10 +130,40 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   tm.start();
   KCore kc;
   kc.init(c, g);
+  const uint64_t n_edge_vertices = kc.n_alive;  // vertices with an edge
   const uint32_t cmax = kc.find_max_core(c);
   st.cmax = cmax;
   st.ms_kcore += tm.stop();
   if (g.m == 0 || cmax < 2) return;  // a triangle needs three vertices of degree >= 2
+
+  // One phase when the maximum core is a large part of the graph (the
+  // search core would contain it anyway): the truss levels of the 2-core,
+  // tried from its support bound as in the prediction phase.
+  if (!c->opt.predict || kc.n_alive * 4 >= n_edge_vertices) {
+    tm.start();
+    kc.restore_core(c, 2);
+    st.ms_kcore += tm.stop();
+    tm.start();
+    Sub s;
+    build_sub(c, g, kc, s);
+    st.core_vertices = s.n;
+    st.core_edges = s.m;
+    build_bits(c, s);
+    st.ms_subgraph += tm.stop();
+    tm.start();
+    DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
+    edge_support(c, s, sup.as<uint32_t>());
+    st.ms_support += tm.stop();
+    tm.start();
+    const PeelResult p = predict_peel(c, s, sup.as<uint32_t>(), cmax);
+    st.ms_peel += tm.stop();
+    st.levels += p.levels;
+    st.rounds += (uint32_t)p.rounds;
+    *kmax = p.kmax;
+    *count = p.count;
+    st.kmax_lower_bound = p.kmax;
+    return;
+  }
 
   uint32_t L = 0;
   uint64_t C = 0;

@@ -203,6 +203,7 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
     copy_d2h(c, sizes.data(), gsize.get(), ngroups * sizeof(uint32_t));
     s.max_group = 0;
     for (uint32_t x : sizes) s.max_group = std::max(s.max_group, x);
+    s.group_n = std::move(sizes);
   }
   scan_u32_to_u64(c, sdeg.as<uint32_t>(), s.off.as<uint64_t>(), na + 1);
   const uint64_t n2 = read_word<uint64_t>(c, s.off.as<uint64_t>() + na);

@@ -1,6 +1,8 @@
 // The working graph of the truss stages: an induced subgraph relabelled by
 // ascending (degree, id), with sorted rows and an id per undirected edge.
 #pragma once
+#include <vector>
+
 #include "kcore.h"
 #include "stages.h"
 
@@ -16,9 +18,13 @@ struct Sub {
   DBuf up;          // uint64[n]   first entry of each row with neighbour > row
   DBuf ends;        // uint64[m]   u << 32 | v of each edge (new ids, u < v)
   uint32_t max_deg = 0;
-  // Dense mode: alive adjacency as bitsets, row u = words [u*W, (u+1)*W).
+  // Dense mode: alive adjacency as bitsets, row u = words [u*W, (u+1)*W);
+  // for a grouped union, per-graph rows: row u = words [roff[u], roff[u] +
+  // rw[u]) over its graph's vertices from vbase[u] (W = the longest row).
   DBuf bits;
   uint32_t W = 0;   // 0 = not built
+  DBuf roff, rw;
+  uint64_t bit_words = 0;  // words of all rows
   // Dense mode: edge ids in tile order (u >> tb, v >> tb, u, v), so that the
   // rows read by concurrently processed edges stay within two vertex blocks
   // whose bitsets fit in L2 together.
@@ -29,6 +35,7 @@ struct Sub {
   // of its graph, max_group = most vertices of one graph.
   DBuf vgid, vbase;
   uint32_t max_group = 0;
+  std::vector<uint32_t> group_n;  // vertices of each graph (host)
 };
 
 // Builds the subgraph induced by the k-core state's alive vertices.

@@ -112,33 +112,44 @@ __global__ void k_support_search(uint64_t m, const uint64_t* __restrict__ ends, 
 
 // Dense mode: row bitsets from the sorted rows.
 __global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj,
-                             uint32_t* __restrict__ bits, uint32_t W) {
+                             DenseRows R) {
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t u = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); u < n; u += warps) {
-    uint32_t* row = bits + u * W;
+    uint32_t* row = R.bits + R.off((uint32_t)u);
     for (uint64_t j = off[u] + lane_id(); j < off[u + 1]; j += 32) {
-      const uint32_t v = adj[j];
+      const uint32_t v = R.col((uint32_t)u, adj[j]);
       atomicOr(&row[v >> 5], 1u << (v & 31));
     }
   }
 }
 
+// Per-graph rows of a grouped union: graph g's rows hold gw[g] words and
+// start at word gbase[g].
+__global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, const uint32_t* __restrict__ vbase,
+                             const uint64_t* __restrict__ gbase, const uint32_t* __restrict__ gw,
+                             uint64_t* __restrict__ roff, uint32_t* __restrict__ rw) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = vgid[v];
+    roff[v] = gbase[g] + (uint64_t)(v - vbase[v]) * gw[g];
+    rw[v] = gw[g];
+  }
+}
+
 template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
-                                                       const uint64_t* __restrict__ ends,
-                                                       const uint32_t* __restrict__ bits, uint32_t W, uint32_t cap,
+                                                       const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
                                                        uint32_t* __restrict__ sup) {
   extern __shared__ uint32_t dense_smem[];
-  uint32_t* su = dense_smem + warp_id() * W;
+  uint32_t* su = dense_smem + warp_id() * R.W;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t groups = (m + 31) / 32;
   for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
     uint32_t e, s;
     bool ok;
     if (kCapped)
-      dense_group_capped(order, g * 32, m, ends, bits, W, cap, su, e, s, ok);
+      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok);
     else
-      dense_group(order, g * 32, m, ends, bits, W, nullptr, su, e, s, ok);
+      dense_group(order, g * 32, m, ends, R, nullptr, su, e, s, ok);
     if (ok) sup[e] = s;
   }
 }
@@ -161,7 +172,7 @@ void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
   k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           s.bits.as<uint32_t>(), s.W, cap, sup);
+                                                           dense_rows(s), cap, sup);
   KT_LAUNCHED(c);
 }
 
@@ -214,18 +225,55 @@ uint32_t support_bound(Ctx* c, const uint32_t* sup, uint64_t m, uint32_t cap) {
 bool build_bits(Ctx* c, Sub& s) {
   s.W = 0;
   s.bits.release();
-  if (s.n == 0 || s.m == 0 || (int64_t)s.n > c->opt.dense_max_n) return false;
-  const uint32_t W = (s.n + 31) / 32;
-  const double avg = 2.0 * (double)s.m / s.n;
-  if (avg * (double)c->opt.dense_min_fill < (double)W) return false;
-  const uint64_t bytes = (uint64_t)s.n * W * 4;
+  s.roff.release();
+  s.rw.release();
+  s.bit_words = 0;
+  if (s.n == 0 || s.m == 0) return false;
+  // Rows: one block of bitsets per graph for a grouped union (every graph
+  // within the vertex limit), else one block for the whole graph.
+  const bool grouped = s.vgid.get() != nullptr && !s.group_n.empty();
+  uint32_t W = 0;
+  uint64_t words = 0;
+  std::vector<uint64_t> gbase;
+  std::vector<uint32_t> gw;
+  if (grouped) {
+    if ((int64_t)s.max_group > c->opt.dense_max_n) return false;
+    gbase.resize(s.group_n.size());
+    gw.resize(s.group_n.size());
+    for (size_t g = 0; g < s.group_n.size(); ++g) {
+      gbase[g] = words;
+      gw[g] = (s.group_n[g] + 31) / 32;
+      words += (uint64_t)s.group_n[g] * gw[g];
+      W = std::max(W, gw[g]);
+    }
+  } else {
+    if ((int64_t)s.n > c->opt.dense_max_n) return false;
+    W = (s.n + 31) / 32;
+    words = (uint64_t)s.n * W;
+  }
+  // Dense enough: adjacency entries * fill >= words of all rows.
+  if (2.0 * (double)s.m * (double)c->opt.dense_min_fill < (double)words) return false;
+  const uint64_t bytes = words * 4;
   if (c->budget && c->in_use + 2 * bytes > c->budget) return false;
   s.bits.alloc(c, bytes);
   zero(c, s.bits.get(), bytes);
-  k_bits_build<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
-      s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), s.bits.as<uint32_t>(), W);
-  KT_LAUNCHED(c);
+  if (grouped) {
+    const uint32_t G = (uint32_t)gw.size();
+    DBuf dgb(c, G * 8ull), dgw(c, G * 4ull);
+    copy_h2d(c, dgb.get(), gbase.data(), G * 8ull);
+    copy_h2d(c, dgw.get(), gw.data(), G * 4ull);
+    s.roff.alloc(c, (uint64_t)s.n * 8);
+    s.rw.alloc(c, (uint64_t)s.n * 4);
+    k_group_rows<<<grid_for(s.n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.n, s.vgid.as<uint32_t>(), s.vbase.as<uint32_t>(), dgb.as<uint64_t>(), dgw.as<uint32_t>(),
+        s.roff.as<uint64_t>(), s.rw.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
   s.W = W;
+  s.bit_words = words;
+  k_bits_build<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), dense_rows(s));
+  KT_LAUNCHED(c);
   // Tile order: blocks of 2^tb vertices, two blocks' bitsets within ~48 MB.
   uint32_t tb = 16;
   while (tb > 6 && 2ull * (1ull << tb) * W * 4 > (48ull << 20)) --tb;
