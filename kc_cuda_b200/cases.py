@@ -9,6 +9,9 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
   rmat21-solve    R-MAT scale 21, edge factor 32, seed 2, cliques 80/120/200:
                   one kt_solve_staged (every stage; peel kernel k_cascade<8>).
   rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
+  rmat24-solve    the bench graph (R-MAT scale 24, edge factor 32, seed 2,
+                  cliques 80/120/200; 15.5 GB of TSV staged on the device).
+--verbose prints the solver's stage decisions and per-level cascades.
 """
 from __future__ import annotations
 
@@ -34,29 +37,37 @@ def dense_support(reps: int) -> None:
         dg.free()
 
 
-def solve(spec: gen.GraphSpec, reps: int) -> None:
+def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
     g = gen.Graph(spec)
     data = g.tsv_bytes()
+    del g
     with Context(0) as ctx:
+        if verbose:
+            ctx.set_option("verbose", 1)
         t = ctx.stage_tsv(data)
         for _ in range(reps):
             r = t.solve()
             st = ctx.stats()
-            print(f"{r} in {st['ms_total']:.1f} ms device", flush=True)
+            stages = " ".join(f"{k[3:]} {st[k]:.1f}" for k in
+                              ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel"))
+            print(f"{r} in {st['ms_total']:.1f} ms device ({stages})", flush=True)
         t.free()
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve"])
+    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve", "rmat24-solve"])
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
     if a.case == "dense-support":
         dense_support(a.reps)
     elif a.case == "rmat21-solve":
-        solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps)
+        solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
+    elif a.case == "rmat24-solve":
+        solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
     else:
-        solve(gen.rmat_s16_k30(), a.reps)
+        solve(gen.rmat_s16_k30(), a.reps, a.verbose)
 
 
 if __name__ == "__main__":

@@ -41,6 +41,12 @@ inline DenseRows dense_rows(const Sub& s) {
                    grouped ? s.vbase.as<uint32_t>() : nullptr};
 }
 
+// Loads of row v in flight per lane.
+#ifndef KT_DENSE_DEPTH
+#define KT_DENSE_DEPTH 16
+#endif
+constexpr int kDenseDepth = KT_DENSE_DEPTH;
+
 // Shared memory a block of `threads` needs for rows of W words.
 inline size_t dense_smem_bytes(uint32_t W, unsigned threads) { return (size_t)(threads / 32) * W * 4; }
 
@@ -56,12 +62,12 @@ __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ 
                                                    uint32_t w1) {
   uint32_t s = 0;
   uint32_t i = w0 + lane_id();
-  for (; i + 15 * 32 < w1; i += 16 * 32) {
-    uint32_t a[16];
+  for (; i + (kDenseDepth - 1) * 32 < w1; i += kDenseDepth * 32) {
+    uint32_t a[kDenseDepth];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) a[k] = __ldcg(p + i + 32 * k);
+    for (int k = 0; k < kDenseDepth; ++k) a[k] = __ldcg(p + i + 32 * k);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) s += __popc(su[i + 32 * k] & a[k]);
+    for (int k = 0; k < kDenseDepth; ++k) s += __popc(su[i + 32 * k] & a[k]);
   }
   for (; i + 3 * 32 < w1; i += 4 * 32) {
     uint32_t a[4];

@@ -32,6 +32,7 @@
 // strides with host backups and rollbacks (src/kc.cu:1140-1309); the result
 // is the same kmax and edge count.
 #include <algorithm>
+#include <chrono>
 #include <memory>
 
 #include "compact.cuh"
@@ -538,6 +539,7 @@ struct Peeler {
     c->timer.begin(c->stream, &c->stats.ms_peel_kernel, &e0);
     uint64_t rounds = 0;
     scanned += na;
+    const auto t_start = std::chrono::steady_clock::now();
     if (coop_grid) {
       void* p[] = {&A};
       KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, smem, c->stream));
@@ -558,8 +560,9 @@ struct Peeler {
     c->timer.end(c->stream, e0, &c->stats.ms_peel_kernel);
     c->stats.peel_launches++;
     check_words(c, "truss peel");
-    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds\n", t,
-           (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds);
+    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds, %.3f ms\n", t,
+           (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds,
+           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     r += (uint32_t)rounds + 1;
     res->rounds += rounds;
     res->levels++;
