@@ -2,7 +2,7 @@
 reference's own CPU solver (run by hand on the GPU host; too large for the
 test suite):
 
-    python tests/large_parity.py [--configs 2 3] [--dir /dev/shm] [--record]
+    python tests/large_parity.py [--configs 2 3] [--dir /dev/shm] [--record] [--ours-only]
 
 For each configuration: the seeded graph is generated and written as the
 reference's TSV; the drop-in CLI (kc_cuda_b200/kt_solve -f) and kc_cpu (all
@@ -55,6 +55,8 @@ def main():
     ap.add_argument("--record", action="store_true")
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--reference-only", action="store_true", help="no GPU: record kc_cpu's answers only")
+    ap.add_argument("--ours-only", action="store_true",
+                    help="compare with the recorded kc_cpu answer instead of running kc_cpu again")
     a = ap.parse_args()
     rec = json.load(open(RECORD)) if os.path.exists(RECORD) else {}
     ok = True
@@ -71,19 +73,26 @@ def main():
         lines = 2 * m
         large = lines > 1_700_000_000 or 2 * m >= (1 << 31) - (1 << 24)
         binary = os.path.join(O.REF, "kc_cpu_large" if large else "kc_cpu")
-        subprocess.run(["cat", path], stdout=subprocess.DEVNULL, check=True)  # page cache, as vmtouch would
-        t = time.perf_counter()
-        ref = O.run_kc_cpu(path, threads=a.threads, timeout=7200, binary=binary)
-        wall_ref = time.perf_counter() - t
-        os.unlink(path)
         prev = rec.get(name, {})
+        if a.ours_only:
+            if "kmax" not in prev:
+                raise SystemExit(f"--ours-only: no recorded kc_cpu answer for {name}")
+            ref, wall_ref = (prev["kmax"], prev["kmax_truss_edges"]), prev["reference_wall_s"]
+            binary, a_threads = prev["reference_binary"], prev["reference_threads"]
+        else:
+            subprocess.run(["cat", path], stdout=subprocess.DEVNULL, check=True)  # page cache, as vmtouch would
+            t = time.perf_counter()
+            ref = O.run_kc_cpu(path, threads=a.threads, timeout=7200, binary=binary)
+            wall_ref = time.perf_counter() - t
+            a_threads = a.threads
+        os.unlink(path)
         if ours is None and prev.get("ours"):
             ours, wall_ours = tuple(prev["ours"]), prev.get("ours_cli_wall_s")
         same = ours == ref if ours is not None else None
         ok &= same is not False
         entry = {"config": cfg, "workload": name, "vertices": n, "edges": m, "tsv_bytes": size,
                  "kmax": ref[0], "kmax_truss_edges": ref[1], "ours": list(ours) if ours else None, "equal": same,
-                 "reference_binary": os.path.basename(binary), "reference_threads": a.threads,
+                 "reference_binary": os.path.basename(binary), "reference_threads": a_threads,
                  "reference_wall_s": round(wall_ref, 2),
                  "ours_cli_wall_s": round(wall_ours, 2) if wall_ours else None,
                  "generate_s": round(t_gen, 1)}
