@@ -587,7 +587,20 @@ void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
       verts += it.n;
       ++i;
     }
+    const kt_stats before = c->stats;
     solve_wave(c, wave);
+    if (c->opt.verbose) {
+      const kt_stats& a = c->stats;
+      uint64_t keys = 0, verts_w = 0;
+      for (const BatchItem* it : wave) keys += it->nkeys, verts_w += it->n;
+      KT_LOG(c,
+             "kt: wave %u: %zu graphs, %llu keys, %llu vertex ids: input %.2f csr %.2f kcore %.2f subgraph %.2f "
+             "support %.2f peel %.2f ms, %u levels, %u rounds\n",
+             out.waves, wave.size(), (unsigned long long)keys, (unsigned long long)verts_w,
+             a.ms_parse - before.ms_parse, a.ms_csr - before.ms_csr, a.ms_kcore - before.ms_kcore,
+             a.ms_subgraph - before.ms_subgraph, a.ms_support - before.ms_support, a.ms_peel - before.ms_peel,
+             a.levels - before.levels, a.rounds - before.rounds);
+    }
     ++out.waves;
   }
 }

@@ -398,6 +398,166 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
   }
 }
 
+// Full core decomposition in one cooperative launch: the level loop runs on
+// the device, so thousands of graphs of a batched union (or one graph) are
+// decomposed without a host round trip per level.
+//
+// Level k removes every alive vertex of degree <= k (core number k).  A level
+// starts with one pass over the compact alive list that writes the survivors
+// to the other list, takes the vertices of degree k as the first frontier and
+// the survivors' minimum degree; the frontier rounds then run as in k_probe
+// (a neighbour stepping from k+1 to k joins the next frontier).  When a pass
+// finds no vertex of degree k, the next level is the survivors' minimum
+// degree (levels without vertices are skipped).  Every vertex is scanned
+// once per level it stays alive and expanded once.
+struct DecompArgs {
+  const uint64_t* off;
+  const uint32_t* adj;
+  uint32_t* deg;
+  uint32_t* rem;       // kAlive, or 0 once removed
+  uint32_t* core;      // out: core number of every removed vertex
+  uint32_t* list[2];   // compact alive lists (ping-pong)
+  uint32_t* front[2];
+  uint32_t* big;
+  // [0..2] frontier sizes, [3..4] big-row counts, [5..7] alive-list sizes and
+  // [8..10] minimum degrees by level % 3, [11] rounds, [12] levels, [13] last level
+  unsigned long long* cnt;
+  uint64_t n_list;     // entries of list[0] at launch
+  uint64_t cap;
+  DevWords* words;
+  unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ void drop_neighbours_core(const DecompArgs& A, uint64_t b, uint64_t e, uint32_t k,
+                                                     uint32_t* next, unsigned long long* ncnt) {
+  for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
+    bool want = false;
+    uint32_t w = 0;
+    if (j < e) {
+      w = A.adj[j];
+      if (A.rem[w] == kAlive) {
+        const uint32_t old = atomicSub(&A.deg[w], 1u);
+        if (old == k + 1) {
+          A.rem[w] = 0u;
+          A.core[w] = k;
+          want = true;
+        }
+      }
+    }
+    push_warp(want, w, next, ncnt, A.cap, &A.words->err);
+  }
+}
+
+__global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
+  const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
+  uint64_t nl = A.n_list;
+  uint32_t k = 1;        // every alive vertex has degree >= k
+  uint32_t i = 0;        // frontier round index, continued across levels
+  uint32_t lev = 0, li = 0;
+  unsigned long long levels_run = 0;
+  while (nl) {
+    unsigned long long* lc = &A.cnt[5 + lev % 3];
+    unsigned long long* mc = &A.cnt[8 + lev % 3];
+    if (gtid == 0) {
+      // Read two passes ago, before the barrier that ended the last pass.
+      A.cnt[5 + (lev + 1) % 3] = 0;
+      A.cnt[8 + (lev + 1) % 3] = ~0ULL;
+      // The pass pushes the frontier of round i + 1.  Slot i % 3 (empty; it
+      // ended the last level) may still be being read by slower blocks, so it
+      // is left alone; slot (i + 2) % 3 and round i + 1's big-row count were
+      // read before the barriers that ended round i - 1, and are cleared.
+      A.cnt[(i + 2) % 3] = 0;
+      A.cnt[3 + ((i + 1) & 1)] = 0;
+    }
+    const uint32_t* cur = li ? A.list[1] : A.list[0];
+    uint32_t* nxt = li ? A.list[0] : A.list[1];
+    uint32_t mn = 0xffffffffu;
+    for (uint64_t j = gtid; j < ((nl + 31) & ~31ULL); j += gthreads) {
+      bool out = false, keep = false;
+      uint32_t v = 0;
+      if (j < nl) {
+        v = cur[j];
+        if (A.rem[v] == kAlive) {
+          const uint32_t d = A.deg[v];
+          if (d <= k) {
+            A.rem[v] = 0u;
+            A.core[v] = k;
+            out = true;
+          } else {
+            keep = true;
+            mn = min(mn, d);
+          }
+        }
+      }
+      push_warp(out, v, (i & 1) ? A.front[0] : A.front[1], &A.cnt[(i + 1) % 3], A.cap, &A.words->err);
+      push_warp(keep, v, nxt, lc, A.cap, &A.words->err);
+    }
+    mn = warp_min(mn);
+    if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(mc, (unsigned long long)mn);
+    if (!grid_barrier(A.words, A.timeout_ns)) return;
+    nl = ld_acquire_u64(lc);
+    const unsigned long long dmin = ld_acquire_u64(mc);
+    li ^= 1;
+    ++lev;
+    // The pass's frontier is round i + 1's; i advances even when it is empty,
+    // so the next pass counts into a slot no slower block is still reading.
+    ++i;
+    if (ld_acquire_u64(&A.cnt[i % 3]) == 0) {
+      if (nl) k = (uint32_t)dmin;  // no vertex of degree k: skip to the next non-empty level
+      continue;
+    }
+    ++levels_run;
+    // Frontier rounds of level k (k_probe's rounds with threshold k + 1).
+    while (true) {
+      const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
+      if (nf == 0) break;
+      const uint32_t* fr = (i & 1) ? A.front[1] : A.front[0];
+      uint32_t* nx = (i & 1) ? A.front[0] : A.front[1];
+      unsigned long long* nc = &A.cnt[(i + 1) % 3];
+      unsigned long long* bc = &A.cnt[3 + (i & 1)];
+      for (uint64_t f = gwarp; f < nf; f += gwarps) {
+        const uint32_t v = fr[f];
+        const uint64_t b = A.off[v], e = A.off[v + 1];
+        if (e - b > kBigRow) {
+          if (lane_id() == 0) {
+            const unsigned long long p = atomicAdd(bc, 1ULL);
+            if (p < A.cap)
+              A.big[p] = v;
+            else
+              atomicOr(&A.words->err, kDevErrCapacity);
+          }
+          continue;
+        }
+        drop_neighbours_core(A, b, e, k, nx, nc);
+      }
+      if (gtid == 0) {
+        A.cnt[(i + 2) % 3] = 0;
+        A.cnt[3 + ((i + 1) & 1)] = 0;
+      }
+      if (!grid_barrier(A.words, A.timeout_ns)) return;
+      const uint64_t nbig = ld_acquire_u64(bc);
+      if (nbig) {
+        for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+          const uint32_t v = A.big[bi];
+          const uint64_t b = A.off[v], e = A.off[v + 1];
+          for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x)
+            drop_neighbours_core(A, j0, min(e, j0 + 32), k, nx, nc);
+        }
+        if (!grid_barrier(A.words, A.timeout_ns)) return;
+      }
+      ++i;
+    }
+    ++k;  // every survivor now has degree >= k + 1
+  }
+  if (gtid == 0) {
+    A.cnt[11] = i;
+    A.cnt[12] = levels_run;
+    A.cnt[13] = k;
+  }
+}
+
 }  // namespace
 
 void KCore::reset_state(Ctx* c, const Graph& gr) {
@@ -639,9 +799,13 @@ void KCore::members(Ctx* c, uint8_t* dout) {
 }
 
 void KCore::core_numbers(Ctx* c, uint32_t* dcore) {
+  if (compacted) throw Error(KT_ERR_INVALID, "core_numbers needs an uncompacted state");
+  if (c->opt.persistent) {
+    core_numbers_persistent(c, dcore);
+    return;
+  }
   // Peel level by level: the alive set is always a d-core where d is its
   // minimum degree, so the probe at d+1 removes exactly the core-d vertices.
-  if (compacted) throw Error(KT_ERR_INVALID, "core_numbers needs an uncompacted state");
   DBuf mn(c, 4);
   while (n_alive) {
     KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));
@@ -660,6 +824,52 @@ void KCore::core_numbers(Ctx* c, uint32_t* dcore) {
     KT_LAUNCHED(c);
   }
   sync(c);
+}
+
+}  // namespace kt
+
+namespace kt {
+
+void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
+  if (!n) return;
+  zero(c, dcore, n * sizeof(uint32_t));  // isolated vertices: core 0
+  if (!n_alive) return;
+  const Graph& g = cur();
+  DBuf list2(c, n * sizeof(uint32_t));
+  DBuf cn(c, 16 * sizeof(unsigned long long));
+  zero(c, cn.get(), cn.bytes());
+  KT_CUDA(cudaMemsetAsync(cn.as<unsigned long long>() + 8, 0xff, 3 * sizeof(unsigned long long), c->stream));
+  DecompArgs A;
+  A.off = g.off.as<uint64_t>();
+  A.adj = g.adj.as<uint32_t>();
+  A.deg = deg.as<uint32_t>();
+  A.rem = rem.as<uint32_t>();
+  A.core = dcore;
+  A.list[0] = alive.as<uint32_t>();
+  A.list[1] = list2.as<uint32_t>();
+  A.front[0] = front[0].as<uint32_t>();
+  A.front[1] = front[1].as<uint32_t>();
+  A.big = big.as<uint32_t>();
+  A.cnt = cn.as<unsigned long long>();
+  A.n_list = n_alive;
+  A.cap = n;
+  A.words = dev_words(c);
+  A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
+  int per_sm = 0;
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_core_levels, 256, 0));
+  const unsigned grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+  void* p[] = {&A};
+  KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_core_levels, dim3(grid), dim3(256), p, 0, c->stream));
+  KT_LAUNCHED(c);
+  uint64_t h[3];
+  copy_d2h(c, h, cn.as<unsigned long long>() + 11, sizeof(h));
+  rounds += h[0];
+  probes += h[1];
+  check_words(c, "core decomposition");
+  KT_LOG(c, "kt: core decomposition of %llu vertices: %llu levels, %llu rounds, max core %llu\n",
+         (unsigned long long)n_alive, (unsigned long long)h[1], (unsigned long long)h[0],
+         (unsigned long long)(h[2] ? h[2] - 1 : 0));
+  n_alive = 0;  // the state is consumed
 }
 
 }  // namespace kt

@@ -43,6 +43,8 @@ struct KCore {
   void members(Ctx* c, uint8_t* dout);
   // Full decomposition (consumes the state; never compacts).
   void core_numbers(Ctx* c, uint32_t* dcore);
+  // The same in one cooperative launch (levels stepped on the device).
+  void core_numbers_persistent(Ctx* c, uint32_t* dcore);
 
  private:
   void reset_state(Ctx* c, const Graph& gr);

@@ -121,6 +121,33 @@ def test_core_numbers_and_kcore(ctx, golden):
             assert np.array_equal(mem, core >= k), (name, k)
 
 
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_core_numbers_generated(ctx, persistent):
+    """Core numbers of larger generated graphs by the one-launch level loop
+    (persistent=1) and by host-stepped probes (persistent=0): R-MAT hubs with
+    rows above the whole-block threshold (2048), a Chung-Lu graph, a mix
+    graph, and a small graph with isolated vertex ids."""
+    specs = [
+        gen.rmat(15, 24, 5, [40]),
+        gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=200_000, draws=1_500_000, seed=9, cl_w_max=20_000.0),
+        gen.mix_graph(17),
+        gen.rmat(8, 2, 3),
+    ]
+    ctx.set_option("persistent", persistent)
+    try:
+        for spec in specs:
+            g = gen.Graph(spec)
+            d = ctx.load_pairs(g.edges())
+            n = d.num_vertices
+            edges = d.edges()
+            want = O.core_numbers(edges, n)
+            got = d.core_numbers()
+            assert np.array_equal(got, want), (spec, persistent)
+            d.free()
+    finally:
+        ctx.set_option("persistent", 1)
+
+
 def test_config1_rmat_s16(ctx, golden):
     e = golden["rmat_s16_ef16_k30"]
     g = gen.Graph(gen.GraphSpec(**e["spec"]))
