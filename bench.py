@@ -206,6 +206,25 @@ def cpu_baseline_run(steps: int, warmup: int, threads: int):
     return m / med, desc, times
 
 
+TUNE_FIRST = 2_000_000  # mix graphs of the autotuner's sample (away from the measured ones)
+
+
+def autotune(ctx, args, rank):
+    """Tunes the context's kernel thresholds on `tune_graphs` mix graphs from
+    TUNE_FIRST on (kt_autotune); returns its report, or None when off."""
+    if not args.tune_graphs:
+        return None
+    b = ctx.batch()
+    b.add_mix(TUNE_FIRST + rank * args.tune_graphs, args.tune_graphs)
+    t0 = time.perf_counter()
+    tune = b.autotune(passes=1)
+    b.free()
+    tune["wall_s"] = round(time.perf_counter() - t0, 1)
+    tune["sample_graphs"] = args.tune_graphs
+    tune["sample_first"] = TUNE_FIRST + rank * args.tune_graphs
+    return tune
+
+
 def run_mix(args, world, rank, local, pg):
     """Batched workload: graphs 0..G-1 of the mix (n log-uniform over
     [1e3, 1e6], R-MAT or Erdos-Renyi, edge factor 4..64, one clique of 5..60),
@@ -221,6 +240,9 @@ def run_mix(args, world, rank, local, pg):
     # Both paths allocate from a pool grown once to the context's budget, so
     # graphs of new sizes do not map device memory in the middle of a solve.
     ctx.set_option("pool_reserve_mb", 1 << 30)
+    # Kernel thresholds tuned on a sample of other mix graphs (same
+    # distribution); both paths below run with the tuned settings.
+    tune = autotune(ctx, args, rank)
     # Per-graph path on a uniform sample.
     lat = []
     sample = list(range(first, first + G, args.sample_every))
@@ -269,6 +291,7 @@ def run_mix(args, world, rank, local, pg):
             "per_graph": {"graphs_per_s": per_graph_gps, "sample": len(lat), "every": args.sample_every,
                           "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
             "batched_vs_per_graph": value / per_graph_gps,
+            "autotune": tune,
             "clocks": clk.summary(),
         }))
     ctx.close()
@@ -290,6 +313,7 @@ def run_serve(args, world, rank, local, pg):
     calib_first, first = base, base + args.calib_graphs
     ctx = K.Context(local)
     ctx.set_option("pool_reserve_mb", 1 << 30)
+    tune = autotune(ctx, args, rank)
     # Calibration: batched graphs/s of this device on other mix graphs.
     b = ctx.batch()
     b.add_mix(calib_first, min(64, args.calib_graphs))
@@ -335,7 +359,7 @@ def run_serve(args, world, rank, local, pg):
                         "max_ms": summ["max_ms"], "wait_p50_ms": summ["wait_p50_ms"]},
             "waves": sst["waves"], "mean_wave_graphs": summ["mean_wave_graphs"],
             "max_wave_graphs": sst["max_wave_graphs"], "device_bytes_peak": sst["device_bytes_peak"],
-            "alone_vs_served_mismatches": mism, "clocks": clk.summary(),
+            "alone_vs_served_mismatches": mism, "autotune": tune, "clocks": clk.summary(),
         }))
     ctx.close()
 
@@ -353,6 +377,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=0.0, help="requests/s (0: 0.8 x calibrated batched)")
     ap.add_argument("--calib-graphs", type=int, default=512)
+    ap.add_argument("--tune-graphs", type=int, default=128,
+                    help="mix/serve: autotune the kernel thresholds on this many other mix graphs first (0: off)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.workload in ("mix4096", "serve") and args.impl == "ours":

@@ -63,7 +63,14 @@ const char* kt_status_string(kt_status s);
  *   debug_checks (0)            extra host-side consistency checks
  *   verbose (0)                 stage decisions on stderr
  *   pool_reserve_mb (0)         setting it grows the device memory pool by that
- *                               much at once (allocations mid-solve then reuse it) */
+ *                               much at once (allocations mid-solve then reuse it)
+ *   kcore_big_row (2048)        k-core rounds expand longer rows with whole blocks
+ *   peel_search_ratio (16)      peel: per-lane binary search when one row is this
+ *                               many times longer than the other
+ *   dense_tile_mb (48)          dense support: bitset rows of two tile blocks fit
+ *                               in this many MB (L2 reuse)
+ *   kcore_blocks_per_sm (0)     core decomposition: resident blocks per SM of its
+ *                               one cooperative launch (0 = as many as fit) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 
@@ -134,6 +141,31 @@ void kt_batch_free(kt_batch* b);
  * path's input, identical to the batch's); kt_get_stats: ms_parse = the
  * generation, ms_csr = the CSR build. */
 kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_graph** out);
+
+/* ---------------------------------------------------------------- tuning */
+
+/* Autotuner of the kernels' bin and tile thresholds (no counterpart in the
+ * reference, whose thresholds are compile-time constants): the options
+ * recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n,
+ * kcore_big_row, peel_search_ratio, dense_tile_mb and kcore_blocks_per_sm.  Solves the graphs of
+ * `sample` repeatedly, one candidate value at a time (coordinate descent from
+ * the context's current settings, up to `passes` sweeps, device time by CUDA
+ * events, a 2% margin against noise), checks that every candidate leaves
+ * every answer unchanged (KT_ERR_CUDA otherwise), and leaves the fastest
+ * settings on the context.  The sample should be graphs like the ones to be
+ * solved, but not those graphs themselves. */
+typedef struct kt_tune_result {
+  int64_t recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n;
+  int64_t kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm;
+  double ms_first;  /* the sample's device time with the settings at entry */
+  double ms_best;   /* ... with the chosen settings */
+  uint32_t trials;  /* timed candidate runs */
+} kt_tune_result;
+kt_status kt_autotune(kt_batch* sample, uint32_t passes, kt_tune_result* out);
+/* The tuned options as "name value" lines (a comment names the GPU), and
+ * back; unknown names are KT_ERR_INVALID. */
+kt_status kt_options_save(kt_ctx* ctx, const char* path);
+kt_status kt_options_load(kt_ctx* ctx, const char* path);
 
 /* ----------------------------------------------------------------- serve */
 

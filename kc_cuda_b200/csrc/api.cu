@@ -281,7 +281,11 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"record_kernel_times", &o.record_kernel_times},
              {"debug_checks", &o.debug_checks},
              {"verbose", &o.verbose},
-             {"pool_reserve_mb", &o.pool_reserve_mb}};
+             {"pool_reserve_mb", &o.pool_reserve_mb},
+             {"kcore_big_row", &o.kcore_big_row},
+             {"peel_search_ratio", &o.peel_search_ratio},
+             {"dense_tile_mb", &o.dense_tile_mb},
+             {"kcore_blocks_per_sm", &o.kcore_blocks_per_sm}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

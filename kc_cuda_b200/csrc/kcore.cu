@@ -5,8 +5,8 @@
 // decrements the degrees of its surviving neighbours; a neighbour whose
 // degree steps from k to k-1 (atomicSub returns k) joins the next frontier,
 // so every vertex enters a frontier at most once.  Rows of more than
-// kBigRow entries are expanded by a whole block each, so hub rows do not
-// serialise on one warp.
+// kcore_big_row (option, 2048) entries are expanded by a whole block each, so
+// hub rows do not serialise on one warp.
 //
 // The search for the maximum core (the reference steps k by a fixed stride
 // with host backups, src/kc.cu:770-884) ramps k geometrically from the
@@ -84,12 +84,13 @@ __global__ void k_frontier_init(const uint32_t* __restrict__ alive, uint64_t n_a
 __global__ void k_expand(const uint32_t* __restrict__ front, uint64_t nf, const uint64_t* __restrict__ off,
                          const uint32_t* __restrict__ adj, uint32_t* __restrict__ deg, uint32_t* __restrict__ rem,
                          uint32_t k, uint32_t tag, uint32_t* __restrict__ next, unsigned long long* ncnt,
-                         uint32_t* __restrict__ big, unsigned long long* nbig, uint64_t cap, uint32_t* err) {
+                         uint32_t* __restrict__ big, unsigned long long* nbig, uint64_t cap, uint32_t* err,
+                         uint32_t big_row) {
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t f = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); f < nf; f += warps) {
     const uint32_t v = front[f];
     const uint64_t b = off[v], e = off[v + 1];
-    if (e - b > kBigRow) {
+    if (e - b > big_row) {
       if (lane_id() == 0) {
         const unsigned long long p = atomicAdd(nbig, 1ULL);
         if (p < cap)
@@ -150,12 +151,12 @@ __global__ void k_expand_big(const uint32_t* __restrict__ big, const unsigned lo
 __global__ void k_recount(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint64_t* __restrict__ off,
                           const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
                           uint32_t* __restrict__ deg, uint32_t* __restrict__ big, unsigned long long* nbig,
-                          uint64_t cap, uint32_t* err) {
+                          uint64_t cap, uint32_t* err, uint32_t big_row) {
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); i < n_alive; i += warps) {
     const uint32_t v = alive[i];
     const uint64_t b = off[v], e = off[v + 1];
-    if (e - b > kBigRow) {
+    if (e - b > big_row) {
       if (lane_id() == 0) {
         deg[v] = 0;
         const unsigned long long p = atomicAdd(nbig, 1ULL);
@@ -308,6 +309,7 @@ struct ProbeArgs {
   unsigned long long* cnt;  // [0..2] frontier sizes, [3..4] big-row counts, [5] rounds, [6] removed
   uint64_t cap;
   uint32_t k, tag;
+  uint32_t big_row;  // rows longer than this are expanded by whole blocks
   DevWords* words;
   unsigned long long timeout_ns;
 };
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
     for (uint64_t f = gwarp; f < nf; f += gwarps) {
       const uint32_t v = fr[f];
       const uint64_t b = A.off[v], e = A.off[v + 1];
-      if (e - b > kBigRow) {
+      if (e - b > A.big_row) {
         if (lane_id() == 0) {
           const unsigned long long p = atomicAdd(bc, 1ULL);
           if (p < A.cap)
@@ -424,6 +426,7 @@ struct DecompArgs {
   unsigned long long* cnt;
   uint64_t n_list;     // entries of list[0] at launch
   uint64_t cap;
+  uint32_t big_row;    // rows longer than this are expanded by whole blocks
   DevWords* words;
   unsigned long long timeout_ns;
 };
@@ -448,7 +451,18 @@ __device__ __forceinline__ void drop_neighbours_core(const DecompArgs& A, uint64
   }
 }
 
+// One thread per block reads a device counter after a grid barrier and
+// shares it through shared memory (one L2 request per block, not per warp).
+__device__ __forceinline__ unsigned long long block_read(const unsigned long long* p, unsigned long long* sh) {
+  if (threadIdx.x == 0) *sh = ld_acquire_u64(p);
+  __syncthreads();
+  const unsigned long long v = *sh;
+  __syncthreads();
+  return v;
+}
+
 __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
+  __shared__ unsigned long long sh;
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
@@ -497,21 +511,21 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
     mn = warp_min(mn);
     if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(mc, (unsigned long long)mn);
     if (!grid_barrier(A.words, A.timeout_ns)) return;
-    nl = ld_acquire_u64(lc);
-    const unsigned long long dmin = ld_acquire_u64(mc);
+    nl = block_read(lc, &sh);
+    const unsigned long long dmin = block_read(mc, &sh);
     li ^= 1;
     ++lev;
     // The pass's frontier is round i + 1's; i advances even when it is empty,
     // so the next pass counts into a slot no slower block is still reading.
     ++i;
-    if (ld_acquire_u64(&A.cnt[i % 3]) == 0) {
+    if (block_read(&A.cnt[i % 3], &sh) == 0) {
       if (nl) k = (uint32_t)dmin;  // no vertex of degree k: skip to the next non-empty level
       continue;
     }
     ++levels_run;
     // Frontier rounds of level k (k_probe's rounds with threshold k + 1).
     while (true) {
-      const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
+      const uint64_t nf = block_read(&A.cnt[i % 3], &sh);
       if (nf == 0) break;
       const uint32_t* fr = (i & 1) ? A.front[1] : A.front[0];
       uint32_t* nx = (i & 1) ? A.front[0] : A.front[1];
@@ -520,7 +534,7 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
       for (uint64_t f = gwarp; f < nf; f += gwarps) {
         const uint32_t v = fr[f];
         const uint64_t b = A.off[v], e = A.off[v + 1];
-        if (e - b > kBigRow) {
+        if (e - b > A.big_row) {
           if (lane_id() == 0) {
             const unsigned long long p = atomicAdd(bc, 1ULL);
             if (p < A.cap)
@@ -537,7 +551,7 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
         A.cnt[3 + ((i + 1) & 1)] = 0;
       }
       if (!grid_barrier(A.words, A.timeout_ns)) return;
-      const uint64_t nbig = ld_acquire_u64(bc);
+      const uint64_t nbig = block_read(bc, &sh);
       if (nbig) {
         for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
           const uint32_t v = A.big[bi];
@@ -556,6 +570,10 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
     A.cnt[12] = levels_run;
     A.cnt[13] = k;
   }
+}
+
+uint32_t big_row(const Ctx* c) {
+  return (uint32_t)std::min<int64_t>(std::max<int64_t>(32, c->opt.kcore_big_row), 1 << 30);
 }
 
 }  // namespace
@@ -641,7 +659,7 @@ void KCore::recount(Ctx* c) {
   unsigned long long* nbig = cnt.as<unsigned long long>() + 4;
   k_recount<<<grid_for(n_alive * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
       alive.as<uint32_t>(), n_alive, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
-      deg.as<uint32_t>(), big.as<uint32_t>(), nbig, n, &dev_words(c)->err);
+      deg.as<uint32_t>(), big.as<uint32_t>(), nbig, n, &dev_words(c)->err, big_row(c));
   KT_LAUNCHED(c);
   k_recount_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), nbig, g.off.as<uint64_t>(),
                                                        g.adj.as<uint32_t>(), rem.as<uint32_t>(),
@@ -674,6 +692,7 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
     A.cap = n;
     A.k = k;
     A.tag = tag;
+    A.big_row = big_row(c);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
     if (!coop_grid) {
@@ -704,7 +723,7 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
       k_expand<<<grid_for(nf * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
           front[cur_f].as<uint32_t>(), nf, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), deg.as<uint32_t>(),
           rem.as<uint32_t>(), k, tag, front[cur_f ^ 1].as<uint32_t>(), cn + (cur_f ^ 1), big.as<uint32_t>(),
-          cn + 4, n, err);
+          cn + 4, n, err, big_row(c));
       KT_LAUNCHED(c);
       k_expand_big<<<c->num_sms * 4, 256, 0, c->stream>>>(big.as<uint32_t>(), cn + 4, g.off.as<uint64_t>(),
                                                           g.adj.as<uint32_t>(), deg.as<uint32_t>(),
@@ -853,10 +872,12 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   A.cnt = cn.as<unsigned long long>();
   A.n_list = n_alive;
   A.cap = n;
+  A.big_row = big_row(c);
   A.words = dev_words(c);
   A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_core_levels, 256, 0));
+  if (c->opt.kcore_blocks_per_sm > 0) per_sm = (int)std::min<int64_t>(per_sm, c->opt.kcore_blocks_per_sm);
   const unsigned grid = (unsigned)std::max(1, per_sm) * c->num_sms;
   void* p[] = {&A};
   KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_core_levels, dim3(grid), dim3(256), p, 0, c->stream));

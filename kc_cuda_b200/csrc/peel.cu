@@ -11,8 +11,8 @@
 // intersects the two sorted rows: 32-wide tiles of both rows are compared
 // with a 5-step shuffle search, and whichever tile ends lower is retired
 // (both when the ends tie), so every common neighbour is met exactly once;
-// when one row is more than 16x longer the lanes binary-search the long row
-// instead.  A common w closes the triangle {e, a, b}; it is skipped if a or b
+// when one row is more than peel_search_ratio (16) times longer the lanes
+// binary-search the long row instead.  A common w closes the triangle {e, a, b}; it is skipped if a or b
 // was deleted in an earlier round.  Each surviving side edge loses one
 // triangle, decremented by exactly one frontier edge of the triangle (the
 // one with the smallest id among those in this round); an edge whose support
@@ -64,6 +64,7 @@ struct PeelArgs {
   DenseRows R;     // dense mode: alive adjacency bitsets (R.bits null otherwise)
   float wavg;      // mean words per bitset row
   uint32_t gamma;  // recount round when nf * thr * gamma > alive * wavg
+  uint32_t search_ratio;  // binary-search the long row when it is this many times longer
   unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements, [2] recounted edges
   DevWords* words;
   unsigned long long timeout_ns;
@@ -152,7 +153,7 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
   const uint64_t na = xe - xb, nb = ye - yb;
   uint32_t* err = &A.words->err;
   const unsigned lane = lane_id();
-  if (nb > 16 * na) {
+  if (nb > (uint64_t)A.search_ratio * na) {
     // Short row against a long one: binary search per lane.
     for (uint64_t q = xb + lane; q < xb + ((na + 31) & ~31ULL); q += 32) {
       bool pa = false, pb = false;
@@ -522,6 +523,7 @@ struct Peeler {
     A.R = s->W ? dense_rows(*s) : DenseRows{nullptr, 0, nullptr, nullptr, nullptr};
     A.wavg = s->W ? (float)((double)s->bit_words / std::max<uint32_t>(s->n, 1)) : 0.f;
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
+    A.search_ratio = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.peel_search_ratio), 1 << 20);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
     A.gthr = track ? gthr.as<uint32_t>() : nullptr;

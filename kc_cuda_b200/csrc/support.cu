@@ -276,7 +276,8 @@ bool build_bits(Ctx* c, Sub& s) {
   KT_LAUNCHED(c);
   // Tile order: blocks of 2^tb vertices, two blocks' bitsets within ~48 MB.
   uint32_t tb = 16;
-  while (tb > 6 && 2ull * (1ull << tb) * W * 4 > (48ull << 20)) --tb;
+  const uint64_t tile_bytes = (uint64_t)std::max<int64_t>(1, c->opt.dense_tile_mb) << 20;
+  while (tb > 6 && 2ull * (1ull << tb) * W * 4 > tile_bytes) --tb;
   s.tile_bits = tb;
   s.order.alloc(c, s.m * sizeof(uint32_t));
   DBuf keys(c, s.m * sizeof(uint64_t));

@@ -78,6 +78,16 @@ class ServerStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "recount_gamma", "dense_min_fill", "dense_max_n", "support_bitmap_max_n", "kcore_big_row",
+        "peel_search_ratio", "dense_tile_mb", "kcore_blocks_per_sm")] + [
+        ("ms_first", ctypes.c_double), ("ms_best", ctypes.c_double), ("trials", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _LIB = None
 
 # (name, restype, argtypes) of every entry point of include/kt.h.
@@ -108,6 +118,9 @@ SIGNATURES = [
     ("kt_batch_run", ctypes.c_int, [_P]),
     ("kt_batch_results", ctypes.c_int, [_P, _U32P, _U64P]),
     ("kt_batch_free", None, [_P]),
+    ("kt_autotune", ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(TuneResult)]),
+    ("kt_options_save", ctypes.c_int, [_P, ctypes.c_char_p]),
+    ("kt_options_load", ctypes.c_int, [_P, ctypes.c_char_p]),
     ("kt_load_mix_graph", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     ("kt_kcore", ctypes.c_int, [_P, _P, ctypes.c_uint32, _U8P, ctypes.POINTER(ctypes.c_uint32)]),
     ("kt_kcore_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
@@ -193,6 +206,12 @@ class Context:
         v = ctypes.c_int64()
         self.check(self._L.kt_get_option(self._h, name.encode(), ctypes.byref(v)))
         return v.value
+
+    def save_options(self, path: str):
+        self.check(self._L.kt_options_save(self._h, path.encode()))
+
+    def load_options(self, path: str):
+        self.check(self._L.kt_options_load(self._h, path.encode()))
 
     def stats(self) -> dict:
         st = Stats()
@@ -291,6 +310,14 @@ class Batch:
 
     def run(self):
         self.ctx.check(self.ctx._L.kt_batch_run(self._h))
+
+    def autotune(self, passes: int = 1) -> dict:
+        """Tunes the context's kernel thresholds on this batch (a sample of
+        graphs like the ones to be solved); returns the chosen settings and
+        the sample's device time before and after."""
+        r = TuneResult()
+        self.ctx.check(self.ctx._L.kt_autotune(self._h, passes, ctypes.byref(r)))
+        return r.as_dict()
 
     def results(self) -> Tuple[np.ndarray, np.ndarray]:
         n = self.size()[0]
