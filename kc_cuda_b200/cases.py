@@ -11,6 +11,8 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
   rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
   rmat24-solve    the bench graph (R-MAT scale 24, edge factor 32, seed 2,
                   cliques 80/120/200; 15.5 GB of TSV staged on the device).
+  mix-batch       graphs 0..255 of the batched mix in one kt_batch_run
+                  (k_core_levels on the union, grouped support and peel).
 --verbose prints the solver's stage decisions and per-level cascades.
 """
 from __future__ import annotations
@@ -54,9 +56,24 @@ def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
         t.free()
 
 
+def mix_batch(reps: int, verbose: bool = False) -> None:
+    with Context(0) as ctx:
+        if verbose:
+            ctx.set_option("verbose", 1)
+        for _ in range(reps):
+            b = ctx.batch()
+            b.add_mix(0, 256)
+            b.run()
+            st = ctx.stats()
+            k, _ = b.results()
+            b.free()
+            print(f"256 mix graphs, kmax sum {int(k.sum())}, {st['ms_total'] - st['ms_parse']:.1f} ms device "
+                  f"({st['batch_waves']} waves)", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve", "rmat24-solve"])
+    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve", "rmat24-solve", "mix-batch"])
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
@@ -64,6 +81,8 @@ def main() -> None:
         dense_support(a.reps)
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
+    elif a.case == "mix-batch":
+        mix_batch(a.reps, a.verbose)
     elif a.case == "rmat24-solve":
         solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
     else:

@@ -98,7 +98,7 @@ void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g
 
 void load_tsv(Ctx* c, const char* bytes, uint64_t len, Graph& g) {
   DBuf dbuf(c, parse_padded_bytes(len));
-  zero(c, dbuf.get(), dbuf.bytes());
+  zero(c, dbuf.as<uint8_t>() + len, dbuf.bytes() - len);  // the parser reads zeros past len
   copy_h2d(c, dbuf.get(), bytes, len);
   graph_from_device_bytes(c, dbuf.as<uint8_t>(), len, g);
 }
@@ -150,7 +150,7 @@ static void load_tsv_file(Ctx* c, const char* path, Graph& g) {
     }
   } unmap{map, len, fd};
   DBuf dbuf(c, parse_padded_bytes(len));
-  zero(c, dbuf.get(), dbuf.bytes());
+  zero(c, dbuf.as<uint8_t>() + len, dbuf.bytes() - len);  // the parser reads zeros past len
   const uint64_t chunk = (uint64_t)std::max<int64_t>(1, c->opt.parse_pipeline_mb) << 20;
   char* stage[2] = {nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
@@ -285,7 +285,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"kcore_big_row", &o.kcore_big_row},
              {"peel_search_ratio", &o.peel_search_ratio},
              {"dense_tile_mb", &o.dense_tile_mb},
-             {"kcore_blocks_per_sm", &o.kcore_blocks_per_sm}};
+             {"kcore_blocks_per_sm", &o.kcore_blocks_per_sm},
+             {"kcore_window", &o.kcore_window}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;
@@ -433,7 +434,7 @@ kt_status kt_tsv_stage(kt_ctx* h, const char* bytes, uint64_t len, kt_tsv** out)
   try {
     t->len = len;
     t->bytes.alloc(c, kt::parse_padded_bytes(len));
-    kt::zero(c, t->bytes.get(), t->bytes.bytes());
+    kt::zero(c, t->bytes.as<uint8_t>() + len, t->bytes.bytes() - len);  // the parser reads zeros past len
     kt::copy_h2d(c, t->bytes.get(), bytes, len);
     kt::sync(c);
   } catch (...) {

@@ -404,50 +404,66 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
 // the device, so thousands of graphs of a batched union (or one graph) are
 // decomposed without a host round trip per level.
 //
-// Level k removes every alive vertex of degree <= k (core number k).  A level
-// starts with one pass over the compact alive list that writes the survivors
-// to the other list, takes the vertices of degree k as the first frontier and
-// the survivors' minimum degree; the frontier rounds then run as in k_probe
-// (a neighbour stepping from k+1 to k joins the next frontier).  When a pass
-// finds no vertex of degree k, the next level is the survivors' minimum
-// degree (levels without vertices are skipped).  Every vertex is scanned
-// once per level it stays alive and expanded once.
+// Level k removes every alive vertex of degree <= k (core number k): a pass
+// over a vertex list takes the vertices of degree <= k as the first frontier,
+// and the frontier rounds then run as in k_probe (a neighbour stepping from
+// k+1 to k joins the next frontier).  Passes are windowed: a full pass over
+// the compact alive list opens a window of `window` levels [k, top] and
+// lists the candidates, the alive vertices of degree <= top; within the
+// window each level's pass reads only the candidates, and a neighbour whose
+// degree steps from top+1 to top during the rounds joins them.  So the alive
+// list is read once per window instead of once per level.  A pass that finds
+// no vertex of degree k moves k to the smallest degree it saw (levels
+// without vertices are skipped).
 struct DecompArgs {
   const uint64_t* off;
   const uint32_t* adj;
   uint32_t* deg;
   uint32_t* rem;       // kAlive, or 0 once removed
   uint32_t* core;      // out: core number of every removed vertex
-  uint32_t* list[2];   // compact alive lists (ping-pong)
+  uint32_t* list[2];   // compact alive lists (ping-pong, rewritten by full passes)
+  uint32_t* cand[2];   // window candidates (ping-pong, rewritten by every pass)
   uint32_t* front[2];
   uint32_t* big;
-  // [0..2] frontier sizes, [3..4] big-row counts, [5..7] alive-list sizes and
-  // [8..10] minimum degrees by level % 3, [11] rounds, [12] levels, [13] last level
+  // [0..2] frontier sizes, [3..4] big-row counts; by pass % 3: [5..7]
+  // alive-list sizes, [8..10] minimum degrees, [11..13] candidate counts;
+  // [14] rounds, [15] levels, [16] passes, [17] full passes, [18] last level
   unsigned long long* cnt;
   uint64_t n_list;     // entries of list[0] at launch
   uint64_t cap;
   uint32_t big_row;    // rows longer than this are expanded by whole blocks
+  uint32_t window;     // levels per window (>= 1)
   DevWords* words;
   unsigned long long timeout_ns;
 };
 
-__device__ __forceinline__ void drop_neighbours_core(const DecompArgs& A, uint64_t b, uint64_t e, uint32_t k,
-                                                     uint32_t* next, unsigned long long* ncnt) {
+struct DropRule {
+  uint32_t k, top;
+  uint32_t* next;              // frontier of the next round
+  unsigned long long* ncnt;
+  uint32_t* cand;              // candidates of this pass
+  unsigned long long* ccnt;
+};
+
+__device__ __forceinline__ void drop_neighbours_core(const DecompArgs& A, uint64_t b, uint64_t e, const DropRule& R) {
   for (uint64_t j = b + lane_id(); j < b + ((e - b + 31) & ~31ULL); j += 32) {
-    bool want = false;
+    bool want = false, join = false;
     uint32_t w = 0;
     if (j < e) {
       w = A.adj[j];
       if (A.rem[w] == kAlive) {
         const uint32_t old = atomicSub(&A.deg[w], 1u);
-        if (old == k + 1) {
+        if (old == R.k + 1) {
           A.rem[w] = 0u;
-          A.core[w] = k;
+          A.core[w] = R.k;
           want = true;
+        } else if (old == R.top + 1) {
+          join = true;  // its degree entered the window
         }
       }
     }
-    push_warp(want, w, next, ncnt, A.cap, &A.words->err);
+    push_warp(want, w, R.next, R.ncnt, A.cap, &A.words->err);
+    push_warp(join, w, R.cand, R.ccnt, A.cap, &A.words->err);
   }
 }
 
@@ -466,18 +482,23 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
-  uint64_t nl = A.n_list;
-  uint32_t k = 1;        // every alive vertex has degree >= k
-  uint32_t i = 0;        // frontier round index, continued across levels
-  uint32_t lev = 0, li = 0;
-  unsigned long long levels_run = 0;
-  while (nl) {
-    unsigned long long* lc = &A.cnt[5 + lev % 3];
-    unsigned long long* mc = &A.cnt[8 + lev % 3];
+  uint64_t nl = A.n_list;  // entries of the current alive list
+  uint64_t nc = 0;         // entries of the current candidate list
+  uint32_t k = 1;          // every alive vertex has degree >= k
+  uint32_t top = 0;        // candidates: every alive vertex of degree <= top
+  bool full = true;        // the next pass reads the alive list
+  uint32_t i = 0;          // frontier round index, continued across levels
+  uint32_t ps = 0, li = 0, ci = 0;
+  unsigned long long levels_run = 0, full_passes = 0;
+  while (true) {
+    unsigned long long* lc = &A.cnt[5 + ps % 3];
+    unsigned long long* mc = &A.cnt[8 + ps % 3];
+    unsigned long long* cc = &A.cnt[11 + ps % 3];
     if (gtid == 0) {
-      // Read two passes ago, before the barrier that ended the last pass.
-      A.cnt[5 + (lev + 1) % 3] = 0;
-      A.cnt[8 + (lev + 1) % 3] = ~0ULL;
+      // Read two passes ago, before the barriers that ended the last pass.
+      A.cnt[5 + (ps + 1) % 3] = 0;
+      A.cnt[8 + (ps + 1) % 3] = ~0ULL;
+      A.cnt[11 + (ps + 1) % 3] = 0;
       // The pass pushes the frontier of round i + 1.  Slot i % 3 (empty; it
       // ended the last level) may still be being read by slower blocks, so it
       // is left alone; slot (i + 2) % 3 and round i + 1's big-row count were
@@ -485,14 +506,20 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
       A.cnt[(i + 2) % 3] = 0;
       A.cnt[3 + ((i + 1) & 1)] = 0;
     }
-    const uint32_t* cur = li ? A.list[1] : A.list[0];
-    uint32_t* nxt = li ? A.list[0] : A.list[1];
+    if (full) {
+      top = k + A.window - 1;
+      ++full_passes;
+    }
+    const uint32_t* src = full ? (li ? A.list[1] : A.list[0]) : (ci ? A.cand[1] : A.cand[0]);
+    const uint64_t nsrc = full ? nl : nc;
+    uint32_t* lnext = li ? A.list[0] : A.list[1];
+    uint32_t* cnext = ci ? A.cand[0] : A.cand[1];
     uint32_t mn = 0xffffffffu;
-    for (uint64_t j = gtid; j < ((nl + 31) & ~31ULL); j += gthreads) {
-      bool out = false, keep = false;
+    for (uint64_t j = gtid; j < ((nsrc + 31) & ~31ULL); j += gthreads) {
+      bool out = false, keep = false, cand = false;
       uint32_t v = 0;
-      if (j < nl) {
-        v = cur[j];
+      if (j < nsrc) {
+        v = src[j];
         if (A.rem[v] == kAlive) {
           const uint32_t d = A.deg[v];
           if (d <= k) {
@@ -500,36 +527,52 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
             A.core[v] = k;
             out = true;
           } else {
-            keep = true;
+            keep = full;
+            cand = d <= top;
             mn = min(mn, d);
           }
         }
       }
       push_warp(out, v, (i & 1) ? A.front[0] : A.front[1], &A.cnt[(i + 1) % 3], A.cap, &A.words->err);
-      push_warp(keep, v, nxt, lc, A.cap, &A.words->err);
+      if (full) push_warp(keep, v, lnext, lc, A.cap, &A.words->err);
+      push_warp(cand, v, cnext, cc, A.cap, &A.words->err);
     }
     mn = warp_min(mn);
     if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(mc, (unsigned long long)mn);
     if (!grid_barrier(A.words, A.timeout_ns)) return;
-    nl = block_read(lc, &sh);
+    if (full) {
+      nl = block_read(lc, &sh);
+      li ^= 1;
+    }
     const unsigned long long dmin = block_read(mc, &sh);
-    li ^= 1;
-    ++lev;
+    ++ps;
     // The pass's frontier is round i + 1's; i advances even when it is empty,
     // so the next pass counts into a slot no slower block is still reading.
     ++i;
     if (block_read(&A.cnt[i % 3], &sh) == 0) {
-      if (nl) k = (uint32_t)dmin;  // no vertex of degree k: skip to the next non-empty level
+      nc = block_read(cc, &sh);
+      ci ^= 1;
+      if (full) {
+        if (nl == 0) break;  // nothing alive
+        k = (uint32_t)dmin;  // the candidates hold level dmin's vertices when it is in the window
+        full = k > top;
+      } else if (nc) {
+        k = (uint32_t)dmin;  // the smallest candidate degree (<= top)
+      } else {
+        k = top + 1;  // no alive vertex of degree <= top: open the next window
+        full = true;
+      }
       continue;
     }
     ++levels_run;
-    // Frontier rounds of level k (k_probe's rounds with threshold k + 1).
+    // Frontier rounds of level k.
+    DropRule R{k, top, nullptr, nullptr, cnext, cc};
     while (true) {
       const uint64_t nf = block_read(&A.cnt[i % 3], &sh);
       if (nf == 0) break;
       const uint32_t* fr = (i & 1) ? A.front[1] : A.front[0];
-      uint32_t* nx = (i & 1) ? A.front[0] : A.front[1];
-      unsigned long long* nc = &A.cnt[(i + 1) % 3];
+      R.next = (i & 1) ? A.front[0] : A.front[1];
+      R.ncnt = &A.cnt[(i + 1) % 3];
       unsigned long long* bc = &A.cnt[3 + (i & 1)];
       for (uint64_t f = gwarp; f < nf; f += gwarps) {
         const uint32_t v = fr[f];
@@ -544,7 +587,7 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
           }
           continue;
         }
-        drop_neighbours_core(A, b, e, k, nx, nc);
+        drop_neighbours_core(A, b, e, R);
       }
       if (gtid == 0) {
         A.cnt[(i + 2) % 3] = 0;
@@ -557,18 +600,24 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
           const uint32_t v = A.big[bi];
           const uint64_t b = A.off[v], e = A.off[v + 1];
           for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x)
-            drop_neighbours_core(A, j0, min(e, j0 + 32), k, nx, nc);
+            drop_neighbours_core(A, j0, min(e, j0 + 32), R);
         }
         if (!grid_barrier(A.words, A.timeout_ns)) return;
       }
       ++i;
     }
-    ++k;  // every survivor now has degree >= k + 1
+    // Every candidate push of this pass is in (rounds end with a barrier).
+    nc = block_read(cc, &sh);
+    ci ^= 1;
+    ++k;  // every survivor now has degree >= k
+    full = k > top;
   }
   if (gtid == 0) {
-    A.cnt[11] = i;
-    A.cnt[12] = levels_run;
-    A.cnt[13] = k;
+    A.cnt[14] = i;
+    A.cnt[15] = levels_run;
+    A.cnt[16] = ps;
+    A.cnt[17] = full_passes;
+    A.cnt[18] = k;
   }
 }
 
@@ -854,8 +903,8 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   zero(c, dcore, n * sizeof(uint32_t));  // isolated vertices: core 0
   if (!n_alive) return;
   const Graph& g = cur();
-  DBuf list2(c, n * sizeof(uint32_t));
-  DBuf cn(c, 16 * sizeof(unsigned long long));
+  DBuf list2(c, n * sizeof(uint32_t)), cand0(c, n * sizeof(uint32_t)), cand1(c, n * sizeof(uint32_t));
+  DBuf cn(c, 24 * sizeof(unsigned long long));
   zero(c, cn.get(), cn.bytes());
   KT_CUDA(cudaMemsetAsync(cn.as<unsigned long long>() + 8, 0xff, 3 * sizeof(unsigned long long), c->stream));
   DecompArgs A;
@@ -866,6 +915,8 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   A.core = dcore;
   A.list[0] = alive.as<uint32_t>();
   A.list[1] = list2.as<uint32_t>();
+  A.cand[0] = cand0.as<uint32_t>();
+  A.cand[1] = cand1.as<uint32_t>();
   A.front[0] = front[0].as<uint32_t>();
   A.front[1] = front[1].as<uint32_t>();
   A.big = big.as<uint32_t>();
@@ -873,6 +924,7 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   A.n_list = n_alive;
   A.cap = n;
   A.big_row = big_row(c);
+  A.window = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.kcore_window), 1 << 20);
   A.words = dev_words(c);
   A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
   int per_sm = 0;
@@ -882,14 +934,14 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   void* p[] = {&A};
   KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_core_levels, dim3(grid), dim3(256), p, 0, c->stream));
   KT_LAUNCHED(c);
-  uint64_t h[3];
-  copy_d2h(c, h, cn.as<unsigned long long>() + 11, sizeof(h));
+  uint64_t h[5];
+  copy_d2h(c, h, cn.as<unsigned long long>() + 14, sizeof(h));
   rounds += h[0];
   probes += h[1];
   check_words(c, "core decomposition");
-  KT_LOG(c, "kt: core decomposition of %llu vertices: %llu levels, %llu rounds, max core %llu\n",
-         (unsigned long long)n_alive, (unsigned long long)h[1], (unsigned long long)h[0],
-         (unsigned long long)(h[2] ? h[2] - 1 : 0));
+  KT_LOG(c, "kt: core decomposition of %llu vertices: %llu levels, %llu rounds, %llu passes (%llu full), max core %llu\n",
+         (unsigned long long)n_alive, (unsigned long long)h[1], (unsigned long long)h[0], (unsigned long long)h[2],
+         (unsigned long long)h[3], (unsigned long long)(h[4] ? h[4] - 1 : 0));
   n_alive = 0;  // the state is consumed
 }
 

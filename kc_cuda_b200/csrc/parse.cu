@@ -87,6 +87,58 @@ __device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t p, bool*
   return x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
 }
 
+// The same parse from the staged words held in a register window: one
+// shared-memory load per 4 bytes and no per-byte range test other than
+// p < lim.  Returns false (and the caller parses the line with parse_line)
+// when the line's first two numbers reach past lim = min(len, staged end).
+__device__ __forceinline__ bool parse_line_fast(const uint32_t* stage, uint64_t blo, uint64_t lim, uint64_t p,
+                                                uint64_t* key, bool* bad, uint32_t* vmax) {
+  if (p >= lim) return false;
+  const uint32_t off = (uint32_t)(p - blo);
+  uint32_t q = off >> 2;
+  uint32_t cur = stage[q] >> (8 * (off & 3));
+  uint32_t nb = 4 - (off & 3);
+  uint32_t b = cur & 0xffu;
+  // Next byte into b; false past lim.
+#define KT_ADV()                 \
+  do {                           \
+    if (++p >= lim) return false; \
+    if (--nb == 0) {             \
+      cur = stage[++q];          \
+      nb = 4;                    \
+    } else {                     \
+      cur >>= 8;                 \
+    }                            \
+    b = cur & 0xffu;             \
+  } while (0)
+#define KT_DIGIT(x) ((uint32_t)((x) - 0x30u) < 0x50u)  // signed char >= '0'
+  while (b != '\n' && !KT_DIGIT(b)) KT_ADV();
+  if (!KT_DIGIT(b)) {
+    *key = ~0ull;
+    return true;
+  }
+  uint32_t x = 0, y = 0;
+  while (KT_DIGIT(b)) {
+    x = x * 10u + (b - 0x30u);
+    KT_ADV();
+  }
+  while (b != '\n' && !KT_DIGIT(b)) KT_ADV();
+  if (!KT_DIGIT(b)) {
+    *bad = true;
+    *key = ~0ull;
+    return true;
+  }
+  while (KT_DIGIT(b)) {
+    y = y * 10u + (b - 0x30u);
+    KT_ADV();
+  }
+#undef KT_ADV
+#undef KT_DIGIT
+  *vmax = max(*vmax, max(x, y));
+  *key = x == y ? ~0ull : (x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x));
+  return true;
+}
+
 // Phase 1 finds the block's line starts (newlines a word at a time, a block
 // scan, offsets into shared memory); phase 2 deals the lines round-robin to
 // the threads, so the per-line work is balanced and the keys are written
@@ -142,9 +194,14 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
   const uint64_t slot0 = block_off[blockIdx.x];
   uint32_t vmax = 0;
   bool any = false;
+  const uint64_t lim = min(len, blo + nvec * 16);
   for (uint32_t i = threadIdx.x; i < total; i += kParseThreads) {
     bool bad = false;
-    const uint64_t key = parse_line(B, blo + starts[i], &bad, &vmax);
+    uint64_t key;
+    if (!parse_line_fast(stage, blo, lim, blo + starts[i], &key, &bad, &vmax)) {
+      bad = false;
+      key = parse_line(B, blo + starts[i], &bad, &vmax);
+    }
     if (bad) {
       atomicOr(&words->err, kDevErrParse);
       atomicMin(&words->bad_line, (unsigned long long)(slot0 + i));
