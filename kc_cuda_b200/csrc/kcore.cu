@@ -5,8 +5,8 @@
 // decrements the degrees of its surviving neighbours; a neighbour whose
 // degree steps from k to k-1 (atomicSub returns k) joins the next frontier,
 // so every vertex enters a frontier at most once.  Rows of more than
-// kcore_big_row (option, 2048) entries are expanded by a whole block each, so
-// hub rows do not serialise on one warp.
+// kcore_big_row (option, 512) entries are cut into 32-entry windows dealt to
+// every warp of the grid, so hub rows do not serialise on one warp.
 //
 // The search for the maximum core (the reference steps k by a fixed stride
 // with host backups, src/kc.cu:770-884) ramps k geometrically from the
@@ -61,6 +61,64 @@ __device__ __forceinline__ void push_warp(bool want, uint32_t item, uint32_t* li
   }
 }
 
+constexpr unsigned kBigBatch = 1024;  // big rows per batch of dealt windows
+
+// Deals the 32-entry windows of the big rows big[0..nbig) to every warp of
+// the grid, so one long row is spread over the whole GPU instead of one
+// block: each block lists the rows' first window numbers (the same block scan
+// in every block, kBigBatch rows at a time) and warp w takes windows w,
+// w + warps, ...; `drop(b, e)` handles entries [b, e) (at most 32) of a row.
+// Every thread of the block must call it (it synchronises the block); blocks
+// have 256 threads.
+template <class Drop>
+__device__ __forceinline__ void deal_big_windows(const uint32_t* __restrict__ big, uint64_t nbig,
+                                                 const uint64_t* __restrict__ off, uint64_t* woff, uint64_t* tmp,
+                                                 Drop drop) {
+  const uint64_t gwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
+  constexpr unsigned per = kBigBatch / 256;  // rows per thread
+  for (uint64_t base = 0; base < nbig; base += kBigBatch) {
+    const uint64_t left = nbig - base;
+    const uint32_t cnt = left < kBigBatch ? (uint32_t)left : kBigBatch;
+    uint64_t w[per];
+    uint64_t sum = 0;
+#pragma unroll
+    for (unsigned j = 0; j < per; ++j) {
+      const uint32_t r = threadIdx.x * per + j;
+      w[j] = 0;
+      if (r < cnt) {
+        const uint32_t v = big[base + r];
+        w[j] = (off[v + 1] - off[v] + 31) / 32;
+      }
+      sum += w[j];
+    }
+    uint64_t total;
+    uint64_t pre = block_excl_scan<uint64_t>(sum, tmp, &total);
+#pragma unroll
+    for (unsigned j = 0; j < per; ++j) {
+      const uint32_t r = threadIdx.x * per + j;
+      if (r < cnt) woff[r] = pre;
+      pre += w[j];
+    }
+    if (threadIdx.x == 0) woff[cnt] = total;
+    __syncthreads();
+    for (uint64_t x = gwarp; x < total; x += gwarps) {
+      uint32_t lo = 0, hi = cnt;  // last row with woff <= x
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (woff[mid] <= x)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint32_t v = big[base + lo];
+      const uint64_t b = off[v] + (x - woff[lo]) * 32, e = min(off[v + 1], b + 32);
+      drop(b, e);
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void k_frontier_init(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint32_t* __restrict__ deg,
                                 uint32_t* __restrict__ rem, uint32_t k, uint32_t tag, uint32_t* __restrict__ front,
                                 unsigned long long* fcnt, uint64_t cap, uint32_t* err) {
@@ -79,7 +137,7 @@ __global__ void k_frontier_init(const uint32_t* __restrict__ alive, uint64_t n_a
   }
 }
 
-// Removes the frontier: warp per vertex; rows longer than kBigRow go to the
+// Removes the frontier: warp per vertex; rows longer than big_row go to the
 // big list for k_expand_big.
 __global__ void k_expand(const uint32_t* __restrict__ front, uint64_t nf, const uint64_t* __restrict__ off,
                          const uint32_t* __restrict__ adj, uint32_t* __restrict__ deg, uint32_t* __restrict__ rem,
@@ -309,7 +367,7 @@ struct ProbeArgs {
   unsigned long long* cnt;  // [0..2] frontier sizes, [3..4] big-row counts, [5] rounds, [6] removed
   uint64_t cap;
   uint32_t k, tag;
-  uint32_t big_row;  // rows longer than this are expanded by whole blocks
+  uint32_t big_row;  // rows longer than this are dealt to all warps in windows
   DevWords* words;
   unsigned long long timeout_ns;
 };
@@ -335,6 +393,8 @@ __device__ __forceinline__ void drop_neighbours(const ProbeArgs& A, uint64_t b, 
 
 // A whole probe (frontier init and every round) in one cooperative launch.
 __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
+  __shared__ uint64_t woff[kBigBatch + 1];
+  __shared__ uint64_t wtmp[33];
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
@@ -383,13 +443,9 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
     if (!grid_barrier(A.words, A.timeout_ns)) return;
     const uint64_t nbig = ld_acquire_u64(bc);
     if (nbig) {
-      // Rows longer than kBigRow: one block per row, warps on 32-entry windows.
-      for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-        const uint32_t v = A.big[bi];
-        const uint64_t b = A.off[v], e = A.off[v + 1];
-        for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x)
-          drop_neighbours(A, j0, min(e, j0 + 32), nx, nc);
-      }
+      // Rows longer than big_row: their 32-entry windows dealt to every warp.
+      deal_big_windows(A.big, nbig, A.off, woff, wtmp,
+                       [&](uint64_t b, uint64_t e) { drop_neighbours(A, b, e, nx, nc); });
       if (!grid_barrier(A.words, A.timeout_ns)) return;
     }
     ++i;
@@ -431,7 +487,7 @@ struct DecompArgs {
   unsigned long long* cnt;
   uint64_t n_list;     // entries of list[0] at launch
   uint64_t cap;
-  uint32_t big_row;    // rows longer than this are expanded by whole blocks
+  uint32_t big_row;    // rows longer than this are dealt to all warps in windows
   uint32_t window;     // levels per window (>= 1)
   DevWords* words;
   unsigned long long timeout_ns;
@@ -479,6 +535,8 @@ __device__ __forceinline__ unsigned long long block_read(const unsigned long lon
 
 __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
   __shared__ unsigned long long sh;
+  __shared__ uint64_t woff[kBigBatch + 1];
+  __shared__ uint64_t wtmp[33];
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t gwarps = gthreads >> 5, gwarp = gtid >> 5;
@@ -596,12 +654,8 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
       if (!grid_barrier(A.words, A.timeout_ns)) return;
       const uint64_t nbig = block_read(bc, &sh);
       if (nbig) {
-        for (uint64_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-          const uint32_t v = A.big[bi];
-          const uint64_t b = A.off[v], e = A.off[v + 1];
-          for (uint64_t j0 = b + warp_id() * 32; j0 < e; j0 += blockDim.x)
-            drop_neighbours_core(A, j0, min(e, j0 + 32), R);
-        }
+        deal_big_windows(A.big, nbig, A.off, woff, wtmp,
+                         [&](uint64_t b, uint64_t e) { drop_neighbours_core(A, b, e, R); });
         if (!grid_barrier(A.words, A.timeout_ns)) return;
       }
       ++i;

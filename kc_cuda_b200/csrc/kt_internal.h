@@ -54,7 +54,7 @@ struct Options {
   int64_t debug_checks = 0;       // extra host-side consistency checks
   int64_t verbose = 0;            // stage decisions on stderr
   int64_t pool_reserve_mb = 0;    // setting it grows the memory pool by this much at once
-  int64_t kcore_big_row = 2048;   // k-core rounds: rows longer than this are expanded by whole blocks
+  int64_t kcore_big_row = 512;    // k-core rounds: longer rows are dealt to all warps in 32-entry windows
   int64_t peel_search_ratio = 16; // peel: binary-search the long row when it is this many times longer
   int64_t dense_tile_mb = 48;     // dense support: bitset rows of two tile blocks within this many MB
   int64_t kcore_blocks_per_sm = 0;  // core decomposition: resident blocks per SM (0 = as many as fit)

@@ -38,7 +38,7 @@ const std::vector<Param>& params() {
       {"dense_min_fill", &Options::dense_min_fill, {4, 8, 16, 32, 64, 128}},
       {"dense_max_n", &Options::dense_max_n, {16384, 32768, 65536, 131072}},
       {"support_bitmap_max_n", &Options::support_bitmap_max_n, {1 << 17, 1 << 18, 1 << 19, 1 << 20}},
-      {"kcore_big_row", &Options::kcore_big_row, {512, 1024, 2048, 4096, 8192}},
+      {"kcore_big_row", &Options::kcore_big_row, {64, 128, 256, 512, 1024, 2048}},
       {"peel_search_ratio", &Options::peel_search_ratio, {4, 8, 16, 32, 64}},
       {"dense_tile_mb", &Options::dense_tile_mb, {12, 24, 48, 96}},
       {"kcore_blocks_per_sm", &Options::kcore_blocks_per_sm, {0, 1, 2, 4}},
