@@ -73,7 +73,9 @@ const char* kt_status_string(kt_status s);
  *   kcore_blocks_per_sm (0)     core decomposition: resident blocks per SM of its
  *                               one cooperative launch (0 = as many as fit)
  *   kcore_window (32)           core decomposition: levels per pass over the whole
- *                               alive list (passes between read window candidates) */
+ *                               alive list (passes between read window candidates)
+ *   peel_bitset (1)             peel: intersect dense rows as bitsets (AND of two
+ *                               rows) when the rows are shorter than the lists */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 
@@ -150,8 +152,8 @@ kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_
 /* Autotuner of the kernels' bin and tile thresholds (no counterpart in the
  * reference, whose thresholds are compile-time constants): the options
  * recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n,
- * kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm and
- * kcore_window.  Solves the graphs of
+ * kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm,
+ * kcore_window and peel_bitset.  Solves the graphs of
  * `sample` repeatedly, one candidate value at a time (coordinate descent from
  * the context's current settings, up to `passes` sweeps, device time by CUDA
  * events, a 2% margin against noise), checks that every candidate leaves
@@ -160,7 +162,7 @@ kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_
  * solved, but not those graphs themselves. */
 typedef struct kt_tune_result {
   int64_t recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n;
-  int64_t kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm, kcore_window;
+  int64_t kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm, kcore_window, peel_bitset;
   double ms_first;  /* the sample's device time with the settings at entry */
   double ms_best;   /* ... with the chosen settings */
   uint32_t trials;  /* timed candidate runs */

@@ -28,6 +28,13 @@ struct DenseRows {
   const uint64_t* roff;
   const uint32_t* rw;
   const uint32_t* cbase;
+  const uint32_t* sbits;  // rows as built (may be null)
+  const uint32_t* spre;   // set bits of the built row before each word
+  // Position of neighbour column `col` in row u's sorted adjacency.
+  __device__ __forceinline__ uint32_t rank(uint32_t u, uint32_t col) const {
+    const uint64_t w = off(u) + (col >> 5);
+    return spre[w] + __popc(sbits[w] & ((1u << (col & 31)) - 1u));
+  }
   __device__ __forceinline__ uint64_t off(uint32_t u) const { return roff ? roff[u] : (uint64_t)u * W; }
   __device__ __forceinline__ uint32_t words(uint32_t u) const { return roff ? rw[u] : W; }
   // Bit position of neighbour v in row u.
@@ -38,7 +45,7 @@ inline DenseRows dense_rows(const Sub& s) {
   const bool grouped = s.roff.get() != nullptr;
   return DenseRows{const_cast<uint32_t*>(s.bits.as<uint32_t>()), s.W,
                    grouped ? s.roff.as<uint64_t>() : nullptr, grouped ? s.rw.as<uint32_t>() : nullptr,
-                   grouped ? s.vbase.as<uint32_t>() : nullptr};
+                   grouped ? s.vbase.as<uint32_t>() : nullptr, s.sbits.as<uint32_t>(), s.spre.as<uint32_t>()};
 }
 
 // Loads of row v in flight per lane.

@@ -59,6 +59,7 @@ struct Options {
   int64_t dense_tile_mb = 48;     // dense support: bitset rows of two tile blocks within this many MB
   int64_t kcore_blocks_per_sm = 0;  // core decomposition: resident blocks per SM (0 = as many as fit)
   int64_t kcore_window = 32;      // core decomposition: levels per pass over the whole alive list
+  int64_t peel_bitset = 1;        // peel: dense rows intersected as bitsets when shorter than the lists
 };
 
 // Stage decisions on stderr when the context's verbose option is set.

@@ -55,7 +55,7 @@ struct PeelArgs {
   const uint32_t* alive;
   uint64_t na;
   uint32_t* front[2];
-  unsigned long long* cnt;  // 3 rotating frontier counters + [3] rounds done + [4] decrements
+  unsigned long long* cnt;  // 3 rotating frontier counters, [3] rounds done, [5] recount rounds
   uint64_t cap;
   uint32_t thr;    // remove support < thr
   uint32_t tval;   // trussness recorded for removed edges
@@ -153,6 +153,36 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
   const uint64_t na = xe - xb, nb = ye - yb;
   uint32_t* err = &A.words->err;
   const unsigned lane = lane_id();
+  if (A.R.sbits && (uint64_t)A.R.words(x) <= na + nb) {
+    // Dense rows shorter than the two lists: AND the two bitset rows (32
+    // words a step, one per lane); each common neighbour's edge ids come from
+    // its position in the sorted rows, a popcount of the rows as built.  Bits
+    // of edges deleted in earlier cascades are clear; deletions of this
+    // cascade are caught by close_triangle's state test, as in the merge.
+    const uint32_t* rx = A.R.bits + A.R.off(x);
+    const uint32_t* ry = A.R.bits + A.R.off(y);
+    const uint32_t W = A.R.words(x);
+    const uint64_t ox = A.off[x], oy = A.off[y];
+    for (uint32_t i0 = 0; i0 < W; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      uint32_t mset = i < W ? __ldcg(rx + i) & __ldcg(ry + i) : 0u;
+      while (__any_sync(kFull, mset != 0)) {
+        bool pa = false, pb = false;
+        uint32_t a = 0, b = 0;
+        if (mset) {
+          const uint32_t col = i * 32 + (uint32_t)(__ffs(mset) - 1);
+          mset &= mset - 1;
+          a = A.eid[ox + A.R.rank(x, col)];
+          b = A.eid[oy + A.R.rank(y, col)];
+          close_triangle(A, e, a, b, r, thr, pa, pb, ndec);
+        }
+        push_warp_full(pa, a, next, ncnt, A.cap, err);
+        push_warp_full(pb, b, next, ncnt, A.cap, err);
+      }
+    }
+    tdec += ndec;
+    return;
+  }
   if (nb > (uint64_t)A.search_ratio * na) {
     // Short row against a long one: binary search per lane.
     for (uint64_t q = xb + lane; q < xb + ((na + 31) & ~31ULL); q += 32) {
@@ -286,7 +316,7 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
   uint64_t tdeg = 0, tdec = 0, trec = 0;
   uint64_t alive = A.na;
   uint32_t cleared = A.r0 - 1;  // bits are current for deletions up to this round
-  uint32_t i = 0;
+  uint32_t i = 0, nrec = 0;
   bool ok = true;
   while (true) {
     const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
@@ -299,6 +329,7 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
     const bool recount = A.R.bits && (double)nf * (double)(thr > 0 ? thr : 1) * (double)A.gamma >
                                          (double)alive * (double)A.wavg;
     if (recount) {
+      ++nrec;
       clear_deleted(A, cleared, r, gtid, gthreads);
       cleared = r;
       if (!grid_barrier(A.words, A.timeout_ns)) {
@@ -321,7 +352,10 @@ __global__ void __launch_bounds__(kPeelThreads) k_cascade(PeelArgs A) {
   if (ok && A.R.bits) clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
   flush_tallies(A, tdeg, tdec);
   if (lane_id() == 0 && trec) atomicAdd(&A.acct[2], (unsigned long long)trec);
-  if (gtid == 0) A.cnt[3] = i;
+  if (gtid == 0) {
+    A.cnt[3] = i;
+    A.cnt[5] = nrec;
+  }
 }
 
 // Host-stepped variant (one launch per round), used when cooperative launch
@@ -520,7 +554,8 @@ struct Peeler {
     A.r0 = r;
     A.adeg = adeg.as<uint32_t>();
     A.acct = acct.as<unsigned long long>();
-    A.R = s->W ? dense_rows(*s) : DenseRows{nullptr, 0, nullptr, nullptr, nullptr};
+    A.R = s->W ? dense_rows(*s) : DenseRows{nullptr, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (!c->opt.peel_bitset) A.R.sbits = nullptr;
     A.wavg = s->W ? (float)((double)s->bit_words / std::max<uint32_t>(s->n, 1)) : 0.f;
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.search_ratio = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.peel_search_ratio), 1 << 20);
@@ -539,14 +574,17 @@ struct Peeler {
     zero(c, cnt.get(), cnt.bytes());
     cudaEvent_t e0;
     c->timer.begin(c->stream, &c->stats.ms_peel_kernel, &e0);
-    uint64_t rounds = 0;
+    uint64_t rounds = 0, recounts = 0;
     scanned += na;
     const auto t_start = std::chrono::steady_clock::now();
     if (coop_grid) {
       void* p[] = {&A};
       KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, smem, c->stream));
       KT_LAUNCHED(c);
-      rounds = read_word<unsigned long long>(c, A.cnt + 3);
+      uint64_t h[3];
+      copy_d2h(c, h, A.cnt + 3, sizeof(h));
+      rounds = h[0];
+      recounts = h[2];
     } else {
       k_level_frontier<<<grid_for(na, kPeelThreads, c->num_sms * 16), kPeelThreads, 0, c->stream>>>(A);
       KT_LAUNCHED(c);
@@ -562,8 +600,9 @@ struct Peeler {
     c->timer.end(c->stream, e0, &c->stats.ms_peel_kernel);
     c->stats.peel_launches++;
     check_words(c, "truss peel");
-    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds, %.3f ms\n", t,
+    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds (%llu recount), %.3f ms\n", t,
            (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds,
+           (unsigned long long)recounts,
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     r += (uint32_t)rounds + 1;
     res->rounds += rounds;

@@ -25,6 +25,10 @@ struct Sub {
   uint32_t W = 0;   // 0 = not built
   DBuf roff, rw;
   uint64_t bit_words = 0;  // words of all rows
+  // Dense mode, when the budget allows: the rows as built (never cleared) and
+  // the set bits before each of their words, so the position of neighbour v
+  // in row u's sorted adjacency is a popcount away (peel intersections).
+  DBuf sbits, spre;
   // Dense mode: edge ids in tile order (u >> tb, v >> tb, u, v), so that the
   // rows read by concurrently processed edges stay within two vertex blocks
   // whose bitsets fit in L2 together.

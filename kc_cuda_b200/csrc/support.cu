@@ -123,6 +123,23 @@ __global__ void k_bits_build(uint32_t n, const uint64_t* __restrict__ off, const
   }
 }
 
+// spre[w] = set bits of row u before its word w (warp per row).
+__global__ void k_row_prefix(uint32_t n, DenseRows R, uint32_t* __restrict__ spre) {
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t u = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); u < n; u += warps) {
+    const uint64_t base = R.off((uint32_t)u);
+    const uint32_t W = R.words((uint32_t)u);
+    uint32_t run = 0;
+    for (uint32_t i0 = 0; i0 < W; i0 += 32) {
+      const uint32_t i = i0 + lane_id();
+      const uint32_t pc = i < W ? __popc(R.bits[base + i]) : 0u;
+      const uint32_t inc = warp_incl_scan(pc);
+      if (i < W) spre[base + i] = run + inc - pc;
+      run += __shfl_sync(kFull, inc, 31);
+    }
+  }
+}
+
 // Per-graph rows of a grouped union: graph g's rows hold gw[g] words and
 // start at word gbase[g].
 __global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, const uint32_t* __restrict__ vbase,
@@ -225,6 +242,8 @@ uint32_t support_bound(Ctx* c, const uint32_t* sup, uint64_t m, uint32_t cap) {
 bool build_bits(Ctx* c, Sub& s) {
   s.W = 0;
   s.bits.release();
+  s.sbits.release();
+  s.spre.release();
   s.roff.release();
   s.rw.release();
   s.bit_words = 0;
@@ -274,6 +293,18 @@ bool build_bits(Ctx* c, Sub& s) {
   k_bits_build<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
       s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), dense_rows(s));
   KT_LAUNCHED(c);
+  // The rows as built and their per-word prefix counts (positions of
+  // neighbours for the peel), when two more copies fit the budget.
+  s.sbits.release();
+  s.spre.release();
+  if (!c->budget || c->in_use + 3 * bytes <= c->budget) {
+    s.sbits.alloc(c, bytes);
+    s.spre.alloc(c, bytes);
+    KT_CUDA(cudaMemcpyAsync(s.sbits.get(), s.bits.get(), bytes, cudaMemcpyDeviceToDevice, c->stream));
+    k_row_prefix<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        s.n, dense_rows(s), s.spre.as<uint32_t>());
+    KT_LAUNCHED(c);
+  }
   // Tile order: blocks of 2^tb vertices, two blocks' bitsets within ~48 MB.
   uint32_t tb = 16;
   const uint64_t tile_bytes = (uint64_t)std::max<int64_t>(1, c->opt.dense_tile_mb) << 20;

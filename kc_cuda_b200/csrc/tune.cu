@@ -5,7 +5,7 @@
 // dense support's tile-block size, the peel's switch from the 32-wide tile
 // merge to per-lane binary search, the cost ratio that turns a peel round
 // into an AND/popcount recount, the core decomposition's blocks per SM and
-// levels per window).
+// levels per window, the peel's bitset intersection of dense rows).
 //
 // The tuner times a sample batch -- graphs like the ones the caller will
 // solve -- under candidate values, one parameter at a time (coordinate
@@ -43,6 +43,7 @@ const std::vector<Param>& params() {
       {"dense_tile_mb", &Options::dense_tile_mb, {12, 24, 48, 96}},
       {"kcore_blocks_per_sm", &Options::kcore_blocks_per_sm, {0, 1, 2, 4}},
       {"kcore_window", &Options::kcore_window, {8, 16, 32, 64, 128}},
+      {"peel_bitset", &Options::peel_bitset, {0, 1}},
   };
   return p;
 }
@@ -87,6 +88,7 @@ void fill_result(const Options& o, kt_tune_result* r) {
   r->dense_tile_mb = o.dense_tile_mb;
   r->kcore_blocks_per_sm = o.kcore_blocks_per_sm;
   r->kcore_window = o.kcore_window;
+  r->peel_bitset = o.peel_bitset;
 }
 
 }  // namespace

@@ -165,14 +165,17 @@ def test_without_prediction_same_answer(ctx, golden):
         ctx.set_option("predict", 1)
 
 
-@pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never", "dense_uncapped"])
+@pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never", "dense_uncapped",
+                                  "dense_merge_only"])
 def test_modes_support_trussness_answer(ctx, golden, mode):
-    """Sparse lists vs dense bitsets, and dense peels that recount every
-    round vs never: all bit-identical to the oracle."""
+    """Sparse lists vs dense bitsets, dense peels that recount every round vs
+    never, and dense peels that intersect sorted lists instead of bitset
+    rows: all bit-identical to the oracle."""
     opts = {"sparse": {"dense_max_n": 0},
             "dense_recount_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1 << 30},
             "dense_recount_never": {"dense_min_fill": 1 << 30, "recount_gamma": 1},
-            "dense_uncapped": {"dense_min_fill": 1 << 30, "capped_support": 0}}[mode]
+            "dense_uncapped": {"dense_min_fill": 1 << 30, "capped_support": 0},
+            "dense_merge_only": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_bitset": 0}}[mode]
     old = {k: ctx.get_option(k) for k in opts}
     for k, v in opts.items():
         ctx.set_option(k, v)
