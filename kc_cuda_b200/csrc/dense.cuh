@@ -48,9 +48,10 @@ inline DenseRows dense_rows(const Sub& s) {
                    grouped ? s.vbase.as<uint32_t>() : nullptr, s.sbits.as<uint32_t>(), s.spre.as<uint32_t>()};
 }
 
-// Loads of row v in flight per lane.
+// 16-byte loads of row v in flight per lane.  Rows are whole 16-byte vectors
+// (W a multiple of 4, rows 16-byte aligned; the padding words stay zero).
 #ifndef KT_DENSE_DEPTH
-#define KT_DENSE_DEPTH 16
+#define KT_DENSE_DEPTH 4
 #endif
 constexpr int kDenseDepth = KT_DENSE_DEPTH;
 
@@ -58,32 +59,34 @@ constexpr int kDenseDepth = KT_DENSE_DEPTH;
 inline size_t dense_smem_bytes(uint32_t W, unsigned threads) { return (size_t)(threads / 32) * W * 4; }
 
 __device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ p, uint32_t W, uint32_t* su) {
-  for (uint32_t i = lane_id(); i < W; i += 32) su[i] = p[i];
+  const uint4* p4 = reinterpret_cast<const uint4*>(p);
+  uint4* s4 = reinterpret_cast<uint4*>(su);
+  for (uint32_t i = lane_id(); i < W / 4; i += 32) s4[i] = p4[i];
   __syncwarp();
 }
 
-// popcount(row u & row v) over words [w0, w1); every lane returns the warp
-// total.  Row v is read 16 strides at a time (16 loads in flight per lane,
-// L2-only caching: each row v is used once per edge).
+__device__ __forceinline__ uint32_t popc_and4(uint4 a, uint4 b) {
+  return __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+}
+
+// popcount(row u & row v) over words [w0, w1) (multiples of 4); every lane
+// returns the warp total.  Lanes read 16-byte vectors, kDenseDepth strides
+// of the warp at a time (L2-only caching: each row v is used once per edge).
 __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
                                                    uint32_t w1) {
+  const uint4* p4 = reinterpret_cast<const uint4*>(p);
+  const uint4* s4 = reinterpret_cast<const uint4*>(su);
   uint32_t s = 0;
-  uint32_t i = w0 + lane_id();
-  for (; i + (kDenseDepth - 1) * 32 < w1; i += kDenseDepth * 32) {
-    uint32_t a[kDenseDepth];
+  uint32_t i = w0 / 4 + lane_id();
+  const uint32_t e = w1 / 4;
+  for (; i + (kDenseDepth - 1) * 32 < e; i += kDenseDepth * 32) {
+    uint4 a[kDenseDepth];
 #pragma unroll
-    for (int k = 0; k < kDenseDepth; ++k) a[k] = __ldcg(p + i + 32 * k);
+    for (int k = 0; k < kDenseDepth; ++k) a[k] = __ldcg(p4 + i + 32 * k);
 #pragma unroll
-    for (int k = 0; k < kDenseDepth; ++k) s += __popc(su[i + 32 * k] & a[k]);
+    for (int k = 0; k < kDenseDepth; ++k) s += popc_and4(s4[i + 32 * k], a[k]);
   }
-  for (; i + 3 * 32 < w1; i += 4 * 32) {
-    uint32_t a[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) a[k] = __ldcg(p + i + 32 * k);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) s += __popc(su[i + 32 * k] & a[k]);
-  }
-  for (; i < w1; i += 32) s += __popc(su[i] & __ldcg(p + i));
+  for (; i < e; i += 32) s += popc_and4(s4[i], __ldcg(p4 + i));
   return warp_sum(s);
 }
 

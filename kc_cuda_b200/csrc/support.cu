@@ -156,7 +156,7 @@ template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
                                                        uint32_t* __restrict__ sup) {
-  extern __shared__ uint32_t dense_smem[];
+  extern __shared__ __align__(16) uint32_t dense_smem[];
   uint32_t* su = dense_smem + warp_id() * R.W;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t groups = (m + 31) / 32;
@@ -261,13 +261,13 @@ bool build_bits(Ctx* c, Sub& s) {
     gw.resize(s.group_n.size());
     for (size_t g = 0; g < s.group_n.size(); ++g) {
       gbase[g] = words;
-      gw[g] = (s.group_n[g] + 31) / 32;
+      gw[g] = ((s.group_n[g] + 31) / 32 + 3) & ~3u;  // rows of whole 16-byte vectors
       words += (uint64_t)s.group_n[g] * gw[g];
       W = std::max(W, gw[g]);
     }
   } else {
     if ((int64_t)s.n > c->opt.dense_max_n) return false;
-    W = (s.n + 31) / 32;
+    W = ((s.n + 31) / 32 + 3) & ~3u;  // rows of whole 16-byte vectors
     words = (uint64_t)s.n * W;
   }
   // Dense enough: adjacency entries * fill >= words of all rows.
