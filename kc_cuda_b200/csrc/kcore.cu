@@ -308,32 +308,89 @@ __global__ void k_compact_rows(const uint32_t* __restrict__ alive, uint64_t na, 
   }
 }
 
-// Rows longer than kBigRow in the compaction: one block per row, tiles of
-// blockDim entries with a block scan for the output positions.
-__global__ void k_compact_big_rows(const uint32_t* __restrict__ alive, uint64_t na, const uint64_t* __restrict__ off,
-                                   const uint32_t* __restrict__ adj, const uint32_t* __restrict__ rem,
-                                   const uint32_t* __restrict__ newid, const uint64_t* __restrict__ noff,
-                                   uint32_t* __restrict__ nadj) {
-  __shared__ uint32_t tmp[33];
-  for (uint64_t i = blockIdx.x; i < na; i += gridDim.x) {
+// Alive-list indices whose rows are longer than kBigRow (compacted apart).
+struct BigAliveRow {
+  const uint32_t* alive;
+  const uint64_t* off;
+  __device__ bool keep(uint64_t i) const {
     const uint32_t v = alive[i];
-    const uint64_t b = off[v], e = off[v + 1];
-    if (e - b <= kBigRow) continue;  // uniform per block
-    uint64_t pos = noff[i];
-    const uint64_t end = noff[i + 1];
-    for (uint64_t j0 = b; j0 < e; j0 += blockDim.x) {
-      const uint64_t j = j0 + threadIdx.x;
-      uint32_t w = 0;
-      uint32_t keep = 0;
-      if (j < e) {
-        w = adj[j];
-        keep = rem[w] == kAlive;
+    return off[v + 1] - off[v] > kBigRow;
+  }
+  __device__ uint32_t value(uint64_t i) const { return (uint32_t)i; }
+};
+
+// Rows longer than kBigRow in the compaction: their 32-entry windows are
+// dealt to every warp of the grid (each block lists the rows' first window
+// numbers with the same block scan, kBigBatch rows at a time); a window's
+// kept entries go to the row's next free positions (a per-row cursor), so a
+// hub row is spread over the whole GPU.  Entry order within these rows is not
+// kept; nothing downstream needs it.
+__global__ void __launch_bounds__(256) k_compact_big_rows(const uint32_t* __restrict__ rows, uint64_t nrows,
+                                                          const uint32_t* __restrict__ alive,
+                                                          const uint64_t* __restrict__ off,
+                                                          const uint32_t* __restrict__ adj,
+                                                          const uint32_t* __restrict__ rem,
+                                                          const uint32_t* __restrict__ newid,
+                                                          const uint64_t* __restrict__ noff,
+                                                          uint32_t* __restrict__ cursor, uint32_t* __restrict__ nadj) {
+  __shared__ uint64_t woff[kBigBatch + 1];
+  __shared__ uint64_t tmp[33];
+  const uint64_t gwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
+  constexpr unsigned per = kBigBatch / 256;  // rows per thread
+  for (uint64_t base = 0; base < nrows; base += kBigBatch) {
+    const uint64_t left = nrows - base;
+    const uint32_t cnt = left < kBigBatch ? (uint32_t)left : kBigBatch;
+    uint64_t w[per];
+    uint64_t sum = 0;
+#pragma unroll
+    for (unsigned j = 0; j < per; ++j) {
+      const uint32_t r = threadIdx.x * per + j;
+      w[j] = 0;
+      if (r < cnt) {
+        const uint32_t v = alive[rows[base + r]];
+        w[j] = (off[v + 1] - off[v] + 31) / 32;
       }
-      uint32_t total;
-      const uint32_t r = block_excl_scan<uint32_t>(keep, tmp, &total);
-      if (keep && pos + r < end) nadj[pos + r] = newid[w];
-      pos += total;
+      sum += w[j];
     }
+    uint64_t total;
+    uint64_t pre = block_excl_scan<uint64_t>(sum, tmp, &total);
+#pragma unroll
+    for (unsigned j = 0; j < per; ++j) {
+      const uint32_t r = threadIdx.x * per + j;
+      if (r < cnt) woff[r] = pre;
+      pre += w[j];
+    }
+    if (threadIdx.x == 0) woff[cnt] = total;
+    __syncthreads();
+    for (uint64_t x = gwarp; x < total; x += gwarps) {
+      uint32_t lo = 0, hi = cnt;  // last row with woff <= x
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (woff[mid] <= x)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint32_t i = rows[base + lo];
+      const uint32_t v = alive[i];
+      const uint64_t j = off[v] + (x - woff[lo]) * 32 + lane_id();
+      bool keep = false;
+      uint32_t nb = 0;
+      if (j < off[v + 1]) {
+        const uint32_t u = adj[j];
+        keep = rem[u] == kAlive;
+        if (keep) nb = newid[u];
+      }
+      const unsigned bal = __ballot_sync(kFull, keep);
+      if (!bal) continue;
+      uint32_t at = 0;
+      if (lane_id() == 0) at = atomicAdd(&cursor[base + lo], (uint32_t)__popc(bal));
+      at = __shfl_sync(kFull, at, 0);
+      const uint64_t p = noff[i] + at + __popc(bal & lanemask_lt());
+      if (keep && p < noff[i + 1]) nadj[p] = nb;
+    }
+    __syncthreads();
   }
 }
 
@@ -733,10 +790,20 @@ void KCore::compact_to_alive(Ctx* c, uint32_t level) {
       alive.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
       newid.as<uint32_t>(), L.off.as<uint64_t>(), L.adj.as<uint32_t>());
   KT_LAUNCHED(c);
-  k_compact_big_rows<<<c->num_sms * 8, 256, 0, c->stream>>>(
-      alive.as<uint32_t>(), na, g.off.as<uint64_t>(), g.adj.as<uint32_t>(), rem.as<uint32_t>(),
-      newid.as<uint32_t>(), L.off.as<uint64_t>(), L.adj.as<uint32_t>());
-  KT_LAUNCHED(c);
+  {
+    DBuf rows(c, (na ? na : 1) * sizeof(uint32_t));
+    const uint64_t nbig = compact(c, na, BigAliveRow{alive.as<uint32_t>(), g.off.as<uint64_t>()},
+                                  rows.as<uint32_t>());
+    if (nbig) {
+      DBuf cursor(c, nbig * sizeof(uint32_t));
+      zero(c, cursor.get(), cursor.bytes());
+      k_compact_big_rows<<<c->num_sms * 8, 256, 0, c->stream>>>(
+          rows.as<uint32_t>(), nbig, alive.as<uint32_t>(), g.off.as<uint64_t>(), g.adj.as<uint32_t>(),
+          rem.as<uint32_t>(), newid.as<uint32_t>(), L.off.as<uint64_t>(), cursor.as<uint32_t>(),
+          L.adj.as<uint32_t>());
+      KT_LAUNCHED(c);
+    }
+  }
   L.max_deg = g.max_deg;  // an upper bound is enough here
   newid.release();
   // Install (the old local graph, if any, is released by the swap).

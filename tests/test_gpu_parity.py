@@ -75,6 +75,44 @@ def test_csr_matches_oracle_clean(ctx, golden):
         assert np.array_equal(g.edges(), want), name
 
 
+def random_record_bytes(seed: int, lines: int) -> bytes:
+    """Lines of two digit runs in the parser's grammar with every kind of
+    byte around them: runs of 1 to 12 "digits" (leading zeros, then up to 4
+    significant bytes from 0x30..0x7f, so letters count as digits worth up
+    to 79; values stay below 10^5), separators of 1 to 3 bytes from tab,
+    space, comma, CR, control bytes, '/', NUL and bytes >= 0x80 (negative as
+    signed char), optional trailing columns, CRLF endings and blank lines."""
+    rng = np.random.default_rng(seed)
+    seps = [b"\t", b" ", b",", b"\r", b"\x01", b"/", b"\x80", b"\xff", b"\x1f", b"\x00"]
+    out = bytearray()
+    for _ in range(lines):
+        kind = rng.integers(0, 20)
+        if kind == 0:
+            out += b"".join(seps[i] for i in rng.integers(0, 5, rng.integers(0, 4))) + b"\n"
+            continue
+        parts = []
+        for _ in range(2 + (rng.integers(0, 3) if kind == 1 else 0)):
+            lead = b"".join(seps[i] for i in rng.integers(0, len(seps), rng.integers(1, 4) if parts else rng.integers(0, 3)))
+            total = int(rng.choice([1, 2, 3, 5, 7, 8, 8, 8, 9, 10, 12]))
+            sig = min(total, int(rng.integers(1, 5)))
+            hi = 0x80 if rng.integers(0, 6) == 0 else 0x3A
+            run = b"0" * (total - sig) + bytes(rng.integers(0x30, hi, sig, dtype=np.uint8))
+            parts.append(lead + run)
+        out += b"".join(parts) + (b"\r\n" if rng.integers(0, 5) == 0 else b"\n")
+    return bytes(out)
+
+
+def test_parse_random_bytes(ctx):
+    """The device parser (8-byte, byte-window and byte-loop paths) against the
+    oracle's restatement of the reference grammar on mixed byte soup."""
+    for seed in range(4):
+        data = random_record_bytes(seed, 60_000)
+        want = O.clean(O.parse(data))
+        g = ctx.load_tsv(data)
+        assert np.array_equal(g.edges(), want), seed
+        g.free()
+
+
 def test_csr_large_random_pairs(ctx):
     rng = np.random.default_rng(5)
     n = 1 << 18
@@ -124,9 +162,10 @@ def test_core_numbers_and_kcore(ctx, golden):
 @pytest.mark.parametrize("persistent", [1, 0])
 def test_core_numbers_generated(ctx, persistent):
     """Core numbers of larger generated graphs by the one-launch level loop
-    (persistent=1) and by host-stepped probes (persistent=0): R-MAT hubs with
-    rows above the whole-block threshold (2048), a Chung-Lu graph, a mix
-    graph, and a small graph with isolated vertex ids."""
+    (persistent=1) and by host-stepped probes (persistent=0), and k-core
+    membership by the maximum-core search: R-MAT hubs with rows above the
+    big-row thresholds (512 in the rounds, 2048 in the compaction), a
+    Chung-Lu graph, a mix graph, and a small graph with isolated vertex ids."""
     specs = [
         gen.rmat(15, 24, 5, [40]),
         gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=200_000, draws=1_500_000, seed=9, cl_w_max=20_000.0),
@@ -143,6 +182,13 @@ def test_core_numbers_generated(ctx, persistent):
             want = O.core_numbers(edges, n)
             got = d.core_numbers()
             assert np.array_equal(got, want), (spec, persistent)
+            # k-core membership through the maximum-core search (compacted
+            # copies of the core, hub rows included).
+            cmax = int(want.max()) if n else 0
+            for k in sorted({2, max(1, cmax // 4), max(1, cmax // 2), cmax}):
+                mem, cm = d.kmax_core(k)
+                assert cm == cmax, (spec, k)
+                assert np.array_equal(mem, want >= k), (spec, k)
             d.free()
     finally:
         ctx.set_option("persistent", 1)
