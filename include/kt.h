@@ -75,7 +75,10 @@ const char* kt_status_string(kt_status s);
  *   kcore_window (32)           core decomposition: levels per pass over the whole
  *                               alive list (passes between read window candidates)
  *   peel_bitset (1)             peel: intersect dense rows as bitsets (AND of two
- *                               rows) when the rows are shorter than the lists */
+ *                               rows) when the rows are shorter than the lists
+ *   peel_split (16)             peel: a round whose frontier edges x 8-word row
+ *                               chunks <= this x warps deals (edge, chunk) units
+ *                               to warps instead of edges (0 = off) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 
@@ -153,7 +156,7 @@ kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_
  * reference, whose thresholds are compile-time constants): the options
  * recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n,
  * kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm,
- * kcore_window and peel_bitset.  Solves the graphs of
+ * kcore_window, peel_bitset and peel_split.  Solves the graphs of
  * `sample` repeatedly, one candidate value at a time (coordinate descent from
  * the context's current settings, up to `passes` sweeps, device time by CUDA
  * events, a 2% margin against noise), checks that every candidate leaves
@@ -163,6 +166,7 @@ kt_status kt_load_mix_graph(kt_ctx* ctx, uint64_t index, uint64_t base_seed, kt_
 typedef struct kt_tune_result {
   int64_t recount_gamma, dense_min_fill, dense_max_n, support_bitmap_max_n;
   int64_t kcore_big_row, peel_search_ratio, dense_tile_mb, kcore_blocks_per_sm, kcore_window, peel_bitset;
+  int64_t peel_split;
   double ms_first;  /* the sample's device time with the settings at entry */
   double ms_best;   /* ... with the chosen settings */
   uint32_t trials;  /* timed candidate runs */

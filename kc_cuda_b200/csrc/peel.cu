@@ -65,6 +65,7 @@ struct PeelArgs {
   float wavg;      // mean words per bitset row
   uint32_t gamma;  // recount round when nf * thr * gamma > alive * wavg
   uint32_t search_ratio;  // binary-search the long row when it is this many times longer
+  uint32_t split;         // split rounds when frontier x chunks <= split x warps (0 = never)
   unsigned long long* acct;  // [0] sum of alive degrees of deleted edges, [1] decrements, [2] recounted edges
   DevWords* words;
   unsigned long long timeout_ns;
@@ -233,6 +234,90 @@ __device__ __forceinline__ void peel_edge(const PeelArgs& A, uint32_t e, uint32_
   tdec += ndec;
 }
 
+// Rounds with few frontier edges split each edge's bitset intersection into
+// chunks of kSplitWords words, one warp per (edge, chunk), so a small
+// frontier of edges with many triangles keeps the whole grid busy.
+constexpr uint32_t kSplitWords = 8;
+
+// Position of the r-th (from 0) set bit of m.
+__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s >= 1; s >>= 1) {
+    const uint32_t low = __popc(m & ((1u << s) - 1u));
+    if (r >= low) {
+      r -= low;
+      m >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
+// Words [w0, w0 + kSplitWords) of frontier edge e's two bitset rows: the
+// common neighbours found there are dealt one per lane (a warp scan of the
+// words' popcounts, then a 3-step search for each task's word and a select of
+// its bit), each closing its triangle as in peel_edge.
+__device__ __forceinline__ void peel_edge_chunk(const PeelArgs& A, uint32_t e, uint32_t x, uint32_t y, uint32_t thr,
+                                                uint32_t W, uint32_t w0, uint32_t r, uint32_t* next,
+                                                unsigned long long* ncnt, uint64_t& tdec) {
+  const unsigned lane = lane_id();
+  const uint32_t i = w0 + lane;
+  uint32_t m = 0;
+  if (lane < kSplitWords && i < W) m = __ldcg(A.R.bits + A.R.off(x) + i) & __ldcg(A.R.bits + A.R.off(y) + i);
+  const uint32_t c = __popc(m);
+  const uint32_t incl = warp_incl_scan(c);
+  const uint32_t T = __shfl_sync(kFull, incl, 31);
+  const uint32_t excl = incl - c;
+  const uint64_t ox = A.off[x], oy = A.off[y];
+  uint32_t ndec = 0;
+  for (uint32_t base = 0; base < T; base += 32) {
+    const uint32_t t = base + lane;
+    uint32_t lo = 0;  // the last word (lane < kSplitWords) whose first task is <= t
+#pragma unroll
+    for (uint32_t st = kSplitWords / 2; st >= 1; st >>= 1) {
+      const uint32_t cand = lo + st;
+      const uint32_t ec = __shfl_sync(kFull, excl, cand & 31);
+      if (cand < kSplitWords && ec <= t) lo = cand;
+    }
+    const uint32_t oexcl = __shfl_sync(kFull, excl, lo), om = __shfl_sync(kFull, m, lo);
+    bool pa = false, pb = false;
+    uint32_t a = 0, b = 0;
+    if (t < T) {
+      const uint32_t col = (w0 + lo) * 32 + select_bit(om, t - oexcl);
+      a = A.eid[ox + A.R.rank(x, col)];
+      b = A.eid[oy + A.R.rank(y, col)];
+      close_triangle(A, e, a, b, r, thr, pa, pb, ndec);
+    }
+    push_warp_full(pa, a, next, ncnt, A.cap, &A.words->err);
+    push_warp_full(pb, b, next, ncnt, A.cap, &A.words->err);
+  }
+  tdec += ndec;
+}
+
+// A decrement round over (frontier edge, chunk) units; edges that use the
+// sorted-list merge go whole to the warp of their first chunk.
+__device__ __forceinline__ void split_round(const PeelArgs& A, const uint32_t* fr, uint64_t nf, uint64_t chunks,
+                                            uint32_t r, uint32_t* next, unsigned long long* ncnt, uint64_t gwarp,
+                                            uint64_t gwarps, uint64_t& tdeg, uint64_t& tdec) {
+  for (uint64_t u = gwarp; u < nf * chunks; u += gwarps) {
+    const uint64_t f = u / chunks;
+    const uint32_t ch = (uint32_t)(u - f * chunks);
+    const uint32_t e = fr[f];
+    const uint64_t k = A.ends[e];
+    const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+    const uint64_t na = A.off[x + 1] - A.off[x], nb = A.off[y + 1] - A.off[y];
+    const uint32_t W = A.R.words(x);
+    if ((uint64_t)W > na + nb) {  // peel_edge would merge the lists
+      if (ch == 0) peel_edge(A, e, r, next, ncnt, tdeg, tdec);
+      continue;
+    }
+    if (ch * kSplitWords >= W) continue;
+    if (ch == 0 && lane_id() == 0) tdeg += (uint64_t)atomicSub(&A.adeg[x], 1u) + atomicSub(&A.adeg[y], 1u);
+    peel_edge_chunk(A, e, x, y, edge_thr(A, e), W, ch * kSplitWords, r, next, ncnt, tdec);
+  }
+}
+
 __device__ __forceinline__ void flush_tallies(const PeelArgs& A, uint64_t tdeg, uint64_t tdec) {
   tdeg = warp_sum(tdeg);
   tdec = warp_sum(tdec);
@@ -338,7 +423,12 @@ __global__ void __launch_bounds__(kPeelThreads, 5) k_cascade(PeelArgs A) {
       }
       recount_round(A, r, nx, nc, gwarp, gwarps, trec, su);
     } else {
-      for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
+      // Few frontier edges for the grid: deal (edge, chunk) units instead.
+      const uint64_t chunks = A.R.sbits ? (A.R.W + kSplitWords - 1) / kSplitWords : 1;
+      if (chunks >= 2 && nf * chunks <= (uint64_t)A.split * gwarps)
+        split_round(A, fr, nf, chunks, r, nx, nc, gwarp, gwarps, tdeg, tdec);
+      else
+        for (uint64_t f = gwarp; f < nf; f += gwarps) peel_edge(A, fr[f], r, nx, nc, tdeg, tdec);
     }
     if (gtid == 0) A.cnt[(i + 2) % 3] = 0;  // read at the start of round i-1, next written in round i+1
     if (!grid_barrier(A.words, A.timeout_ns)) {
@@ -559,6 +649,7 @@ struct Peeler {
     A.wavg = s->W ? (float)((double)s->bit_words / std::max<uint32_t>(s->n, 1)) : 0.f;
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.search_ratio = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.peel_search_ratio), 1 << 20);
+    A.split = (uint32_t)std::min<int64_t>(std::max<int64_t>(0, c->opt.peel_split), 1 << 20);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
     A.gthr = track ? gthr.as<uint32_t>() : nullptr;

@@ -5,7 +5,8 @@
 // dense support's tile-block size, the peel's switch from the 32-wide tile
 // merge to per-lane binary search, the cost ratio that turns a peel round
 // into an AND/popcount recount, the core decomposition's blocks per SM and
-// levels per window, the peel's bitset intersection of dense rows).
+// levels per window, the peel's bitset intersection of dense rows and its
+// split rounds).
 //
 // The tuner times a sample batch -- graphs like the ones the caller will
 // solve -- under candidate values, one parameter at a time (coordinate
@@ -44,6 +45,7 @@ const std::vector<Param>& params() {
       {"kcore_blocks_per_sm", &Options::kcore_blocks_per_sm, {0, 1, 2, 4}},
       {"kcore_window", &Options::kcore_window, {8, 16, 32, 64, 128}},
       {"peel_bitset", &Options::peel_bitset, {0, 1}},
+      {"peel_split", &Options::peel_split, {0, 4, 16, 64}},
   };
   return p;
 }
@@ -89,6 +91,7 @@ void fill_result(const Options& o, kt_tune_result* r) {
   r->kcore_blocks_per_sm = o.kcore_blocks_per_sm;
   r->kcore_window = o.kcore_window;
   r->peel_bitset = o.peel_bitset;
+  r->peel_split = o.peel_split;
 }
 
 }  // namespace

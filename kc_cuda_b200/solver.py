@@ -81,7 +81,8 @@ class ServerStats(ctypes.Structure):
 class TuneResult(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in (
         "recount_gamma", "dense_min_fill", "dense_max_n", "support_bitmap_max_n", "kcore_big_row",
-        "peel_search_ratio", "dense_tile_mb", "kcore_blocks_per_sm", "kcore_window", "peel_bitset")] + [
+        "peel_search_ratio", "dense_tile_mb", "kcore_blocks_per_sm", "kcore_window", "peel_bitset",
+        "peel_split")] + [
         ("ms_first", ctypes.c_double), ("ms_best", ctypes.c_double), ("trials", ctypes.c_uint32)]
 
     def as_dict(self):

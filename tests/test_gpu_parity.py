@@ -212,7 +212,7 @@ def test_without_prediction_same_answer(ctx, golden):
 
 
 @pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never", "dense_uncapped",
-                                  "dense_merge_only"])
+                                  "dense_merge_only", "dense_split_always"])
 def test_modes_support_trussness_answer(ctx, golden, mode):
     """Sparse lists vs dense bitsets, dense peels that recount every round vs
     never, and dense peels that intersect sorted lists instead of bitset
@@ -221,7 +221,8 @@ def test_modes_support_trussness_answer(ctx, golden, mode):
             "dense_recount_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1 << 30},
             "dense_recount_never": {"dense_min_fill": 1 << 30, "recount_gamma": 1},
             "dense_uncapped": {"dense_min_fill": 1 << 30, "capped_support": 0},
-            "dense_merge_only": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_bitset": 0}}[mode]
+            "dense_merge_only": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_bitset": 0},
+            "dense_split_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_split": 1 << 20}}[mode]
     old = {k: ctx.get_option(k) for k in opts}
     for k, v in opts.items():
         ctx.set_option(k, v)

@@ -10,7 +10,8 @@ import kc_cuda_b200 as K
 pytestmark = pytest.mark.gpu
 
 TUNED = ("recount_gamma", "dense_min_fill", "dense_max_n", "support_bitmap_max_n", "kcore_big_row",
-         "peel_search_ratio", "dense_tile_mb", "kcore_blocks_per_sm", "kcore_window", "peel_bitset")
+         "peel_search_ratio", "dense_tile_mb", "kcore_blocks_per_sm", "kcore_window", "peel_bitset",
+         "peel_split")
 
 
 def mix_indices(first, limit, max_draws=1_000_000):
@@ -71,6 +72,7 @@ def test_autotune_keeps_answers_and_options(tmp_path):
     ("kcore_blocks_per_sm", [1, 2]),
     ("kcore_window", [1, 2, 7, 1000]),
     ("peel_bitset", [0, 1]),
+    ("peel_split", [0, 1, 1000]),
     ("recount_gamma", [1, 1000]),
 ])
 def test_thresholds_do_not_change_answers(name, values):
