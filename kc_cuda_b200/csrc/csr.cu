@@ -53,9 +53,28 @@ __global__ void k_max_u32(const uint32_t* __restrict__ a, uint64_t n, uint32_t* 
   if (lane_id() == 0 && mx) atomicMax(out, mx);
 }
 
+// u << 32 | v -> u << vb | v (both below 2^vb - 1); the "no edge" key ~0
+// becomes 2^(2 vb) - 1, which sorts after every real key.  The sort then
+// runs over 2 vb bits instead of 32 + vb.
+__global__ void k_pack(uint64_t* __restrict__ keys, uint64_t n, int vb) {
+  const uint64_t none = (((uint64_t)1) << (2 * vb)) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    keys[i] = k == ~0ULL ? none : ((k >> 32) << vb) | (uint32_t)k;
+  }
+}
+
 __global__ void k_remap(uint64_t* __restrict__ keys, uint64_t n, uint64_t from, uint64_t to) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     if (keys[i] == from) keys[i] = to;
+}
+
+__global__ void k_unpack(uint64_t* __restrict__ keys, uint64_t n, int vb) {
+  const uint64_t none = (((uint64_t)1) << (2 * vb)) - 1, low = (((uint64_t)1) << vb) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    keys[i] = k == none ? ~0ULL : ((k >> vb) << 32) | (k & low);
+  }
 }
 
 int bits_for(uint64_t n) {
@@ -68,21 +87,27 @@ int bits_for(uint64_t n) {
 
 void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
   g.n = n;
-  // Keys are min << 32 | max with both halves below 2^vb.  The "no edge" key
-  // ~0 is rewritten to ((2^vb - 1) << 32) | (2^vb - 1), which still sorts
-  // after every real key but leaves bits vb..31 and 32+vb..63 zero in all
-  // keys, so the radix sort skips those digits.
+  // Keys are min << 32 | max with both halves below 2^vb - 1; the radix sort
+  // skips digits shared by every key, so it runs 2 ceil(vb / 8) passes once
+  // the "no edge" key ~0 is rewritten to ((2^vb - 1) << 32) | (2^vb - 1)
+  // (still last).  When packing to min << vb | max saves a pass (2 vb bits,
+  // ceil(2 vb / 8) passes), the keys are packed instead.
   const int vb = bits_for(n + 1);
-  uint64_t sentinel = ~0ULL;
-  if (vb < 32) {
-    sentinel = ((((uint64_t)1 << vb) - 1) << 32) | (((uint64_t)1 << vb) - 1);
-    if (nkeys) {
-      k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL, sentinel);
-      KT_LAUNCHED(c);
-    }
+  const bool small = vb < 32 && nkeys;
+  const bool pack = small && (2 * vb + 7) / 8 < 2 * ((vb + 7) / 8);
+  const uint64_t sentinel = ((((uint64_t)1 << (vb & 31)) - 1) << 32) | (((uint64_t)1 << (vb & 31)) - 1);
+  if (pack) {
+    k_pack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
+    KT_LAUNCHED(c);
+  } else if (small) {
+    k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL, sentinel);
+    KT_LAUNCHED(c);
   }
   if (nkeys > 1) radix_sort_u64(c, keys, nullptr, nkeys, 64);
-  if (vb < 32 && nkeys) {
+  if (pack) {
+    k_unpack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
+    KT_LAUNCHED(c);
+  } else if (small) {
     k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, sentinel, ~0ULL);
     KT_LAUNCHED(c);
   }
