@@ -63,6 +63,7 @@ struct PeelArgs {
   uint32_t* adeg;  // alive degree per vertex (for the byte accounting)
   DenseRows R;     // dense mode: alive adjacency bitsets (R.bits null otherwise)
   float wavg;      // mean words per bitset row
+  uint64_t bit_words;  // words of all bitset rows (a multiple of 4)
   uint32_t gamma;  // recount round when nf * thr * gamma > alive * wavg
   uint32_t search_ratio;  // binary-search the long row when it is this many times longer
   uint32_t split;         // split rounds when frontier x chunks <= split x warps (0 = never)
@@ -352,6 +353,26 @@ __device__ __forceinline__ void clear_edge_bits(const PeelArgs& A, uint32_t e) {
   atomicAnd(&A.R.bits[A.R.off(y) + (cx >> 5)], ~(1u << (cx & 31)));
 }
 
+// Rebuilds the bitsets from the surviving edges when more edges were deleted
+// since the bits were last current than survive: zero every word, then (after
+// a grid barrier, in the caller) set the bits of the alive-list edges still
+// alive -- fewer atomics than clearing the deleted edges one by one.
+__device__ __forceinline__ void zero_bits(const PeelArgs& A, uint64_t gtid, uint64_t gthreads) {
+  uint4* p = reinterpret_cast<uint4*>(A.R.bits);
+  for (uint64_t w = gtid; w < A.bit_words / 4; w += gthreads) p[w] = make_uint4(0u, 0u, 0u, 0u);
+}
+__device__ __forceinline__ void set_alive_bits(const PeelArgs& A, uint64_t gtid, uint64_t gthreads) {
+  for (uint64_t i = gtid; i < A.na; i += gthreads) {
+    const uint32_t e = A.alive[i];
+    if (A.state[e] != kAlive) continue;
+    const uint64_t k = A.ends[e];
+    const uint32_t x = (uint32_t)(k >> 32), y = (uint32_t)k;
+    const uint32_t cy = A.R.col(x, y), cx = A.R.col(y, x);
+    atomicOr(&A.R.bits[A.R.off(x) + (cy >> 5)], 1u << (cy & 31));
+    atomicOr(&A.R.bits[A.R.off(y) + (cx >> 5)], 1u << (cx & 31));
+  }
+}
+
 // Clears the bits of alive-list edges deleted in rounds (lo, hi].
 __device__ __forceinline__ void clear_deleted(const PeelArgs& A, uint32_t lo, uint32_t hi, uint64_t gtid,
                                               uint64_t gthreads) {
@@ -401,6 +422,7 @@ __global__ void __launch_bounds__(kPeelThreads, 5) k_cascade(PeelArgs A) {
   uint64_t tdeg = 0, tdec = 0, trec = 0;
   uint64_t alive = A.na;
   uint32_t cleared = A.r0 - 1;  // bits are current for deletions up to this round
+  uint64_t pending = 0;          // edges deleted since then
   uint32_t i = 0, nrec = 0;
   bool ok = true;
   while (true) {
@@ -413,10 +435,21 @@ __global__ void __launch_bounds__(kPeelThreads, 5) k_cascade(PeelArgs A) {
     const uint32_t thr = A.gthr_max ? *A.gthr_max : A.thr;
     const bool recount = A.R.bits && (double)nf * (double)(thr > 0 ? thr : 1) * (double)A.gamma >
                                          (double)alive * (double)A.wavg;
+    pending += nf;
     if (recount) {
       ++nrec;
-      clear_deleted(A, cleared, r, gtid, gthreads);
+      if (pending > alive - nf) {
+        zero_bits(A, gtid, gthreads);
+        if (!grid_barrier(A.words, A.timeout_ns)) {
+          ok = false;
+          break;
+        }
+        set_alive_bits(A, gtid, gthreads);
+      } else {
+        clear_deleted(A, cleared, r, gtid, gthreads);
+      }
       cleared = r;
+      pending = 0;
       if (!grid_barrier(A.words, A.timeout_ns)) {
         ok = false;
         break;
@@ -439,7 +472,14 @@ __global__ void __launch_bounds__(kPeelThreads, 5) k_cascade(PeelArgs A) {
     ++i;
   }
   // Bring the bitsets up to date with this cascade's remaining deletions.
-  if (ok && A.R.bits) clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
+  if (ok && A.R.bits && pending) {
+    if (pending > alive) {
+      zero_bits(A, gtid, gthreads);
+      if (grid_barrier(A.words, A.timeout_ns)) set_alive_bits(A, gtid, gthreads);
+    } else {
+      clear_deleted(A, cleared, A.r0 + i, gtid, gthreads);
+    }
+  }
   flush_tallies(A, tdeg, tdec);
   if (lane_id() == 0 && trec) atomicAdd(&A.acct[2], (unsigned long long)trec);
   if (gtid == 0) {
@@ -647,6 +687,7 @@ struct Peeler {
     A.R = s->W ? dense_rows(*s) : DenseRows{nullptr, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (!c->opt.peel_bitset) A.R.sbits = nullptr;
     A.wavg = s->W ? (float)((double)s->bit_words / std::max<uint32_t>(s->n, 1)) : 0.f;
+    A.bit_words = s->W ? s->bit_words : 0;
     A.gamma = (uint32_t)std::max<int64_t>(1, c->opt.recount_gamma);
     A.search_ratio = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.peel_search_ratio), 1 << 20);
     A.split = (uint32_t)std::min<int64_t>(std::max<int64_t>(0, c->opt.peel_split), 1 << 20);
