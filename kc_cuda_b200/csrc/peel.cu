@@ -411,7 +411,11 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
 
 // One whole cascade in one cooperative launch.  Dense mode uses W words of
 // shared memory per warp for the recount rounds.
-__global__ void __launch_bounds__(kPeelThreads, 5) k_cascade(PeelArgs A) {
+// Resident blocks per SM the register allocation aims at (a build constant).
+#ifndef KT_PEEL_MIN_BLOCKS
+#define KT_PEEL_MIN_BLOCKS 5
+#endif
+__global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(PeelArgs A) {
   extern __shared__ __align__(16) uint32_t dense_smem[];
   uint32_t* su = dense_smem + warp_id() * A.R.W;
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
