@@ -96,7 +96,91 @@ void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g
   c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
 }
 
+// Host TSV bytes -> Graph with the host-to-device copy overlapped with the
+// parse: the bytes go over in chunks (parse_pipeline_mb, whole parse blocks)
+// on the copy stream; each chunk's lines are counted as soon as it lands and
+// parsed into a record buffer of its own once the next chunk -- which its
+// last lines may reach into -- has landed, so only the last chunk's parse and
+// the joining of the chunks' records follow the copy.  A line that needs
+// bytes not yet on the device (a line longer than a chunk) makes the whole
+// parse run again once every byte is there.
+static void load_tsv_pipelined(Ctx* c, const char* bytes, uint64_t len, uint64_t chunk, Graph& g) {
+  DBuf dbuf(c, parse_padded_bytes(len));
+  zero(c, dbuf.as<uint8_t>() + len, dbuf.bytes() - len);  // the parser reads zeros past len
+  reset_words(c);
+  const uint64_t nch = (len + chunk - 1) / chunk;
+  const uint64_t bpc = chunk / parse_block_bytes();
+  const uint64_t nblk = (len + parse_block_bytes() - 1) / parse_block_bytes();
+  std::vector<cudaEvent_t> landed(nch + 1, nullptr);
+  struct Events {
+    std::vector<cudaEvent_t>& v;
+    ~Events() {
+      for (cudaEvent_t e : v)
+        if (e) {
+          cudaEventSynchronize(e);
+          cudaEventDestroy(e);
+        }
+    }
+  } guard{landed};
+  for (cudaEvent_t& e : landed) KT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  // The copy stream starts once the buffer exists (it is allocated in order on
+  // the main stream).
+  KT_CUDA(cudaEventRecord(landed[nch], c->stream));
+  KT_CUDA(cudaStreamWaitEvent(c->copy_stream, landed[nch], 0));
+  for (uint64_t i = 0; i < nch; ++i) {
+    const uint64_t off = i * chunk, n = std::min(chunk, len - off);
+    KT_CUDA(cudaMemcpyAsync(dbuf.as<char>() + off, bytes + off, n, cudaMemcpyHostToDevice, c->copy_stream));
+    KT_CUDA(cudaEventRecord(landed[i], c->copy_stream));
+    c->h2d_bytes += n;
+  }
+  KT_CUDA(cudaEventRecord(c->ev[4], c->stream));
+  std::vector<DBuf> part(nch);
+  std::vector<uint64_t> plines(nch, 0);
+  uint64_t lines = 0;
+  for (uint64_t i = 0; i < nch; ++i) {
+    KT_CUDA(cudaStreamWaitEvent(c->stream, landed[i], 0));
+    const uint64_t b0 = i * bpc, nb = std::min(bpc, nblk - b0);
+    DBuf boff;
+    plines[i] = parse_count_lines(c, dbuf.as<uint8_t>(), len, boff, b0, nb);
+    if (i + 1 < nch) KT_CUDA(cudaStreamWaitEvent(c->stream, landed[i + 1], 0));
+    const uint64_t ready = i + 1 < nch ? std::min(len, (i + 2) * chunk) : len;
+    part[i].alloc(c, (plines[i] ? plines[i] : 1) * sizeof(uint64_t));
+    parse_lines(c, dbuf.as<uint8_t>(), len, boff, part[i].as<uint64_t>(), dev_words(c), b0, nb, ready, lines);
+    lines += plines[i];
+  }
+  DevWords w;
+  copy_d2h(c, &w, c->words.get(), sizeof(DevWords));
+  if (w.counters[2]) {
+    part.clear();
+    graph_from_device_bytes(c, dbuf.as<uint8_t>(), len, g);
+    return;
+  }
+  check_words(c, "parse");
+  DBuf keys(c, (lines ? lines : 1) * sizeof(uint64_t));
+  uint64_t at = 0;
+  for (uint64_t i = 0; i < nch; ++i) {
+    if (plines[i])
+      KT_CUDA(cudaMemcpyAsync(keys.as<uint64_t>() + at, part[i].get(), plines[i] * sizeof(uint64_t),
+                              cudaMemcpyDeviceToDevice, c->stream));
+    at += plines[i];
+    part[i].release();
+  }
+  const uint64_t n = (w.counters[1] & 1) ? (uint64_t)(uint32_t)w.counters[0] + 1 : 0;
+  reset_words(c);
+  KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
+  build_graph(c, keys.as<uint64_t>(), lines, n, g);
+  KT_CUDA(cudaEventRecord(c->ev[6], c->stream));
+  c->stats.ms_parse = event_ms(c->ev[4], c->ev[5]);  // copy and parse, overlapped
+  c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
+}
+
 void load_tsv(Ctx* c, const char* bytes, uint64_t len, Graph& g) {
+  const uint64_t blk = parse_block_bytes();
+  const uint64_t chunk = std::max<uint64_t>(1, ((uint64_t)std::max<int64_t>(1, c->opt.parse_pipeline_mb) << 20) / blk) * blk;
+  if (len >= 3 * chunk) {
+    load_tsv_pipelined(c, bytes, len, chunk, g);
+    return;
+  }
   DBuf dbuf(c, parse_padded_bytes(len));
   zero(c, dbuf.as<uint8_t>() + len, dbuf.bytes() - len);  // the parser reads zeros past len
   copy_h2d(c, dbuf.get(), bytes, len);
@@ -226,6 +310,7 @@ kt_status kt_init(int device, uint64_t budget, kt_ctx** out) {
     KT_CUDA(cudaSetDevice(device));
     KT_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
     KT_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    KT_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
     size_t fr = 0, tot = 0;
     KT_CUDA(cudaMemGetInfo(&fr, &tot));
     c.budget = budget ? budget : (uint64_t)(fr * 0.9);
@@ -258,6 +343,7 @@ void kt_destroy(kt_ctx* h) {
       if (e) cudaEventDestroy(e);
     if (h->c.pinned) cudaFreeHost(h->c.pinned);
     if (h->c.stream) cudaStreamDestroy(h->c.stream);
+    if (h->c.copy_stream) cudaStreamDestroy(h->c.copy_stream);
   }
   delete h;
 }

@@ -137,6 +137,7 @@ struct Ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host-to-device chunks of the pipelined ingest
   uint64_t budget = 0;
   uint64_t in_use = 0;
   uint64_t peak = 0;

@@ -32,9 +32,10 @@ __device__ __forceinline__ uint32_t count_nl4(uint32_t w) { return __popc(__vcmp
 
 // Lines owned by a block: its '\n' bytes except one at len-1, plus line 0.
 __global__ void __launch_bounds__(kParseThreads) k_count_lines(const uint8_t* __restrict__ buf, uint64_t len,
-                                                               uint32_t* __restrict__ block_lines) {
+                                                               uint64_t block0, uint32_t* __restrict__ block_lines) {
   __shared__ uint32_t tmp[33];
-  const uint64_t blo = (uint64_t)blockIdx.x * kBlockBytes;
+  const uint64_t b = block0 + blockIdx.x;
+  const uint64_t blo = b * kBlockBytes;
   const uint64_t bhi = min(len, blo + kBlockBytes);
   const uint64_t nvec = (bhi - blo + 15) / 16;  // the padding past len is zero
   uint32_t c = 0;
@@ -45,7 +46,7 @@ __global__ void __launch_bounds__(kParseThreads) k_count_lines(const uint8_t* __
   c = block_sum<uint32_t>(c, tmp);
   if (threadIdx.x == 0) {
     if (bhi == len && len > 0 && buf[len - 1] == '\n') c -= 1;
-    if (blockIdx.x == 0 && len > 0) c += 1;
+    if (b == 0 && len > 0) c += 1;
     block_lines[blockIdx.x] = c;
   }
 }
@@ -56,9 +57,16 @@ struct Bytes {
   const uint8_t* sm;  // staged bytes [lo, hi)
   const uint8_t* g;   // global buffer
   uint64_t lo, hi, len;
+  uint64_t ready;     // bytes [0, ready) of the buffer are on the device
+  uint32_t* deferred; // set when a line reads past `ready` (its record is then redone)
   __device__ __forceinline__ int at(uint64_t q) const {  // -1 past the end
     if (q >= len) return -1;
-    return q < hi ? sm[q - lo] : g[q];
+    if (q < hi) return sm[q - lo];
+    if (q >= ready) {
+      *deferred = 1u;
+      return -1;
+    }
+    return g[q];
   }
 };
 
@@ -144,12 +152,13 @@ __device__ __forceinline__ bool parse_line_fast(const uint32_t* stage, uint64_t 
 // the threads, so the per-line work is balanced and the keys are written
 // with consecutive threads on consecutive slots.
 __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __restrict__ buf, uint64_t len,
+                                                               uint64_t block0, uint64_t ready, uint64_t line_base,
                                                                const uint64_t* __restrict__ block_off,
                                                                uint64_t* __restrict__ keys, DevWords* words) {
   __shared__ __align__(16) uint32_t stage[(kBlockBytes + kOverhang) / 4];
   __shared__ uint16_t starts[kBlockBytes + 1];
   __shared__ uint32_t tmp[33];
-  const uint64_t blo = (uint64_t)blockIdx.x * kBlockBytes;
+  const uint64_t blo = (block0 + blockIdx.x) * kBlockBytes;
   const uint64_t bhi = min(len, blo + kBlockBytes + kOverhang);
   // The device buffer is padded (zeros) to whole 16-byte words past len.
   const uint64_t nvec = (bhi - blo + 15) / 16;
@@ -190,7 +199,8 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
     }
   }
   __syncthreads();
-  const Bytes B{reinterpret_cast<const uint8_t*>(stage), buf, blo, blo + nvec * 16, len};
+  const Bytes B{reinterpret_cast<const uint8_t*>(stage), buf, blo, blo + nvec * 16, len, ready,
+                reinterpret_cast<uint32_t*>(&words->counters[2])};
   const uint64_t slot0 = block_off[blockIdx.x];
   uint32_t vmax = 0;
   bool any = false;
@@ -204,7 +214,7 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
     }
     if (bad) {
       atomicOr(&words->err, kDevErrParse);
-      atomicMin(&words->bad_line, (unsigned long long)(slot0 + i));
+      atomicMin(&words->bad_line, (unsigned long long)(line_base + slot0 + i));
     }
     any = true;
     keys[slot0 + i] = key;
@@ -219,12 +229,16 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
 
 }  // namespace
 
-uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& block_off) {
-  const uint64_t blocks = (len + kBlockBytes - 1) / kBlockBytes;
+uint64_t parse_block_bytes() { return kBlockBytes; }
+
+uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& block_off, uint64_t block0,
+                           uint64_t nblocks) {
+  const uint64_t total = (len + kBlockBytes - 1) / kBlockBytes;
+  if (total > 0x7fffffffULL) throw Error(KT_ERR_LIMIT, "TSV larger than the parser's grid");
+  const uint64_t blocks = nblocks == ~0ULL ? total - block0 : nblocks;
   if (blocks == 0) return 0;
-  if (blocks > 0x7fffffffULL) throw Error(KT_ERR_LIMIT, "TSV larger than the parser's grid");
   DBuf cnt(c, (blocks + 1) * sizeof(uint32_t));
-  k_count_lines<<<(unsigned)blocks, kParseThreads, 0, c->stream>>>(dbuf, len, cnt.as<uint32_t>());
+  k_count_lines<<<(unsigned)blocks, kParseThreads, 0, c->stream>>>(dbuf, len, block0, cnt.as<uint32_t>());
   KT_LAUNCHED(c);
   zero(c, cnt.as<uint32_t>() + blocks, sizeof(uint32_t));
   block_off.ensure(c, (blocks + 1) * sizeof(uint64_t));
@@ -232,10 +246,13 @@ uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& bloc
   return read_word<uint64_t>(c, block_off.as<uint64_t>() + blocks);
 }
 
-void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words) {
-  const uint64_t blocks = (len + kBlockBytes - 1) / kBlockBytes;
+void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words,
+                 uint64_t block0, uint64_t nblocks, uint64_t ready, uint64_t line_base) {
+  const uint64_t total = (len + kBlockBytes - 1) / kBlockBytes;
+  const uint64_t blocks = nblocks == ~0ULL ? total - block0 : nblocks;
   if (blocks == 0) return;
-  k_parse_lines<<<(unsigned)blocks, kParseThreads, 0, c->stream>>>(dbuf, len, block_off.as<uint64_t>(), keys, words);
+  k_parse_lines<<<(unsigned)blocks, kParseThreads, 0, c->stream>>>(dbuf, len, block0, ready == ~0ULL ? len : ready,
+                                                                   line_base, block_off.as<uint64_t>(), keys, words);
   KT_LAUNCHED(c);
 }
 

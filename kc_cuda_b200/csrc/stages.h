@@ -9,8 +9,19 @@ void scan_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n);
 
 // parse.cu -- stage (a)
 uint64_t parse_padded_bytes(uint64_t len);
-uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& block_off);
-void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words);
+// Bytes per parse block; a chunk of the input for the pipelined ingest is a
+// whole number of blocks.
+uint64_t parse_block_bytes();
+// Lines of blocks [block0, block0 + nblocks) (~0: to the end); block_off
+// receives their exclusive scan (relative to the first of them).
+uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& block_off, uint64_t block0 = 0,
+                           uint64_t nblocks = ~0ULL);
+// Parses those blocks' lines into keys[block_off[b] + i].  Bytes at or past
+// `ready` (~0: len) are not yet on the device: a line that needs one sets
+// DevWords::counters[2] (its record must be redone).  line_base numbers the
+// lines for parse errors.
+void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words,
+                 uint64_t block0 = 0, uint64_t nblocks = ~0ULL, uint64_t ready = ~0ULL, uint64_t line_base = 0);
 
 // csr.cu -- stage (b): canonical keys (any order, ~0 = none) -> Graph.
 // `keys` is consumed (sorted in place).

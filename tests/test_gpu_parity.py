@@ -113,6 +113,38 @@ def test_parse_random_bytes(ctx):
         g.free()
 
 
+def test_pipelined_ingest(ctx):
+    """Host bytes of three or more chunks go over in chunks overlapped with
+    the parse (1 MB chunks here): the same graph as the one-shot path, the
+    same records on byte soup, a line longer than a chunk (parsed again once
+    every byte has landed), and a parse error numbered from the first line."""
+    old = ctx.get_option("parse_pipeline_mb")
+    ctx.set_option("parse_pipeline_mb", 1)
+    try:
+        g = gen.Graph(gen.rmat(15, 16, 3, [20]))
+        data = g.tsv_bytes()
+        assert len(data) > 3 << 20
+        d = ctx.load_tsv(data)
+        assert np.array_equal(d.edges(), g.edges())
+        assert d.kmax_truss() == ctx.solve_tsv(data)
+        d.free()
+        soup = random_record_bytes(7, 250_000)
+        assert len(soup) > 3 << 20
+        d = ctx.load_tsv(soup)
+        assert np.array_equal(d.edges(), O.clean(O.parse(soup)))
+        d.free()
+        longline = b"1\t2\n" * 200_000 + b"3" + b" " * 2_500_000 + b"4\n" + b"5\t6\n4\t5\n" * 200_000
+        d = ctx.load_tsv(longline)
+        assert np.array_equal(d.edges(), O.clean(O.parse(longline)))
+        d.free()
+        bad = b"1\t2\n" * 1_000_000 + b"7\n" + b"2\t3\n" * 10
+        with pytest.raises(K.KtError) as ei:
+            ctx.load_tsv(bad)
+        assert ei.value.status == 4 and "line 1000001" in ei.value.message
+    finally:
+        ctx.set_option("parse_pipeline_mb", old)
+
+
 def test_csr_large_random_pairs(ctx):
     rng = np.random.default_rng(5)
     n = 1 << 18
