@@ -207,6 +207,25 @@ def cpu_baseline_run(steps: int, warmup: int, threads: int):
 
 
 TUNE_FIRST = 2_000_000  # mix graphs of the autotuner's sample (away from the measured ones)
+SERVE_FIRST = 1_000_000  # mix graphs of the serving workload (away from the batched ones)
+
+
+def rank_index_ranges(rank: int, mix_graphs: int, tune_graphs: int, serve_requests: int, calib_graphs: int) -> dict:
+    """Mix-graph index ranges [first, end) a replica uses.  Replicas solve
+    independent graphs (no data-path collective): every rank takes its own
+    slice of the batched mix, of the tuner's sample, and of the serving
+    workload's calibration batch and requests, and no two ranges overlap."""
+    serve = SERVE_FIRST + rank * (serve_requests + calib_graphs)
+    return {
+        "mix": (rank * mix_graphs, (rank + 1) * mix_graphs),
+        "tune": (TUNE_FIRST + rank * tune_graphs, TUNE_FIRST + (rank + 1) * tune_graphs),
+        "calib": (serve, serve + calib_graphs),
+        "serve": (serve + calib_graphs, serve + calib_graphs + serve_requests),
+    }
+
+
+def ranges_for(args, rank: int) -> dict:
+    return rank_index_ranges(rank, args.mix_graphs, args.tune_graphs, args.serve_requests, args.calib_graphs)
 
 
 def autotune(ctx, args, rank):
@@ -214,14 +233,15 @@ def autotune(ctx, args, rank):
     TUNE_FIRST on (kt_autotune); returns its report, or None when off."""
     if not args.tune_graphs:
         return None
+    first = ranges_for(args, rank)["tune"][0]
     b = ctx.batch()
-    b.add_mix(TUNE_FIRST + rank * args.tune_graphs, args.tune_graphs)
+    b.add_mix(first, args.tune_graphs)
     t0 = time.perf_counter()
     tune = b.autotune(passes=1)
     b.free()
     tune["wall_s"] = round(time.perf_counter() - t0, 1)
     tune["sample_graphs"] = args.tune_graphs
-    tune["sample_first"] = TUNE_FIRST + rank * args.tune_graphs
+    tune["sample_first"] = first
     return tune
 
 
@@ -235,7 +255,7 @@ def run_mix(args, world, rank, local, pg):
 
     import kc_cuda_b200 as K
     G = args.mix_graphs
-    first = rank * G  # each rank its own slice of the mix (independent graphs)
+    first = ranges_for(args, rank)["mix"][0]  # each rank its own slice of the mix (independent graphs)
     ctx = K.Context(local)
     # Both paths allocate from a pool grown once to the context's budget, so
     # graphs of new sizes do not map device memory in the middle of a solve.
@@ -309,8 +329,8 @@ def run_serve(args, world, rank, local, pg):
     import kc_cuda_b200 as K
     from kc_cuda_b200 import serving
     R = args.serve_requests
-    base = 1_000_000 + rank * (R + args.calib_graphs)  # away from the graphs of the batched workload
-    calib_first, first = base, base + args.calib_graphs
+    ranges = ranges_for(args, rank)
+    calib_first, first = ranges["calib"][0], ranges["serve"][0]
     ctx = K.Context(local)
     ctx.set_option("pool_reserve_mb", 1 << 30)
     tune = autotune(ctx, args, rank)
