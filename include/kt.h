@@ -76,6 +76,9 @@ const char* kt_status_string(kt_status s);
  *                               alive list (passes between read window candidates)
  *   peel_bitset (1)             peel: intersect dense rows as bitsets (AND of two
  *                               rows) when the rows are shorter than the lists
+ *   kcore_compact (8)           maximum-core search: copy the core into a compact
+ *                               graph once it holds < 1/this of the vertices
+ *                               (0 = never)
  *   peel_split (16)             peel: a round whose frontier edges x 8-word row
  *                               chunks <= this x warps deals (edge, chunk) units
  *                               to warps instead of edges (0 = off) */

@@ -374,7 +374,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"kcore_blocks_per_sm", &o.kcore_blocks_per_sm},
              {"kcore_window", &o.kcore_window},
              {"peel_bitset", &o.peel_bitset},
-             {"peel_split", &o.peel_split}};
+             {"peel_split", &o.peel_split},
+             {"kcore_compact", &o.kcore_compact}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

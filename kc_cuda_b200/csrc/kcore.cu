@@ -929,7 +929,8 @@ uint32_t KCore::find_max_core(Ctx* c) {
       succ.push_back(tag);
       rebuild_alive(c);
       // Work on a compacted copy once the core is a small part of the graph.
-      if (n_alive * 8 < n) compact_to_alive(c, (uint32_t)lo);
+      if (c->opt.kcore_compact > 0 && n_alive * (uint64_t)c->opt.kcore_compact < n)
+        compact_to_alive(c, (uint32_t)lo);
     } else {
       hi = k;
       ramp = false;
