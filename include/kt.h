@@ -76,6 +76,8 @@ const char* kt_status_string(kt_status s);
  *                               alive list (passes between read window candidates)
  *   peel_bitset (1)             peel: intersect dense rows as bitsets (AND of two
  *                               rows) when the rows are shorter than the lists
+ *   wave_budget_pct (50)        batch: a wave's estimated device footprint stays
+ *                               within this % of the free budget
  *   kcore_compact (8)           maximum-core search: copy the core into a compact
  *                               graph once it holds < 1/this of the vertices
  *                               (0 = never)

@@ -375,7 +375,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"kcore_window", &o.kcore_window},
              {"peel_bitset", &o.peel_bitset},
              {"peel_split", &o.peel_split},
-             {"kcore_compact", &o.kcore_compact}};
+             {"kcore_compact", &o.kcore_compact},
+             {"wave_budget_pct", &o.wave_budget_pct}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

@@ -61,6 +61,7 @@ struct Options {
   int64_t kcore_window = 32;      // core decomposition: levels per pass over the whole alive list
   int64_t peel_bitset = 1;        // peel: dense rows intersected as bitsets when shorter than the lists
   int64_t kcore_compact = 8;      // max-core search: compact once the core is < 1/this of the graph (0 = never)
+  int64_t wave_budget_pct = 50;   // batch: a wave's estimated footprint within this % of the free budget
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
 };
 
