@@ -68,6 +68,30 @@ def test_batched_mix_equals_graph_alone(ctx):
         assert O.solve_edges(gen.Graph(gen.mix_graph(i)).edges()) == alone[j], i
 
 
+@pytest.mark.parametrize("capped", [1, 0])
+def test_batch_of_golden_specs_and_files(ctx, golden, capped):
+    """The generated golden graphs (R-MAT with dense cores, two phases) and
+    the golden files in one batch, with the capped search-phase support of
+    the single-graph path switched on and off: the reference's answers."""
+    graphs = []
+    for name, e in sorted(golden.items()):
+        if "spec" in e:
+            graphs.append((gen.Graph(gen.GraphSpec(**e["spec"])).edges(), (e["kmax"], e["edges"])))
+        elif "file" in e and "error" not in e:
+            graphs.append((O.parse(golden_bytes(e)), (e["kmax"], e["edges"])))
+    ctx.set_option("capped_support", capped)
+    try:
+        b = ctx.batch()
+        for xy, _ in graphs:
+            b.add_pairs(xy)
+        b.run()
+        k, cnt = b.results()
+        b.free()
+        assert list(zip(k.tolist(), cnt.tolist())) == [w for _, w in graphs]
+    finally:
+        ctx.set_option("capped_support", 1)
+
+
 def test_batch_in_several_waves_same_answers(golden):
     """A small HBM budget forces many waves; answers must not change."""
     graphs = []
