@@ -54,9 +54,13 @@ inline DenseRows dense_rows(const Sub& s) {
 #define KT_DENSE_DEPTH 4
 #endif
 constexpr int kDenseDepth = KT_DENSE_DEPTH;
-// Capped support: two edges per warp, one per half (build constant).
+// Capped and exact support: two edges sharing row u per warp, one per half
+// (build constants).
 #ifndef KT_CAPPED_PAIRS
 #define KT_CAPPED_PAIRS 1
+#endif
+#ifndef KT_EXACT_PAIRS
+#define KT_EXACT_PAIRS 1
 #endif
 
 // Shared memory a block of `threads` needs for rows of W words.
@@ -92,6 +96,31 @@ __device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ 
   }
   for (; i < e; i += 32) s += popc_and4(s4[i], __ldcg(p4 + i));
   return warp_sum(s);
+}
+
+// popcount(row u & row v) over words [w0, w1) (multiples of 4) by one half
+// of the warp (16 lanes, 16-byte vectors); `active` false contributes 0.
+// Every lane of the warp must call it; each lane gets its half's total.
+__device__ __forceinline__ uint32_t half_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
+                                                  uint32_t w1, bool active) {
+  uint32_t s = 0;
+  if (active) {
+    const uint4* p4 = reinterpret_cast<const uint4*>(p);
+    const uint4* s4 = reinterpret_cast<const uint4*>(su);
+    uint32_t i = w0 / 4 + (lane_id() & 15);
+    const uint32_t e = w1 / 4;
+    for (; i + 3 * 16 < e; i += 4 * 16) {
+      uint4 a[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = __ldcg(p4 + i + 16 * k);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += popc_and4(s4[i + 16 * k], a[k]);
+    }
+    for (; i < e; i += 16) s += popc_and4(s4[i], __ldcg(p4 + i));
+  }
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+  return s;
 }
 
 // One group of up to 32 list entries [base, min(base+32, cnt)).  Entries
@@ -130,36 +159,32 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
       dense_load_row(R.bits + R.off(uj), W, su);
       cu = uj;
     }
+#if KT_EXACT_PAIRS
+    // The next edge with the same row u goes to the upper half of the warp.
+    int j2 = -1;
+    uint32_t vj2 = 0;
+    if (todo) {
+      const int cand = __ffs(todo) - 1;
+      const uint32_t uc = __shfl_sync(kFull, u, cand), vc = __shfl_sync(kFull, v, cand);
+      if (uc == uj) {
+        j2 = cand;
+        vj2 = vc;
+        todo &= todo - 1;
+      }
+    }
+    const bool upper = l >= 16;
+    const uint32_t s = half_and_popc(R.bits + R.off(upper ? vj2 : vj), su, 0, W, !upper || j2 >= 0);
+    const uint32_t f0 = __shfl_sync(kFull, s, 0), f1 = __shfl_sync(kFull, s, 16);
+    if (l == (unsigned)j) my_s = f0;
+    if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
+#else
     const uint32_t s = dense_and_popc(R.bits + R.off(vj), su, 0, W);
     if (l == (unsigned)j) my_s = s;
+#endif
   }
   __syncwarp();
 }
 
-// popcount(row u & row v) over words [w0, w1) (multiples of 4) by one half
-// of the warp (16 lanes, 16-byte vectors); `active` false contributes 0.
-// Every lane of the warp must call it; each lane gets its half's total.
-__device__ __forceinline__ uint32_t half_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
-                                                  uint32_t w1, bool active) {
-  uint32_t s = 0;
-  if (active) {
-    const uint4* p4 = reinterpret_cast<const uint4*>(p);
-    const uint4* s4 = reinterpret_cast<const uint4*>(su);
-    uint32_t i = w0 / 4 + (lane_id() & 15);
-    const uint32_t e = w1 / 4;
-    for (; i + 3 * 16 < e; i += 4 * 16) {
-      uint4 a[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) a[k] = __ldcg(p4 + i + 16 * k);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s += popc_and4(s4[i + 16 * k], a[k]);
-    }
-    for (; i < e; i += 16) s += popc_and4(s4[i], __ldcg(p4 + i));
-  }
-#pragma unroll
-  for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-  return s;
-}
 
 // As dense_group, but an edge whose count can no longer reach `thr` is
 // abandoned: the rows are ANDed in four segments, and after each one the
