@@ -58,7 +58,9 @@ const char* kt_status_string(kt_status s);
  *   recount_gamma (16)          recount round when frontier * thr * gamma > alive * words
  *   capped_support (1)          search phase: abandon supports below the threshold
  *   timeout_ms (20000)          bound on every device-side wait
- *   parse_pipeline_mb (256)     host->device chunk of file ingest
+ *   parse_pipeline_mb (256)     host->device chunk of file ingest, and of host TSV
+ *                               bytes parsed chunk by chunk as they land (inputs of
+ *                               three chunks or more)
  *   record_kernel_times (0)     events around support / peel kernels
  *   debug_checks (0)            extra host-side consistency checks
  *   verbose (0)                 stage decisions on stderr
