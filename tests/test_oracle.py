@@ -87,3 +87,28 @@ def test_core_numbers_against_definition():
         alive &= ~drop
     assert alive.any()
     assert set(np.nonzero(alive)[0]) == set(np.nonzero(core >= k)[0])
+
+
+def test_trussness_against_definition():
+    """Every level of the oracle's per-edge trussness, not only kmax: for each
+    k the k-truss found by definition (drop edges in fewer than k-2 triangles
+    of the surviving graph until none is left) is the set truss >= k."""
+    g = gen.Graph(gen.rmat(9, 8, 5, [10, 14]))
+    e, n = g.edges(), g.num_vertices
+    truss = O.trussness(e)
+    u = (e >> np.uint64(32)).astype(np.int64)
+    v = (e & np.uint64(0xFFFFFFFF)).astype(np.int64)
+    assert int(truss.max()) >= 14
+    for k in range(3, int(truss.max()) + 2):
+        alive = np.ones(len(e), bool)
+        while True:
+            a = np.zeros((n, n), np.int64)
+            a[u[alive], v[alive]] = 1
+            a[v[alive], u[alive]] = 1
+            sup = (a @ a)[u, v]
+            drop = alive & (sup < k - 2)
+            if not drop.any():
+                break
+            alive &= ~drop
+        assert np.array_equal(alive, truss >= k), k
+    assert O.kmax_from_truss(truss) == O.solve_edges(e)
