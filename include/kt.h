@@ -216,7 +216,10 @@ kt_status kt_server_submit_pairs(kt_server* s, const uint64_t* xy, uint64_t coun
 /* Queues graph `index` of the batched mix (generated on the device). */
 kt_status kt_server_submit_mix(kt_server* s, uint64_t index, uint64_t base_seed, uint64_t* request_id);
 /* A request's result; waits up to timeout_ms (0 = do not wait) and returns
- * KT_ERR_TIMEOUT while it is still pending. */
+ * KT_ERR_TIMEOUT while it is still pending.  A result can be read any number
+ * of times: the server keeps each finished request's result record (about
+ * 200 host bytes; its graph's records are freed when its wave ends) until
+ * kt_server_destroy. */
 kt_status kt_server_wait(kt_server* s, uint64_t request_id, uint32_t timeout_ms, kt_request_result* out);
 kt_status kt_server_get_stats(kt_server* s, kt_server_stats* out);
 /* Finishes every queued request, stops the worker and frees the server. */

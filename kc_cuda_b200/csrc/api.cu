@@ -407,6 +407,7 @@ kt_status kt_set_option(kt_ctx* h, const char* name, int64_t value) {
 
 kt_status kt_get_option(const kt_ctx* h, const char* name, int64_t* value) {
   if (!h || !value) return KT_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
   int64_t* p = option_slot(const_cast<kt::Options&>(h->c.opt), name);
   if (!p) return KT_ERR_INVALID;
   *value = *p;
@@ -723,6 +724,8 @@ kt_status kt_edge_trussness(kt_ctx* h, kt_graph* g, uint32_t* truss) {
 
 kt_status kt_get_stats(const kt_ctx* h, kt_stats* out) {
   if (!h || !out) return KT_ERR_INVALID;
+  // A serving worker may be writing these mid-wave: read them under the lock.
+  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
   *out = h->c.stats;
   out->kernel_launches = h->c.launches;
   out->device_bytes_peak = h->c.peak;

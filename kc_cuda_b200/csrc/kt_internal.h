@@ -148,7 +148,7 @@ struct Ctx {
   std::string last_error;
   Options opt;
   kt_stats stats{};
-  std::recursive_mutex mu;
+  mutable std::recursive_mutex mu;  // every entry point, readers included
   // Pinned host words for small device-to-host reads.
   uint64_t* pinned = nullptr;
   cudaEvent_t ev[8] = {};

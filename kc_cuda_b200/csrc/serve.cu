@@ -99,6 +99,7 @@ struct kt_server {
         items.push_back(&r->item);
       }
       kt_status status = KT_OK;
+      uint64_t peak = 0;
       {
         std::lock_guard<std::recursive_mutex> lk(c->mu);
         try {
@@ -119,6 +120,7 @@ struct kt_server {
           c->timer.resolve();
         } catch (...) {
         }
+        peak = c->peak;
       }
       const Clock::time_point t_done = Clock::now();
       std::lock_guard<std::mutex> lk(m);
@@ -139,7 +141,7 @@ struct kt_server {
         r->item.extra.shrink_to_fit();
         st.completed++;
       }
-      st.device_bytes_peak = c->peak;
+      st.device_bytes_peak = peak;
       done_cv.notify_all();
     }
   }
