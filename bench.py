@@ -68,6 +68,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def core_bitset_bytes(n: int) -> int:
+    """Bytes of the dense support's bitset rows for an n-vertex core: one row
+    of ceil(n/32) words per vertex, padded to whole 16-byte vectors."""
+    words = ((n + 31) // 32 + 3) & ~3
+    return n * words * 4
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -518,7 +525,13 @@ def main():
             "gpu_launches": launches,
             "roofline": dict(dominant, note=(
                 "algorithmic bytes = merge-intersection model (support) and per-deletion list reads (peel); "
-                "the dense kernels read bitset rows from L2 instead, so frac can exceed 1")),
+                "the dense kernels read bitset rows from L2 instead, so frac can exceed 1"),
+                traffic_note=(
+                    f"null: no ncu capture at this size; the maximum core's bitset rows "
+                    f"({core_bitset_bytes(stats_last['core_vertices']) / 1e6:.0f} MB) exceed L2, so a smaller "
+                    "case's DRAM bytes do not scale in proportion; the nearest capture (G(n=40000), 200 MB of "
+                    "rows) read 39.1 GB from DRAM per launch for 233 GB of row reads "
+                    "(profiles/k_dense_support_er40k.md)")),
             "rooflines": {"support": roof_sup, "peel": roof_peel},
             "stage_ms": {k: round(stats_last[k], 3) for k in
                          ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel")},
