@@ -95,7 +95,8 @@ kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
  * dropped, repeated and reverse-repeated edges merged).  The record grammar is
  * the reference's (src/kc_gpu.cpp:243-306): a byte is a digit when, as a
  * signed char, it is >= '0'; a line's first two digit runs are x and y; other
- * lines are skipped; a line with one digit run is KT_ERR_PARSE.
+ * lines are skipped; a line with one digit run is KT_ERR_PARSE.  Vertex ids
+ * (here and in kt_load_pairs) must be below 2^32 - 1, else KT_ERR_LIMIT.
  * Replaces the host parse and init_graph (src/kc_gpu.cpp:221-322, 38-65). */
 kt_status kt_load_tsv(kt_ctx* ctx, const char* bytes, uint64_t len, kt_graph** out);
 /* As kt_load_tsv, from a file (mmap, pipelined host-to-device copies).

@@ -86,6 +86,9 @@ int bits_for(uint64_t n) {
 }  // namespace
 
 void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
+  // Vertex counts travel as u32 through the later stages: the all-ones id
+  // (which would make n = 2^32) is refused.
+  if (n > 0xffffffffULL) throw Error(KT_ERR_LIMIT, "vertex id 4294967295: ids must be below 2^32 - 1");
   g.n = n;
   // Keys are min << 32 | max with both halves below 2^vb - 1; the radix sort
   // skips digits shared by every key, so it runs 2 ceil(vb / 8) passes once

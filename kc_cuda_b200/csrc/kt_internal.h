@@ -49,7 +49,7 @@ struct Options {
   int64_t recount_gamma = 16;     // recount round when |F| * thr * gamma > alive * words
   int64_t capped_support = 1;     // search phase: abandon supports that cannot reach the threshold
   int64_t timeout_ms = 20000;     // bound on any device-side wait
-  int64_t parse_pipeline_mb = 256;  // host->device chunk for file ingest
+  int64_t parse_pipeline_mb = 256;  // host->device chunk: file ingest, and the chunked parse of host bytes
   int64_t record_kernel_times = 0;  // events around support / peel kernels
   int64_t debug_checks = 0;       // extra host-side consistency checks
   int64_t verbose = 0;            // stage decisions on stderr
