@@ -130,7 +130,7 @@ void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
   zero(c, degx.get(), (n + 1) * sizeof(uint32_t));
   if (n) KT_CUDA(cudaMemcpyAsync(degx.get(), g.deg.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
   scan_u32_to_u64(c, degx.as<uint32_t>(), g.off.as<uint64_t>(), n + 1);
-  g.adj.alloc(c, (2 * g.m ? 2 * g.m : 1) * sizeof(uint32_t));
+  g.adj.alloc(c, (g.m ? 2 * g.m : 1) * sizeof(uint32_t));
   if (g.m) {
     zero(c, degx.get(), (n + 1) * sizeof(uint32_t));  // reused as per-row cursors
     k_fill<<<grid, 256, 0, c->stream>>>(g.edges.as<uint64_t>(), g.m, g.off.as<uint64_t>(), degx.as<uint32_t>(),
