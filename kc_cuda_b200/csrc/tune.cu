@@ -158,10 +158,10 @@ kt_status kt_autotune(kt_batch* b, uint32_t passes, kt_tune_result* out) {
 kt_status kt_options_save(kt_ctx* h, const char* path) {
   if (!path) return KT_ERR_INVALID;
   KT_API_BEGIN(h)
-  FILE* f = std::fopen(path, "w");
-  if (!f) throw kt::Error(KT_ERR_IO, std::string("cannot write ") + path);
   cudaDeviceProp prop;
   KT_CUDA(cudaGetDeviceProperties(&prop, h->c.device));
+  FILE* f = std::fopen(path, "w");
+  if (!f) throw kt::Error(KT_ERR_IO, std::string("cannot write ") + path);
   std::fprintf(f, "# kt options, tuned on %s (%d SMs)\n", prop.name, prop.multiProcessorCount);
   for (const kt::Param& p : kt::params()) std::fprintf(f, "%s %lld\n", p.name, (long long)(h->c.opt.*p.field));
   const bool ok = std::fclose(f) == 0;
@@ -177,7 +177,8 @@ kt_status kt_options_load(kt_ctx* h, const char* path) {
   char line[256];
   kt::Options o = h->c.opt;
   while (std::fgets(line, sizeof(line), f)) {
-    if (line[0] == '#' || line[0] == '\n') continue;
+    const char* first = line + std::strspn(line, " \t\r\n");
+    if (*first == '#' || *first == '\0') continue;  // comments and blank (or CRLF) lines
     char name[128];
     long long v = 0;
     if (std::sscanf(line, "%127s %lld", name, &v) != 2) {
