@@ -45,7 +45,8 @@ typedef struct kt_graph kt_graph;
  * Replaces initGPU (src/kc.cu:30-53, src/kc_gpu.h:48). */
 kt_status kt_init(int device, uint64_t hbm_budget_bytes, kt_ctx** out);
 void kt_destroy(kt_ctx* ctx);
-/* Text of the last error on this context ("" if none). */
+/* Text of the last error on this context ("" if none): a copy owned by the
+ * calling thread, valid until that thread's next kt_last_error call. */
 const char* kt_last_error(const kt_ctx* ctx);
 const char* kt_status_string(kt_status s);
 

@@ -348,7 +348,15 @@ void kt_destroy(kt_ctx* h) {
   delete h;
 }
 
-const char* kt_last_error(const kt_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
+const char* kt_last_error(const kt_ctx* h) {
+  if (!h) return "null context";
+  // A copy per calling thread, taken under the lock: a serving worker may
+  // overwrite the context's text while the caller reads it.
+  static thread_local std::string copy;
+  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+  copy = h->c.last_error;
+  return copy.c_str();
+}
 
 static int64_t* option_slot(kt::Options& o, const char* name) {
   if (!name) return nullptr;
