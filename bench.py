@@ -1,13 +1,18 @@
-"""Benchmark: kmax-truss solve of one large graph per GPU.
+"""Benchmark: kmax-truss solve of one large graph per GPU, with the batched
+and serving figures of the same run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rmat24|rmat21|rmat16|mix4096|serve]
+                    [--workload rmat24|rmat21|rmat16|chunglu50m|mix4096|serve]
+                    [--no-batched] [--no-serving] [--no-cpu-baseline]
 
 Workload (default rmat24): undirected R-MAT, scale 24 (16.7M vertex ids), edge
 factor 32 (536.9M draws), a/b/c/d = .57/.19/.19/.05, seed 2, cliques of 80,
 120 and 200 planted on seeded random vertices, written as the reference's TSV
-edge list (both directions, grouped by the second column).  Synthetic: the
-seeded generator in kc_cuda_b200/csrc/ktgen.cpp.
+edge list (both directions, grouped by the second column).  chunglu50m is the
+skewed-degree graph: Chung-Lu, 50M vertices, power-law exponent 2.1, expected
+degrees capped at 2M, ~1B edge draws, seed 3, a 150-vertex block of pair
+probability 0.95 (a 32 GB TSV).  Synthetic: the seeded generator in
+kc_cuda_b200/csrc/ktgen.cpp.
 
 One step = one solve of the whole graph:
   value : edges / device time of kt_solve_staged (TSV bytes already in HBM:
@@ -17,16 +22,21 @@ One step = one solve of the whole graph:
           host-to-device copy of the TSV and the device-to-host reads of the
           answer inside).
 The TSV (16 GB) is larger than L2, so no flush is needed between steps.
+`parity` compares the answer with the reference CPU solver's answer on the
+same graph (kc_cpu, recorded in tests/golden/large_configs.json); a mismatch
+fails the run.
+
+`batched` (unless --no-batched): graphs/s of the batched path over graphs
+0..4095 of the batched mix, against the one-graph-per-launch path over the
+same 4,096 graphs (every answer compared), with a per-size-decile table.
+`serving` (unless --no-serving): the serving loop under Poisson arrivals of
+2,000 other mix graphs at 0.8 x the batched graphs/s; p50/p99 latency beside
+the per-graph path under the same arrivals.  Both use fixed counts, not
+--steps.
 
 Under torchrun each rank solves its own replica on its own GPU (graphs are
 independent units: no data-path collective); the step time is the max over
 ranks and value counts the edges of all ranks.
-
---workload mix4096: graphs/s of the batched path over graphs 0..4095 of the
-batched mix, beside the one-graph-per-launch path on a sample (run_mix).
---workload serve: the serving loop under Poisson arrivals of mix graphs at
-0.8 x the batched graphs/s measured in the same run; p50/p99 latency and
-served graphs/s (run_serve).
 
 --impl reference runs the reference's own CPU solver (kc_cpu, built from the
 reference sources into oracle/_ref/) on a bounded sample of the same
@@ -41,22 +51,47 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# name: (scale, edge factor, seed, cliques) of an R-MAT graph, or a spec builder name
 WORKLOADS = {
-    # name: (scale, edge factor, seed, cliques)
     "rmat24": (24, 32, 2, [80, 120, 200]),
     "rmat21": (21, 32, 2, [80, 120, 200]),
     "rmat16": (16, 16, 1, [30]),
-    "mix4096": None,  # batched: the 4,096-graph mix (see run_mix)
-    "serve": None,    # serving loop under Poisson arrivals (see run_serve)
+    "chunglu50m": "chunglu_50m",
+    "mix4096": None,  # batched alone: the 4,096-graph mix
+    "serve": None,    # serving alone: Poisson arrivals of mix graphs
 }
 # CPU sample of the same family for the reference solver (about 10-30 s).
 CPU_SAMPLE = (20, 32, 2, [80, 120, 200])
+# Answers of the reference CPU solver on the single-graph workloads.
+REFERENCE_ANSWERS = os.path.join(ROOT, "tests", "golden", "large_configs.json")
+
+
+def workload_spec(name: str):
+    """(config name, GraphSpec) of a single-graph workload."""
+    from kc_cuda_b200 import gen
+    w = WORKLOADS[name]
+    if isinstance(w, str):
+        spec = getattr(gen, w)()
+        return "chunglu_n50m_g2.1_wmax2m_seed3_block150", spec
+    scale, ef, seed, cliques = w
+    return f"rmat{scale}_ef{ef}_seed{seed}_k" + "_".join(map(str, cliques)), gen.rmat(scale, ef, seed, cliques)
+
+
+def reference_answer(config_name: str):
+    """The reference CPU solver's (kmax, edges) on this workload, if recorded."""
+    try:
+        with open(REFERENCE_ANSWERS) as f:
+            rec = json.load(f).get(config_name)
+    except OSError:
+        return None
+    if not rec:
+        return None
+    return [int(rec["kmax"]), int(rec["kmax_truss_edges"])], rec
 
 
 def load_peaks():
@@ -162,12 +197,11 @@ def barrier(pg):
         pg.barrier()
 
 
-def make_tsv(spec_t, pinned: bool):
+def make_tsv(spec, pinned: bool):
     """Generates the workload graph and its TSV bytes (pinned host memory
     when torch can provide it)."""
     from kc_cuda_b200 import gen
-    scale, ef, seed, cliques = spec_t
-    g = gen.Graph(gen.rmat(scale, ef, seed, cliques))
+    g = gen.Graph(spec)
     size = g.tsv_size()
     buf = None
     if pinned:
@@ -213,6 +247,36 @@ def cpu_baseline_run(steps: int, warmup: int, threads: int):
     return m / med, desc, times
 
 
+def cpu_mix_sample(indices, threads: int, answers: dict):
+    """kc_cpu on a seeded sample of mix graphs (the CPU baseline of the
+    batched path, and the check of its answers against the reference solver):
+    returns graphs/s of kc_cpu (whole-process wall time, one graph at a time
+    on all host cores) and the mismatches against `answers`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import kt_oracle as O
+    if not O.have_kc_cpu():
+        return None
+    from kc_cuda_b200 import gen
+    total = 0.0
+    mism = []
+    with tempfile.TemporaryDirectory() as d:
+        for i in indices:
+            path = os.path.join(d, f"mix{i}.tsv")
+            gen.Graph(gen.mix_graph(i)).write_tsv(path)
+            with open(path, "rb") as f:
+                while f.read(1 << 26):
+                    pass
+            t0 = time.perf_counter()
+            ref = O.run_kc_cpu(path, threads=threads, timeout=900)
+            total += time.perf_counter() - t0
+            os.unlink(path)
+            if tuple(ref) != tuple(answers[i]):
+                mism.append([i, list(ref), list(answers[i])])
+    return {"graphs": len(indices), "graphs_per_s": len(indices) / total, "cores": threads, "kind": "reference",
+            "sample": f"kc_cpu -f on {len(indices)} seeded mix graphs, one at a time, whole-process wall time",
+            "answers_equal": not mism, "mismatches": mism}
+
+
 TUNE_FIRST = 2_000_000  # mix graphs of the autotuner's sample (away from the measured ones)
 SERVE_FIRST = 1_000_000  # mix graphs of the serving workload (away from the batched ones)
 
@@ -252,191 +316,263 @@ def autotune(ctx, args, rank):
     return tune
 
 
-def run_mix(args, world, rank, local, pg):
-    """Batched workload: graphs 0..G-1 of the mix (n log-uniform over
-    [1e3, 1e6], R-MAT or Erdos-Renyi, edge factor 4..64, one clique of 5..60),
-    generated on the device.  value = graphs/s of kt_batch_run with the input
-    generation excluded; the per-graph path (kt_load_mix_graph + kt_solve,
-    one graph at a time) is timed on every `sample_every`-th graph."""
-    import numpy as np
+def mix_sizes(first: int, count: int):
+    """(index, edge keys) of mix graphs first..first+count-1: the generated
+    draws plus the planted clique's edges."""
+    from kc_cuda_b200 import gen
+    out = []
+    for i in range(first, first + count):
+        s = gen.mix_graph(i)
+        c = s.cliques[0] if s.cliques else 0
+        out.append((i, s.draws + c * (c - 1) // 2))
+    return out
 
-    import kc_cuda_b200 as K
+
+def batch_run(ctx, indices=None, first=0, count=0):
+    """One kt_batch_run over mix graphs (a list of indices, or a range);
+    returns (device ms without the input generation, waves, answers)."""
+    b = ctx.batch()
+    if indices is None:
+        b.add_mix(first, count)
+    else:
+        for i in indices:
+            b.add_mix(i, 1)
+    b.run()
+    st = ctx.stats()
+    k, c = b.results()
+    b.free()
+    return st["ms_total"] - st["ms_parse"], st["batch_waves"], [(int(a), int(e)) for a, e in zip(k, c)]
+
+
+def measure_mix(ctx, args, rank, pg, threads):
+    """Batched path vs the one-graph-per-launch path over graphs first..first+G-1
+    of the mix (n log-uniform over [1e3, 1e6], R-MAT or Erdos-Renyi, edge factor
+    4..64, one clique of 5..60), generated on the device (generation excluded
+    from both).  Every batched answer is compared with the graph solved alone."""
+    import numpy as np
     G = args.mix_graphs
-    first = ranges_for(args, rank)["mix"][0]  # each rank its own slice of the mix (independent graphs)
-    ctx = K.Context(local)
-    # Both paths allocate from a pool grown once to the context's budget, so
-    # graphs of new sizes do not map device memory in the middle of a solve.
-    ctx.set_option("pool_reserve_mb", 1 << 30)
-    # Kernel thresholds tuned on a sample of other mix graphs (same
-    # distribution); both paths below run with the tuned settings.
-    tune = autotune(ctx, args, rank)
-    # Per-graph path on a uniform sample.
-    lat = []
-    sample = list(range(first, first + G, args.sample_every))
-    for i in sample[: min(3, len(sample))]:  # warm-up
+    first = ranges_for(args, rank)["mix"][0]
+    idx = list(range(first, first + G))
+    # One graph per launch sequence: kt_load_mix_graph (CSR build timed) + kt_solve.
+    for i in idx[: min(3, G)]:
         g = ctx.load_mix_graph(i)
         g.kmax_truss()
         g.free()
-    answers_alone = {}
-    for i in sample:
+    lat, alone = {}, {}
+    for i in idx:
         g = ctx.load_mix_graph(i)
-        csr_ms = ctx.stats()["ms_csr"]  # the CSR build counts, the generation does not
-        answers_alone[i] = g.kmax_truss()
-        lat.append(csr_ms + ctx.stats()["ms_total"])
+        csr_ms = ctx.stats()["ms_csr"]
+        alone[i] = g.kmax_truss()
+        lat[i] = csr_ms + ctx.stats()["ms_total"]
         g.free()
-    per_graph_gps = len(lat) / (sum(lat) / 1000.0)
-    # Batched.
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        b = ctx.batch()
-        b.add_mix(first, min(G, 64))
-        b.run()
-        b.free()
+    per_graph_ms = max_over_ranks(pg, sum(lat.values()))
+    # Batched: a warm-up batch, then the whole mix in one kt_batch_run per step.
+    batch_run(ctx, first=first, count=min(G, 64))
     barrier(pg)
     times = []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            b = ctx.batch()
-            b.add_mix(first, G)
-            b.run()
-            st = ctx.stats()
-            times.append(st["ms_total"] - st["ms_parse"])
-            k, c = b.results()
-            b.free()
-    for i in sample:
-        assert (int(k[i - first]), int(c[i - first])) == answers_alone[i], i
-    step_ms = max_over_ranks(pg, sum(times) / len(times))
+    for _ in range(args.mix_steps):
+        ms, waves, got = batch_run(ctx, first=first, count=G)
+        times.append(ms)
+    mism = [i for i, a in zip(idx, got) if a != alone[i]]
+    batched_ms = max_over_ranks(pg, sum(times) / len(times))
     total = sum_over_ranks(pg, float(G))
-    value = total / (step_ms / 1000.0)
-    if rank == 0:
-        lat_np = np.array(lat)
-        print(json.dumps({
-            "metric": "batched kmax-truss graphs/s (mix of graphs 0..G-1)", "value": value, "unit": "graphs/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"mix{G}", "graphs": G, "waves": st["batch_waves"],
-                       "edge_records": int(b.size()[1]) if False else None},
-            "per_graph": {"graphs_per_s": per_graph_gps, "sample": len(lat), "every": args.sample_every,
-                          "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
-            "batched_vs_per_graph": value / per_graph_gps,
-            "autotune": tune,
-            "clocks": clk.summary(),
-        }))
-    ctx.close()
+    # Where the ratio comes from: each size decile (by edge keys) as a batch
+    # of its own, against the same graphs one at a time.
+    deciles = []
+    order = sorted(mix_sizes(first, G), key=lambda t: (t[1], t[0]))
+    for d in range(10):
+        part = order[d * G // 10:(d + 1) * G // 10]
+        if not part:
+            continue
+        ids = [i for i, _ in part]
+        bms, bw, dgot = batch_run(ctx, indices=ids)
+        mism += [i for i, a in zip(ids, dgot) if a != alone[i]]
+        pms = sum(lat[i] for i in ids)
+        deciles.append({"decile": d + 1, "graphs": len(ids), "edge_keys": int(sum(s for _, s in part)),
+                        "keys_min": int(part[0][1]), "keys_max": int(part[-1][1]), "waves": bw,
+                        "per_graph_ms": round(pms, 2), "batched_ms": round(bms, 2), "ratio": round(pms / bms, 3)})
+    lat_np = np.array([lat[i] for i in idx])
+    out = {
+        "workload": f"mix graphs {first}..{first + G - 1}", "graphs": G, "steps": args.mix_steps,
+        "graphs_per_s": total / (batched_ms / 1000.0), "ms_per_step": batched_ms, "waves": waves,
+        "per_graph": {"graphs_per_s": total / (per_graph_ms / 1000.0), "ms_total": per_graph_ms, "graphs": G,
+                      "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
+        "ratio": per_graph_ms / batched_ms,
+        "answers_equal_alone": not mism, "mismatches": sorted(set(mism))[:20], "deciles": deciles,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        rng = np.random.default_rng(7)
+        sample = sorted(int(x) for x in rng.choice(idx, size=min(32, G), replace=False))
+        cpu = cpu_mix_sample(sample, threads, alone)
+        if cpu is not None:
+            out["cpu_baseline"] = cpu
+    return out
 
 
-def run_serve(args, world, rank, local, pg):
-    """Serving workload: R requests, request i = graph (offset + i) of the
-    batched mix, Poisson arrivals (fixed seed) at 0.8 x the batched graphs/s
-    measured first on a calibration batch of other mix graphs.  The server
-    admits arrivals into waves as the device frees (kt_server_*).  value =
-    served graphs/s (completed / first submission -> last result); p50/p99
-    latency = submission -> result, measured by the library."""
+def fifo_latencies(arrivals_s, service_ms):
+    """Latencies (ms) of requests served one at a time in arrival order, each
+    taking its measured service time: the per-graph path under the same
+    arrivals."""
+    done = 0.0
+    out = []
+    for a, s in zip(arrivals_s, service_ms):
+        start = max(a * 1000.0, done)
+        done = start + s
+        out.append(done - a * 1000.0)
+    return out
+
+
+def measure_serve(ctx, args, rank, pg, batched_gps=None):
+    """Serving loop: R requests, request i = mix graph (first + i), Poisson
+    arrivals (fixed seed) at 0.8 x the batched graphs/s (measured on the mix,
+    or on a calibration batch of other mix graphs).  Latency = submission ->
+    result, measured by the library.  Every served answer is compared with the
+    graph solved alone, whose device time also gives the per-graph path's
+    latencies under the same arrivals."""
     import numpy as np
 
-    import kc_cuda_b200 as K
     from kc_cuda_b200 import serving
     R = args.serve_requests
     ranges = ranges_for(args, rank)
     calib_first, first = ranges["calib"][0], ranges["serve"][0]
+    calib = None
+    if batched_gps is None:
+        batch_run(ctx, first=calib_first, count=min(64, args.calib_graphs))
+        ms, _, _ = batch_run(ctx, first=calib_first, count=args.calib_graphs)
+        batched_gps = args.calib_graphs / (ms / 1000.0)
+        calib = {"graphs": args.calib_graphs, "first": calib_first}
+    rate = args.serve_rate if args.serve_rate > 0 else 0.8 * batched_gps
+    arrivals = serving.poisson_arrivals(R, rate, seed=55 + rank)
+    barrier(pg)
+    srv = ctx.server()
+    submitted = serving.drive(arrivals, lambda i: srv.submit_mix(first + i))
+    results = [srv.wait(rid) for rid, _ in submitted]
+    sst = srv.stats()
+    srv.close()
+    if not all(r["status"] == 0 for r in results):
+        raise RuntimeError("serving: a request failed")
+    summ = serving.summarize(submitted, results)
+    service, mism = [], []
+    for j in range(R):
+        g = ctx.load_mix_graph(first + j)
+        csr_ms = ctx.stats()["ms_csr"]
+        ans = g.kmax_truss()
+        service.append(csr_ms + ctx.stats()["ms_total"])
+        g.free()
+        if ans != (results[j]["kmax"], results[j]["edges"]):
+            mism.append(first + j)
+    pg_lat = fifo_latencies(arrivals, service)
+    span = max_over_ranks(pg, summ["span_s"])
+    total = sum_over_ranks(pg, float(R))
+    return {
+        "workload": f"{R} Poisson requests, mix graphs {first}..{first + R - 1}", "requests": R,
+        "arrival_rate_per_s": rate, "arrival_seed": 55 + rank, "rate_basis_graphs_per_s": batched_gps,
+        "calibration": calib, "graphs_per_s": total / span, "span_s": span,
+        "p50_ms": summ["p50_ms"], "p99_ms": max_over_ranks(pg, summ["p99_ms"]), "mean_ms": summ["mean_ms"],
+        "max_ms": summ["max_ms"], "wait_p50_ms": summ["wait_p50_ms"],
+        "waves": sst["waves"], "mean_wave_graphs": summ["mean_wave_graphs"],
+        "max_wave_graphs": sst["max_wave_graphs"], "device_bytes_peak": sst["device_bytes_peak"],
+        "per_graph_same_arrivals": {
+            "p50_ms": float(np.percentile(pg_lat, 50)), "p99_ms": float(np.percentile(pg_lat, 99)),
+            "service_p50_ms": float(np.percentile(service, 50)),
+            "method": "one request at a time in arrival order, each taking its measured per-graph device time"},
+        "answers_equal_alone": not mism, "mismatches": mism[:20],
+    }
+
+
+def line_base(metric, value, unit, world, steps, warmup, ms, config):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": config}
+
+
+def run_mix(args, world, rank, local, pg):
+    """--workload mix4096: the batched figures as the line itself."""
+    import kc_cuda_b200 as K
     ctx = K.Context(local)
     ctx.set_option("pool_reserve_mb", 1 << 30)
     tune = autotune(ctx, args, rank)
-    # Calibration: batched graphs/s of this device on other mix graphs.
-    b = ctx.batch()
-    b.add_mix(calib_first, min(64, args.calib_graphs))
-    b.run()
-    b.free()
-    b = ctx.batch()
-    b.add_mix(calib_first, args.calib_graphs)
-    b.run()
-    st = ctx.stats()
-    b.free()
-    calib_gps = args.calib_graphs / ((st["ms_total"] - st["ms_parse"]) / 1000.0)
-    rate = args.serve_rate if args.serve_rate > 0 else 0.8 * calib_gps
-    arrivals = serving.poisson_arrivals(R, rate, seed=55 + rank)
-    barrier(pg)
+    ctx.reset_stats()
     with ClockSampler(local) as clk:
-        srv = ctx.server()
-        submitted = serving.drive(arrivals, lambda i: srv.submit_mix(first + i))
-        results = [srv.wait(rid) for rid, _ in submitted]
-        sst = srv.stats()
-        srv.close()
-    assert all(r["status"] == 0 for r in results)
-    summ = serving.summarize(submitted, results)
-    # Alone vs served on a sample of the requests.
-    mism = 0
-    for j in range(0, R, max(1, R // 16)):
-        g = ctx.load_mix_graph(first + j)
-        if g.kmax_truss() != (results[j]["kmax"], results[j]["edges"]):
-            mism += 1
-        g.free()
-    span = max_over_ranks(pg, summ["span_s"])
-    total = sum_over_ranks(pg, float(R))
-    p99 = max_over_ranks(pg, summ["p99_ms"])
+        mix = measure_mix(ctx, args, rank, pg, os.cpu_count() or 1)
+    launches = ctx.stats()["kernel_launches"]
     if rank == 0:
-        print(json.dumps({
-            "metric": "served kmax-truss graphs/s with p50/p99 latency (Poisson arrivals of mix graphs)",
-            "value": total / span, "unit": "graphs/s", "n_gpus": world, "steps": 1, "warmup": 1,
-            "ms_per_step": span * 1000.0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"serve{R}", "requests": R, "first_graph": first,
-                       "arrival_rate_per_s": rate, "calibration_graphs_per_s": calib_gps,
-                       "calibration_graphs": args.calib_graphs, "arrival_seed": 55 + rank},
-            "latency": {"p50_ms": summ["p50_ms"], "p99_ms": p99, "mean_ms": summ["mean_ms"],
-                        "max_ms": summ["max_ms"], "wait_p50_ms": summ["wait_p50_ms"]},
-            "waves": sst["waves"], "mean_wave_graphs": summ["mean_wave_graphs"],
-            "max_wave_graphs": sst["max_wave_graphs"], "device_bytes_peak": sst["device_bytes_peak"],
-            "alone_vs_served_mismatches": mism, "autotune": tune, "clocks": clk.summary(),
-        }))
+        line = line_base("batched kmax-truss graphs/s (mix of graphs 0..G-1)", mix["graphs_per_s"], "graphs/s",
+                         world, args.mix_steps, 1, mix["ms_per_step"],
+                         {"workload": f"mix{args.mix_graphs}", "graphs": args.mix_graphs, "waves": mix["waves"]})
+        line.update({"batched": mix, "autotune": tune, "gpu_launches": launches, "clocks": clk.summary()})
+        print(json.dumps(line))
     ctx.close()
+    if not mix["answers_equal_alone"]:
+        raise SystemExit("batched answers differ from the graphs solved alone")
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mix-graphs", type=int, default=4096)
-    ap.add_argument("--sample-every", type=int, default=32)
-    ap.add_argument("--serve-requests", type=int, default=2000)
-    ap.add_argument("--serve-rate", type=float, default=0.0, help="requests/s (0: 0.8 x calibrated batched)")
-    ap.add_argument("--calib-graphs", type=int, default=512)
-    ap.add_argument("--tune-graphs", type=int, default=128,
-                    help="mix/serve: autotune the kernel thresholds on this many other mix graphs first (0: off)")
-    args = ap.parse_args()
-    world, rank, local, pg = dist_setup()
-    if args.workload in ("mix4096", "serve") and args.impl == "ours":
-        (run_mix if args.workload == "mix4096" else run_serve)(args, world, rank, local, pg)
-        if pg is not None:
-            pg.destroy_process_group()
-        return
-    threads = os.cpu_count() or 1
-    metric = "kmax-truss solve edges/s per graph"
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        v, desc, times = cpu_baseline_run(args.steps, args.warmup, threads)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": desc}))
-            return
-        print(json.dumps({
-            "impl": "reference", "metric": metric, "value": v, "unit": "edges/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.median(times),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "rmat20_ef32_k80_120_200 (CPU sample of the rmat24 family)", "threads": threads},
-            "cpu_baseline": {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc},
-            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }))
-        return
-
+def run_serve(args, world, rank, local, pg):
+    """--workload serve: the serving figures as the line itself."""
     import kc_cuda_b200 as K
-    spec_t = WORKLOADS[args.workload]
-    g, tsv = make_tsv(spec_t, pinned=True)
+    ctx = K.Context(local)
+    ctx.set_option("pool_reserve_mb", 1 << 30)
+    tune = autotune(ctx, args, rank)
+    ctx.reset_stats()
+    with ClockSampler(local) as clk:
+        srv = measure_serve(ctx, args, rank, pg)
+    launches = ctx.stats()["kernel_launches"]
+    if rank == 0:
+        line = line_base("served kmax-truss graphs/s with p50/p99 latency (Poisson arrivals of mix graphs)",
+                         srv["graphs_per_s"], "graphs/s", world, 1, 1, srv["span_s"] * 1000.0,
+                         {"workload": f"serve{args.serve_requests}", "requests": args.serve_requests})
+        line.update({"serving": srv, "autotune": tune, "gpu_launches": launches, "clocks": clk.summary()})
+        print(json.dumps(line))
+    ctx.close()
+    if not srv["answers_equal_alone"]:
+        raise SystemExit("served answers differ from the graphs solved alone")
+
+
+def run_reference(args, rank, threads):
+    if rank != 0:
+        return
+    metric = "kmax-truss solve edges/s per graph"
+    v, desc, times = cpu_baseline_run(args.steps, args.warmup, threads)
+    if v is None:
+        print(json.dumps({"impl": "reference", "unavailable": desc}))
+        return
+    line = line_base(metric, v, "edges/s", args.gpus, args.steps, args.warmup, 1000 * statistics.median(times),
+                     {"workload": "rmat20_ef32_seed2_k80_120_200 (CPU sample of the rmat24 family: kc_cpu takes "
+                                  "about 2 minutes on the full graph, too long for a bounded step)",
+                      "threads": threads, "same_config": False})
+    line.update({
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    print(json.dumps(line))
+
+
+# DRAM traffic of the dense support kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of a k_dense_support launch
+# on the core55k-support case of cases.py: G(n=55455, 95M draws), whose core
+# has the bench graph's search-core shape.  The bench graph's launches are
+# too large to capture under the profiling size rule, so their traffic is
+# scaled from this one by the row words each launch reads.  None: no capture.
+SUPPORT_CAPTURE = None  # {"dram_bytes": ..., "row_words": ...}
+
+
+def roofline(name, kbytes, kms, klaunch, steps, hbm, peak_kind, **extra):
+    achieved = (kbytes / (kms / 1000.0)) / 1e9 if kms > 0 else 0.0
+    r = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+         "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind,
+         "bytes_per_step": kbytes / steps, "kernel_ms_per_step": kms / steps, "launches_per_step": klaunch / steps}
+    r.update(extra)
+    return r
+
+
+def run_single(args, world, rank, local, pg, threads):
+    import kc_cuda_b200 as K
+    metric = "kmax-truss solve edges/s per graph"
+    config_name, spec = workload_spec(args.workload)
+    g, tsv = make_tsv(spec, pinned=True)
     n_edges, n_vertices = g.num_edges, g.num_vertices
+    del g
     ctx = K.Context(local)
     staged = ctx.stage_tsv(tsv)
 
@@ -451,19 +587,17 @@ def main():
     ctx.reset_stats()
     dev_ms = []
     stats_last = None
-    sup_ms = peel_ms = 0.0
-    sup_bytes = peel_bytes = 0
-    sup_launch = peel_launch = 0
+    acc = {k: 0.0 for k in ("ms_support_kernel", "ms_peel_kernel", "support_bytes", "support_kernel_bytes",
+                            "support_row_words", "peel_bytes", "peel_recount_bytes")}
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             got = staged.solve()
             st = ctx.stats()
-            assert got == answer, (got, answer)
+            if got != answer:
+                raise SystemExit(f"answer changed between steps: {got} vs {answer}")
             dev_ms.append(st["ms_total"])
-            sup_ms += st["ms_support_kernel"]
-            peel_ms += st["ms_peel_kernel"]
-            sup_bytes += st["support_bytes"]
-            peel_bytes += st["peel_bytes"]
+            for k in acc:
+                acc[k] += st[k]
             stats_last = st
     launches = ctx.stats()["kernel_launches"]
     # Launch counters run from reset_stats: they cover the timed steps.
@@ -482,67 +616,137 @@ def main():
         t0 = time.perf_counter()
         got = ctx.solve_tsv(tsv)
         e2e_s.append(time.perf_counter() - t0)
-        assert got == answer
+        if got != answer:
+            raise SystemExit(f"end-to-end answer differs: {got} vs {answer}")
     est = ctx.stats()
     barrier(pg)
     e2e_step = max_over_ranks(pg, sum(e2e_s) / len(e2e_s))
     e2e_value = total_edges / e2e_step
 
     hbm, peak_kind = load_peaks()
+    S = args.steps
+    sup_traffic = None
+    if SUPPORT_CAPTURE and sup_launch:
+        per_word = SUPPORT_CAPTURE["dram_bytes"] / SUPPORT_CAPTURE["row_words"]
+        sup_traffic = per_word * acc["support_row_words"] / sup_launch
+    roof_sup = roofline(
+        "support: k_dense_support (edge support by bitset AND/popcount, all launches of a solve)",
+        acc["support_kernel_bytes"], acc["ms_support_kernel"], sup_launch, S, hbm, peak_kind,
+        bytes_model="row words the kernels read (row u loads, row v words ANDed) x 4 + 16 per edge",
+        merge_model_bytes_per_step=acc["support_bytes"] / S, row_words_per_step=acc["support_row_words"] / S)
+    roof_sup["traffic"] = sup_traffic
+    if sup_traffic is not None:
+        roof_sup["traffic_basis"] = ("DRAM bytes per row word of the core55k-support capture x the row words "
+                                     "of an average launch here")
+    roof_peel = roofline(
+        "peel: k_cascade (one cooperative launch per truss level)", acc["peel_bytes"], acc["ms_peel_kernel"],
+        peel_launch, S, hbm, peak_kind,
+        bytes_model="8 per alive-degree unit of each deleted edge + 8 per support decrement + 4 per alive-list "
+                    "entry scanned",
+        recount_bytes_per_step=acc["peel_recount_bytes"] / S)
+    dominant = roof_sup if acc["ms_support_kernel"] >= acc["ms_peel_kernel"] else roof_peel
 
-    def roof(name, kbytes, kms, klaunch):
-        achieved = (kbytes / (kms / 1000.0)) / 1e9 if kms > 0 else 0.0
-        return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind,
-                "algorithmic_bytes_per_step": kbytes / args.steps, "kernel_ms_per_step": kms / args.steps,
-                "launches_per_step": klaunch / args.steps}
+    ref = reference_answer(config_name)
+    parity = None
+    if ref is not None:
+        parity = {"reference": ref[0], "ours": list(answer), "equal": list(answer) == ref[0],
+                  "reference_solver": f"{ref[1].get('reference_binary', 'kc_cpu')} "
+                                      f"({ref[1].get('reference_threads')} threads)"}
 
-    roof_sup = roof("support: k_dense_support / k_support_bitmap (edge support, all launches of a solve)",
-                    sup_bytes, sup_ms, sup_launch)
-    roof_peel = roof("peel: k_cascade (one cooperative launch per truss level)", peel_bytes, peel_ms, peel_launch)
-    # The dominant of the two by device time is the headline roofline.
-    dominant = roof_sup if sup_ms >= peel_ms else roof_peel
+    mix = srv = None
+    mix_tune = None
+    if not args.no_batched or not args.no_serving:
+        staged.free()
+        staged = None
+        ctx.close()
+        ctx = K.Context(local)
+        ctx.set_option("pool_reserve_mb", 1 << 30)
+        mix_tune = autotune(ctx, args, rank)
+        if not args.no_batched:
+            mix = measure_mix(ctx, args, rank, pg, threads)
+            mix["autotune"] = mix_tune
+        if not args.no_serving:
+            srv = measure_serve(ctx, args, rank, pg, mix["graphs_per_s"] / world if mix else None)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         v, desc, _ = cpu_baseline_run(1, 0, threads)
         if v is not None:
             cpu = {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc}
     if rank == 0:
-        line = {
-            "metric": metric, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"rmat{spec_t[0]}_ef{spec_t[1]}_seed{spec_t[2]}_k" + "_".join(map(str, spec_t[3])),
-                       "vertices": n_vertices, "edges": n_edges, "tsv_bytes": int(tsv.nbytes),
-                       "kmax": answer[0], "kmax_truss_edges": answer[1], "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (TSV bytes re-read every step)",
-                       "cmax": stats_last["cmax"], "core_vertices": stats_last["core_vertices"],
-                       "core_edges": stats_last["core_edges"], "predict_vertices": stats_last["predict_vertices"],
-                       "predict_edges": stats_last["predict_edges"], "levels": stats_last["levels"],
-                       "rounds": stats_last["rounds"], "peel_decrements": stats_last["peel_decrements"]},
+        line = line_base(metric, value, "edges/s", world, args.steps, args.warmup, step_ms, {
+            "workload": config_name, "vertices": n_vertices, "edges": n_edges, "tsv_bytes": int(tsv.nbytes),
+            "kmax": answer[0], "kmax_truss_edges": answer[1], "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (TSV bytes re-read every step)",
+            "cmax": stats_last["cmax"], "core_vertices": stats_last["core_vertices"],
+            "core_edges": stats_last["core_edges"], "predict_vertices": stats_last["predict_vertices"],
+            "predict_edges": stats_last["predict_edges"], "levels": stats_last["levels"],
+            "rounds": stats_last["rounds"], "peel_decrements": stats_last["peel_decrements"]})
+        line.update({
+            "parity": parity,
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": est["h2d_bytes"] // args.steps,
                     "d2h_bytes_per_step": est["d2h_bytes"] // args.steps, "ms_per_step": 1000 * e2e_step},
             "gpu_launches": launches,
             "roofline": dict(dominant, note=(
-                "algorithmic bytes = merge-intersection model (support) and per-deletion list reads (peel); "
-                "the dense kernels read bitset rows from L2 instead, so frac can exceed 1"),
-                traffic_note=(
-                    f"null: no ncu capture at this size; the maximum core's bitset rows "
-                    f"({core_bitset_bytes(stats_last['core_vertices']) / 1e6:.0f} MB) exceed L2, so a smaller "
-                    "case's DRAM bytes do not scale in proportion; the nearest capture (G(n=40000), 200 MB of "
-                    "rows) read 39.1 GB from DRAM per launch for 233 GB of row reads "
-                    "(profiles/k_dense_support_er40k.md)")),
+                "dense support rows are read mostly from L2 (tile order), so frac near 1 of the HBM copy "
+                "bandwidth is L2-served work; traffic is the DRAM share")),
             "rooflines": {"support": roof_sup, "peel": roof_peel},
             "stage_ms": {k: round(stats_last[k], 3) for k in
                          ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel")},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-        }
-        print(json.dumps(line))
-    staged.free()
+            "batched": mix,
+            "serving": srv,
+        })
+        print(json.dumps(line), flush=True)
+    if staged is not None:
+        staged.free()
     ctx.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    bad = []
+    if parity is not None and not parity["equal"]:
+        bad.append(f"answer {list(answer)} differs from the reference solver's {ref[0]}")
+    if mix is not None and not mix["answers_equal_alone"]:
+        bad.append("batched answers differ from the graphs solved alone")
+    if mix is not None and mix.get("cpu_baseline") and not mix["cpu_baseline"]["answers_equal"]:
+        bad.append("batched answers differ from the reference solver's")
+    if srv is not None and not srv["answers_equal_alone"]:
+        bad.append("served answers differ from the graphs solved alone")
+    if bad:
+        raise SystemExit("; ".join(bad))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="single-graph workloads: skip the batched figures")
+    ap.add_argument("--no-serving", action="store_true", help="single-graph workloads: skip the serving figures")
+    ap.add_argument("--mix-graphs", type=int, default=4096)
+    ap.add_argument("--mix-steps", type=int, default=1, help="timed kt_batch_run passes over the whole mix")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="requests/s (0: 0.8 x batched graphs/s)")
+    ap.add_argument("--calib-graphs", type=int, default=512)
+    ap.add_argument("--tune-graphs", type=int, default=128,
+                    help="autotune the kernel thresholds on this many other mix graphs first (0: off)")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    threads = os.cpu_count() or 1
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, threads)
+        elif args.workload == "mix4096":
+            run_mix(args, world, rank, local, pg)
+        elif args.workload == "serve":
+            run_serve(args, world, rank, local, pg)
+        else:
+            run_single(args, world, rank, local, pg, threads)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -1,11 +1,16 @@
 """Small, named workloads for profiling single kernels of the solver.
 
-    python -m kc_cuda_b200.cases <case> [--reps N]
+    python cases.py <case> [--reps N]
 
 Cases (each fits in a few GB of device memory, inputs larger than L2):
   dense-support   Erdos-Renyi G(n=40000, M=48,000,000 draws), seed 7: one
                   kt_edge_support call -> k_dense_support<64> on ~46M edges
                   (bitset rows of 1250 words).
+  core55k-support Erdos-Renyi G(n=55455, M=95,000,000 draws), seed 7: one
+                  kt_edge_support call -> k_dense_support on ~92M edges with
+                  bitset rows of 1736 words (385 MB of rows, above L2): the
+                  shape of the bench graph's search core (55,455 vertices,
+                  92.1M edges).
   rmat21-solve    R-MAT scale 21, edge factor 32, seed 2, cliques 80/120/200:
                   one kt_solve_staged (every stage; peel kernel k_cascade<8>).
   rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
@@ -22,19 +27,21 @@ import time
 
 import numpy as np
 
-from . import gen
-from .solver import Context
+from kc_cuda_b200 import gen
+from kc_cuda_b200.solver import Context
 
 
-def dense_support(reps: int) -> None:
-    spec = gen.GraphSpec(kind=gen.KTG_ER, n=40000, draws=48_000_000, seed=7)
+def dense_support(reps: int, n: int = 40000, draws: int = 48_000_000) -> None:
+    spec = gen.GraphSpec(kind=gen.KTG_ER, n=n, draws=draws, seed=7)
     g = gen.Graph(spec)
     with Context(0) as ctx:
         dg = ctx.load_pairs(g.edges())
         for _ in range(reps):
             t = time.perf_counter()
             sup = dg.tricount()
+            st = ctx.stats()
             print(f"support of {dg.num_edges} edges: {1e3 * (time.perf_counter() - t):.1f} ms, "
+                  f"kernel {st['ms_support_kernel']:.2f} ms, row words read {st['support_row_words']}, "
                   f"sum {int(sup.astype(np.uint64).sum())}", flush=True)
         dg.free()
 
@@ -73,12 +80,14 @@ def mix_batch(reps: int, verbose: bool = False) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense-support", "rmat21-solve", "rmat16-solve", "rmat24-solve", "mix-batch"])
+    ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve", "mix-batch"])
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
     if a.case == "dense-support":
         dense_support(a.reps)
+    elif a.case == "core55k-support":
+        dense_support(a.reps, n=55455, draws=95_000_000)
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
     elif a.case == "mix-batch":

@@ -46,11 +46,13 @@ typedef struct kt_graph kt_graph;
 kt_status kt_init(int device, uint64_t hbm_budget_bytes, kt_ctx** out);
 void kt_destroy(kt_ctx* ctx);
 /* Text of the last error on this context ("" if none): a copy owned by the
- * calling thread, valid until that thread's next kt_last_error call. */
+ * calling thread, valid until that thread's next kt_last_error call.  It does
+ * not wait for a serving wave that holds the context. */
 const char* kt_last_error(const kt_ctx* ctx);
 const char* kt_status_string(kt_status s);
 
-/* Tunables by name; KT_ERR_INVALID for an unknown name.
+/* Tunables by name; KT_ERR_INVALID for an unknown name or a value out of
+ * range (every option is >= 0).
  *   predict (1)                 prediction phase (truss of the maximum core)
  *   persistent (1)              peel / k-core rounds in one cooperative launch
  *   support_bitmap_max_n (2^20) vertex-bitmap support up to this many vertices
@@ -58,7 +60,9 @@ const char* kt_status_string(kt_status s);
  *   dense_min_fill (32)         bitsets when avg degree * this >= words per row
  *   recount_gamma (16)          recount round when frontier * thr * gamma > alive * words
  *   capped_support (1)          search phase: abandon supports below the threshold
- *   timeout_ms (20000)          bound on every device-side wait
+ *   timeout_ms (20000)          bound on every device-side wait, 0..3600000; 0 makes
+ *                               every bounded wait give up at once, so a solve
+ *                               returns KT_ERR_TIMEOUT (a test of the error path)
  *   parse_pipeline_mb (256)     host->device chunk of file ingest, and of host TSV
  *                               bytes parsed chunk by chunk as they land (inputs of
  *                               three chunks or more)
@@ -239,8 +243,10 @@ kt_status kt_kcore(kt_ctx* ctx, kt_graph* g, uint32_t k, uint8_t* member_out, ui
  * cannot afford the synchronisation an allocation may imply).  No
  * counterpart in the reference.  DEVICE pointers: d_off (n+1 row offsets)
  * and d_adj (neighbour ids; symmetric, no self-loops, any row order) in,
- * d_member (n bytes, 1 = in the k-core) out; stream may be NULL (default
- * stream).  Allocates nothing: its working memory is one fixed device array
+ * d_member (n bytes, 1 = in the k-core) out; none may be NULL (KT_ERR_INVALID).
+ * stream may be NULL (default stream); otherwise it must belong to the current
+ * device (KT_ERR_INVALID).  d_member is unspecified unless the call returns
+ * KT_OK.  Allocates nothing: its working memory is one fixed device array
  * of about 16 MB that every GPU loading the library holds until exit, which
  * caps n at 1,048,576 (KT_ERR_LIMIT above).  The first call on a device looks
  * up that array's device address and should come before any stream capture.
@@ -267,13 +273,25 @@ typedef struct kt_stats {
   uint64_t core_vertices, core_edges;       /* search-phase subgraph */
   uint64_t predict_vertices, predict_edges; /* prediction-phase subgraph */
   uint32_t cmax, kmax_lower_bound, levels, rounds;
-  uint64_t support_bytes, peel_bytes;       /* algorithmic bytes of the last solve */
+  uint64_t support_bytes, peel_bytes;       /* algorithmic bytes of the last solve: a merge
+                                               intersection's reads (support); list reads and
+                                               decrements of the deletions (peel) */
   double ms_support_kernel, ms_peel_kernel; /* summed kernel time (events) */
   uint64_t support_launches, peel_launches;
   uint64_t device_bytes_peak;
   uint64_t h2d_bytes, d2h_bytes;            /* host<->device traffic since kt_stats_reset */
   uint64_t peel_decrements;                 /* support decrements of the last solve */
   uint32_t batch_waves, batch_graphs;       /* last kt_batch_run */
+  /* Bytes the support kernels that ran moved, by their own access pattern:
+   * for the dense (bitset) kernels 4 per row word read (row u loads, and the
+   * words of row v actually ANDed, so a capped count's abandoned segments are
+   * not counted) plus 16 per edge (list entry, ends, result); for the list
+   * kernels the merge model of support_bytes. */
+  uint64_t support_kernel_bytes;
+  uint64_t support_row_words;               /* the dense kernels' row words read */
+  uint64_t peel_recount_bytes;              /* bitset rows read by the peel's recount rounds */
+  uint32_t csr_grouped;  /* last graph build took the rows straight from grouped TSV lines (1) or sorted (0) */
+  uint32_t pad0;
 } kt_stats;
 kt_status kt_get_stats(const kt_ctx* ctx, kt_stats* out);
 kt_status kt_stats_reset(kt_ctx* ctx);

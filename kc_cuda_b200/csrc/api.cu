@@ -20,6 +20,14 @@ namespace kt {
 
 DevWords* dev_words(Ctx* c) { return c->words.as<DevWords>(); }
 
+bool option_value_ok(const char* name, int64_t value) {
+  if (value < 0) return false;
+  // timeout_ms = 0 is allowed: every bounded device wait then gives up at
+  // once (the error path, for tests); above an hour is refused.
+  if (!std::strcmp(name, "timeout_ms")) return value <= 3600000;
+  return true;
+}
+
 void reset_words(Ctx* c) {
   KT_CUDA(cudaMemsetAsync(c->words.get(), 0, sizeof(DevWords), c->stream));
   KT_CUDA(cudaMemsetAsync(&dev_words(c)->bad_line, 0xff, sizeof(unsigned long long), c->stream));
@@ -90,7 +98,7 @@ void graph_from_device_bytes(Ctx* c, const uint8_t* dbuf, uint64_t len, Graph& g
   reset_words(c);
   block_off.release();
   KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
-  build_graph(c, keys.as<uint64_t>(), lines, n, g);
+  build_graph(c, keys.as<uint64_t>(), lines, n, g, true);
   KT_CUDA(cudaEventRecord(c->ev[6], c->stream));
   c->stats.ms_parse = event_ms(c->ev[4], c->ev[5]);
   c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
@@ -168,7 +176,7 @@ static void load_tsv_pipelined(Ctx* c, const char* bytes, uint64_t len, uint64_t
   const uint64_t n = (w.counters[1] & 1) ? (uint64_t)(uint32_t)w.counters[0] + 1 : 0;
   reset_words(c);
   KT_CUDA(cudaEventRecord(c->ev[5], c->stream));
-  build_graph(c, keys.as<uint64_t>(), lines, n, g);
+  build_graph(c, keys.as<uint64_t>(), lines, n, g, true);
   KT_CUDA(cudaEventRecord(c->ev[6], c->stream));
   c->stats.ms_parse = event_ms(c->ev[4], c->ev[5]);  // copy and parse, overlapped
   c->stats.ms_csr = event_ms(c->ev[5], c->ev[6]);
@@ -350,10 +358,11 @@ void kt_destroy(kt_ctx* h) {
 
 const char* kt_last_error(const kt_ctx* h) {
   if (!h) return "null context";
-  // A copy per calling thread, taken under the lock: a serving worker may
-  // overwrite the context's text while the caller reads it.
+  // A copy per calling thread, taken under the error text's own mutex: a
+  // serving worker may overwrite the text while the caller reads it, and the
+  // worker holds the context lock for a whole wave.
   static thread_local std::string copy;
-  std::lock_guard<std::recursive_mutex> lk(h->c.mu);
+  std::lock_guard<std::mutex> lk(h->c.err_mu);
   copy = h->c.last_error;
   return copy.c_str();
 }
@@ -394,7 +403,7 @@ kt_status kt_set_option(kt_ctx* h, const char* name, int64_t value) {
   if (!h) return KT_ERR_INVALID;
   std::lock_guard<std::recursive_mutex> lk(h->c.mu);
   int64_t* p = option_slot(h->c.opt, name);
-  if (!p) return KT_ERR_INVALID;
+  if (!p || !kt::option_value_ok(name, value)) return KT_ERR_INVALID;
   *p = value;
   if (!std::strcmp(name, "pool_reserve_mb") && value > 0) {
     // Grow the context's memory pool once, up front: later allocations up to

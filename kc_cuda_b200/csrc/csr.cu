@@ -1,13 +1,28 @@
-// Stage (b): canonical edge keys -> cleaned undirected graph on the device.
+// Stage (b): edge records -> cleaned undirected graph on the device.
 //
-// keys (min << 32 | max, ~0 = no edge) are radix sorted over 2*ceil(log2 n)
-// bits, repeats are dropped by a sorted-unique compaction, and the symmetric
-// CSR is filled from the unique list: degrees with warp-aggregated atomics
-// (runs of equal u in the sorted list collapse to one atomic), an exclusive
-// scan for the uint64 row offsets, and a cursor scatter (rows unsorted; the
-// k-core stage does not need them sorted, the subgraph stage re-sorts).
-// Replaces init_graph (src/kc_gpu.cpp:38-65), whose rows come straight from
-// the file because the reference requires pre-cleaned, grouped input.
+// Two routes to the same Graph (sorted canonical edge list, symmetric CSR,
+// degrees):
+//
+// * Grouped input -- the reference's input contract (lines grouped by the
+//   second column in ascending order, every edge listed in both directions,
+//   no repeats, no self-loops), with each row's first-column values in
+//   ascending order.  The rows are the lines themselves, as the reference
+//   builds them by concatenation (init_graph, src/kc_gpu.cpp:38-65, degrees
+//   from run lengths at src/kc_gpu.cpp:283-302): one pass checks the order,
+//   writes the adjacency and the row offsets; a second pass checks symmetry
+//   (every arc (y -> x) with x < y is found in row x by binary search, and
+//   the arcs with x > y are as many as those with x < y) and writes the
+//   canonical edge list, which is the x > y arcs in line order.  Any check
+//   that fails sends the records to the general route; nothing is modified
+//   before that decision.
+// * General route -- records in any order with repeats and self-loops:
+//   canonical keys min << 32 | max (~0 = no edge) radix sorted over
+//   2*ceil(log2 n) bits, repeats dropped by a sorted-unique compaction, and
+//   the symmetric CSR filled from the unique list: degrees with warp-
+//   aggregated atomics (runs of equal u in the sorted list collapse to one
+//   atomic), an exclusive scan for the uint64 row offsets, and a cursor
+//   scatter (rows unsorted; the k-core stage does not need them sorted, the
+//   subgraph stage re-sorts).
 #include "stages.h"
 
 namespace kt {
@@ -53,20 +68,151 @@ __global__ void k_max_u32(const uint32_t* __restrict__ a, uint64_t n, uint32_t* 
   if (lane_id() == 0 && mx) atomicMax(out, mx);
 }
 
-// u << 32 | v -> u << vb | v (both below 2^vb - 1); the "no edge" key ~0
+// A record a << 32 | b (either order) as the canonical min << 32 | max.
+__device__ __forceinline__ uint64_t canon_key(uint64_t k) {
+  const uint32_t a = (uint32_t)(k >> 32), b = (uint32_t)k;
+  return a < b ? k : (((uint64_t)b << 32) | a);
+}
+
+// record -> min << vb | max (both below 2^vb - 1); the "no edge" key ~0
 // becomes 2^(2 vb) - 1, which sorts after every real key.  The sort then
 // runs over 2 vb bits instead of 32 + vb.
 __global__ void k_pack(uint64_t* __restrict__ keys, uint64_t n, int vb) {
   const uint64_t none = (((uint64_t)1) << (2 * vb)) - 1;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
-    keys[i] = k == ~0ULL ? none : ((k >> 32) << vb) | (uint32_t)k;
+    const uint64_t c = canon_key(k);
+    keys[i] = k == ~0ULL ? none : ((c >> 32) << vb) | (uint32_t)c;
+  }
+}
+
+// record -> canonical key, with `from` (the "no edge" key) replaced by `to`.
+__global__ void k_canon_remap(uint64_t* __restrict__ keys, uint64_t n, uint64_t from, uint64_t to) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    keys[i] = k == from ? to : canon_key(k);
   }
 }
 
 __global__ void k_remap(uint64_t* __restrict__ keys, uint64_t n, uint64_t from, uint64_t to) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     if (keys[i] == from) keys[i] = to;
+}
+
+// ------------------------------------------------------------ grouped input
+
+// Largest run of vertex ids without lines between two groups that one
+// thread fills in; inputs with longer gaps take the general route.
+constexpr uint64_t kMaxGap = 4096;
+
+// Pass 1 over the records y << 32 | x in line order: *bad is set unless
+// every line is a record, y never decreases, and x strictly increases within
+// a group.  Writes adj[i] = x, off[v] = first line of row v for every
+// v in [0, n] (rows without lines get the next row's start), and up[y] =
+// the first line of row y with x > y (left at ~0 when there is none).
+__global__ void k_grouped_rows(const uint64_t* __restrict__ keys, uint64_t nk, uint64_t n,
+                               uint64_t* __restrict__ off, uint64_t* __restrict__ up, uint32_t* __restrict__ adj,
+                               uint32_t* __restrict__ bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    if (k == ~0ULL) {  // a blank line or a self-loop
+      atomicOr(bad, 1u);
+      continue;
+    }
+    const uint64_t y = k >> 32;
+    const uint32_t x = (uint32_t)k;
+    adj[i] = x;
+    bool row_start = true;
+    bool prev_up = false;
+    if (i == 0) {
+      if (y + 1 > kMaxGap) {
+        atomicOr(bad, 1u);
+      } else {
+        for (uint64_t v = 0; v <= y; ++v) off[v] = 0;
+      }
+    } else {
+      const uint64_t p = keys[i - 1];
+      if (p != ~0ULL) {  // a ~0 line flags itself
+        const uint64_t py = p >> 32;
+        if (y < py) {
+          atomicOr(bad, 1u);
+        } else if (y > py) {
+          if (y - py > kMaxGap) {
+            atomicOr(bad, 1u);
+          } else {
+            for (uint64_t v = py + 1; v <= y; ++v) off[v] = i;
+          }
+        } else {
+          row_start = false;
+          if ((uint32_t)p >= x) atomicOr(bad, 1u);
+          prev_up = (uint32_t)p > y;
+        }
+      }
+    }
+    if (i == nk - 1) {
+      if (n - y > kMaxGap) {
+        atomicOr(bad, 1u);
+      } else {
+        for (uint64_t v = y + 1; v <= n; ++v) off[v] = nk;
+      }
+    }
+    if (x > y && (row_start || !prev_up)) up[y] = i;
+  }
+}
+
+// Per vertex: degree, upper-part start (rows without x > y end there), the
+// upper count, and the largest degree.
+__global__ void k_grouped_degrees(uint64_t n, const uint64_t* __restrict__ off, uint64_t* __restrict__ up,
+                                  uint32_t* __restrict__ deg, uint32_t* __restrict__ ucnt, uint32_t* __restrict__ mx) {
+  uint32_t m = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = off[v], e = off[v + 1];
+    uint64_t u = up[v];
+    if (u == ~0ULL) {
+      u = e;
+      up[v] = u;
+    }
+    deg[v] = (uint32_t)(e - b);
+    ucnt[v] = (uint32_t)(e - u);
+    m = max(m, (uint32_t)(e - b));
+  }
+  m = warp_max(m);
+  if (lane_id() == 0 && m) atomicMax(mx, m);
+}
+
+// First position in sorted a[lo, hi) holding a value >= x.
+__device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t* __restrict__ a, uint64_t lo, uint64_t hi,
+                                                    uint32_t x) {
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Pass 2: every arc (y -> x) with x < y must have its reverse in row x's
+// upper part (else *bad); every arc with x > y is the canonical edge
+// y << 32 | x, written at its row's edge offset (the edges come out sorted).
+// Runs only once the upper arcs are known to be half of the lines, so every
+// edge index is below that half.
+__global__ void k_grouped_edges(const uint64_t* __restrict__ keys, uint64_t nk, const uint64_t* __restrict__ off,
+                                const uint64_t* __restrict__ up, const uint64_t* __restrict__ eoff,
+                                const uint32_t* __restrict__ adj, uint64_t* __restrict__ edges,
+                                uint32_t* __restrict__ bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const uint32_t y = (uint32_t)(k >> 32), x = (uint32_t)k;
+    if (x > y) {
+      edges[eoff[y] + (i - up[y])] = k;
+    } else {
+      const uint64_t lo = up[x], hi = off[x + 1];
+      const uint64_t p = lower_bound_u32(adj, lo, hi, y);
+      if (p == hi || adj[p] != y) atomicOr(bad, 1u);
+    }
+  }
 }
 
 __global__ void k_unpack(uint64_t* __restrict__ keys, uint64_t n, int vb) {
@@ -83,12 +229,66 @@ int bits_for(uint64_t n) {
   return b;
 }
 
+// The grouped-input route; false (g and keys untouched) when the records
+// are not in that form.
+bool build_graph_grouped(Ctx* c, const uint64_t* keys, uint64_t nk, uint64_t n, Graph& g) {
+  if (nk == 0 || (nk & 1) || n == 0 || n > 0xffffffffULL) return false;
+  const unsigned grid = grid_for(nk, 256, c->num_sms * 16);
+  DBuf flags(c, 8);  // [0] bad, [1] largest degree
+  zero(c, flags.get(), 8);
+  DBuf off(c, (n + 1) * sizeof(uint64_t)), up(c, n * sizeof(uint64_t)), adj(c, nk * sizeof(uint32_t));
+  KT_CUDA(cudaMemsetAsync(up.get(), 0xff, up.bytes(), c->stream));
+  k_grouped_rows<<<grid, 256, 0, c->stream>>>(keys, nk, n, off.as<uint64_t>(), up.as<uint64_t>(), adj.as<uint32_t>(),
+                                              flags.as<uint32_t>());
+  KT_LAUNCHED(c);
+  if (read_word<uint32_t>(c, flags.as<uint32_t>())) return false;
+  DBuf deg(c, n * sizeof(uint32_t)), ucnt(c, (n + 1) * sizeof(uint32_t));
+  zero(c, ucnt.as<uint32_t>() + n, sizeof(uint32_t));
+  k_grouped_degrees<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      n, off.as<uint64_t>(), up.as<uint64_t>(), deg.as<uint32_t>(), ucnt.as<uint32_t>(), flags.as<uint32_t>() + 1);
+  KT_LAUNCHED(c);
+  DBuf eoff(c, (n + 1) * sizeof(uint64_t));
+  scan_u32_to_u64(c, ucnt.as<uint32_t>(), eoff.as<uint64_t>(), n + 1);
+  ucnt.release();
+  // Arcs with x > y must be exactly half of the lines (the other half being
+  // their reverses, checked next).
+  if (2 * read_word<uint64_t>(c, eoff.as<uint64_t>() + n) != nk) return false;
+  DBuf edges(c, nk / 2 * sizeof(uint64_t));
+  k_grouped_edges<<<grid, 256, 0, c->stream>>>(keys, nk, off.as<uint64_t>(), up.as<uint64_t>(), eoff.as<uint64_t>(),
+                                               adj.as<uint32_t>(), edges.as<uint64_t>(), flags.as<uint32_t>());
+  KT_LAUNCHED(c);
+  uint32_t h[2];
+  copy_d2h(c, h, flags.get(), 8);
+  if (h[0]) return false;
+  g.n = n;
+  g.m = nk / 2;
+  g.off = std::move(off);
+  g.adj = std::move(adj);
+  g.edges = std::move(edges);
+  g.deg = std::move(deg);
+  g.max_deg = h[1];
+  return true;
+}
+
+void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g);
+
 }  // namespace
 
-void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
+void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines) {
   // Vertex counts travel as u32 through the later stages: the all-ones id
   // (which would make n = 2^32) is refused.
   if (n > 0xffffffffULL) throw Error(KT_ERR_LIMIT, "vertex id 4294967295: ids must be below 2^32 - 1");
+  c->stats.csr_grouped = 0;
+  if (lines && build_graph_grouped(c, keys, nkeys, n, g)) {
+    c->stats.csr_grouped = 1;
+    return;
+  }
+  build_graph_sorted(c, keys, nkeys, n, g);
+}
+
+namespace {
+
+void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
   g.n = n;
   // Keys are min << 32 | max with both halves below 2^vb - 1; the radix sort
   // skips digits shared by every key, so it runs 2 ceil(vb / 8) passes once
@@ -99,11 +299,13 @@ void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
   const bool small = vb < 32 && nkeys;
   const bool pack = small && (2 * vb + 7) / 8 < 2 * ((vb + 7) / 8);
   const uint64_t sentinel = ((((uint64_t)1 << (vb & 31)) - 1) << 32) | (((uint64_t)1 << (vb & 31)) - 1);
+  // Records may hold either end first: every route makes them canonical.
   if (pack) {
     k_pack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
     KT_LAUNCHED(c);
-  } else if (small) {
-    k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL, sentinel);
+  } else if (nkeys) {
+    k_canon_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL,
+                                                                                 small ? sentinel : ~0ULL);
     KT_LAUNCHED(c);
   }
   if (nkeys > 1) radix_sort_u64(c, keys, nullptr, nkeys, 64);
@@ -145,5 +347,7 @@ void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
   }
   g.max_deg = read_word<uint32_t>(c, mx.as<uint32_t>());
 }
+
+}  // namespace
 
 }  // namespace kt

@@ -130,7 +130,7 @@ __device__ __forceinline__ uint32_t half_and_popc(const uint32_t* __restrict__ p
 __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                             const uint64_t* __restrict__ ends, const DenseRows& R,
                                             const uint32_t* __restrict__ state, uint32_t* su, uint32_t& my_e,
-                                            uint32_t& my_s, bool& my_ok) {
+                                            uint32_t& my_s, bool& my_ok, unsigned long long* wr = nullptr) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -158,6 +158,7 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
       W = R.words(uj);
       dense_load_row(R.bits + R.off(uj), W, su);
       cu = uj;
+      if (wr && l == 0) *wr += W;
     }
 #if KT_EXACT_PAIRS
     // The next edge with the same row u goes to the upper half of the warp.
@@ -177,9 +178,11 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
     const uint32_t f0 = __shfl_sync(kFull, s, 0), f1 = __shfl_sync(kFull, s, 16);
     if (l == (unsigned)j) my_s = f0;
     if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
+    if (wr && l == 0) *wr += j2 >= 0 ? 2ull * W : W;
 #else
     const uint32_t s = dense_and_popc(R.bits + R.off(vj), su, 0, W);
     if (l == (unsigned)j) my_s = s;
+    if (wr && l == 0) *wr += W;
 #endif
   }
   __syncwarp();
@@ -193,7 +196,7 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends, const DenseRows& R,
                                                    uint32_t thr, uint32_t* su, uint32_t& my_e, uint32_t& my_s,
-                                                   bool& my_ok) {
+                                                   bool& my_ok, unsigned long long* wr = nullptr) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -233,6 +236,7 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       s1 = warp_sum(b);
       s2 = warp_sum(c);
       s3 = warp_sum(d);
+      if (wr && l == 0) *wr += W;
     }
 #if KT_CAPPED_PAIRS
     // The next edge with the same row u goes to the upper half of the warp:
@@ -251,31 +255,45 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     const bool upper = l >= 16;
     bool go = !upper || j2 >= 0;
     const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
+    uint32_t wds = go ? c1 : 0u;  // row-v words this half reads
     uint32_t found = half_and_popc(pv, su, 0, c1, go);
     go = go && found + s1 + s2 + s3 >= thr;
     if (__any_sync(kFull, go)) {
+      wds += go ? c2 - c1 : 0u;
       found += half_and_popc(pv, su, c1, c2, go);
       go = go && found + s2 + s3 >= thr;
       if (__any_sync(kFull, go)) {
+        wds += go ? c3 - c2 : 0u;
         found += half_and_popc(pv, su, c2, c3, go);
         go = go && found + s3 >= thr;
-        if (__any_sync(kFull, go)) found += half_and_popc(pv, su, c3, W, go);
+        if (__any_sync(kFull, go)) {
+          wds += go ? W - c3 : 0u;
+          found += half_and_popc(pv, su, c3, W, go);
+        }
       }
     }
     const uint32_t f0 = __shfl_sync(kFull, found, 0), f1 = __shfl_sync(kFull, found, 16);
     if (l == (unsigned)j) my_s = f0;
     if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
+    if (wr && (l & 15u) == 0) *wr += wds;
 #else
     const uint32_t* pv = R.bits + R.off(vj);
+    uint32_t wds = c1;
     uint32_t found = dense_and_popc(pv, su, 0, c1);
     if (found + s1 + s2 + s3 >= thr) {
+      wds = c2;
       found += dense_and_popc(pv, su, c1, c2);
       if (found + s2 + s3 >= thr) {
+        wds = c3;
         found += dense_and_popc(pv, su, c2, c3);
-        if (found + s3 >= thr) found += dense_and_popc(pv, su, c3, W);
+        if (found + s3 >= thr) {
+          wds = W;
+          found += dense_and_popc(pv, su, c3, W);
+        }
       }
     }
     if (l == (unsigned)j) my_s = found;
+    if (wr && l == 0) *wr += wds;
 #endif
   }
   __syncwarp();

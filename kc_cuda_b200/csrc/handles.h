@@ -32,15 +32,15 @@ struct kt_batch {
   return KT_OK;                                      \
   }                                                  \
   catch (const kt::Error& e) {                       \
-    (ctx)->c.last_error = e.what();                  \
+    (ctx)->c.set_error(e.what());                    \
     return e.status;                                 \
   }                                                  \
   catch (const std::bad_alloc&) {                    \
-    (ctx)->c.last_error = "host allocation failed";  \
+    (ctx)->c.set_error("host allocation failed");    \
     return KT_ERR_NOMEM;                             \
   }                                                  \
   catch (const std::exception& e) {                  \
-    (ctx)->c.last_error = e.what();                  \
+    (ctx)->c.set_error(e.what());                    \
     return KT_ERR_CUDA;                              \
   }
 

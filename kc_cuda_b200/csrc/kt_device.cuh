@@ -151,7 +151,9 @@ __device__ __forceinline__ bool grid_barrier(DevWords* w, unsigned long long tim
       unsigned spins = 0;
       while (ld_acquire_u32(&w->bar_gen) == gen) {
         if (++spins > 32) __nanosleep(spins > 1024 ? 256 : 32);
-        if ((spins & 63) == 0 && globaltimer_ns() - t0 > timeout_ns) {
+        // The bound is checked on the first spin and every 64th after it, so
+        // a bound of 0 gives up at once.
+        if ((spins & 63) == 1 && globaltimer_ns() - t0 >= timeout_ns) {
           atomicOr(&w->err, kDevErrBarrier);
           break;
         }

@@ -65,6 +65,10 @@ struct Options {
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
 };
 
+// Range check of an option value: every option is a count, size, ratio or
+// flag (no negative values); timeout_ms is at most one hour.
+bool option_value_ok(const char* name, int64_t value);
+
 // Stage decisions on stderr when the context's verbose option is set.
 #define KT_LOG(c, ...)                                  \
   do {                                                  \
@@ -145,7 +149,14 @@ struct Ctx {
   uint64_t peak = 0;
   uint64_t launches = 0;
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
+  // Text of the last error.  Guarded by its own mutex, not by `mu`, so a
+  // reader is never held up by a serving wave that owns the context.
   std::string last_error;
+  mutable std::mutex err_mu;
+  void set_error(const std::string& m) {
+    std::lock_guard<std::mutex> l(err_mu);
+    last_error = m;
+  }
   Options opt;
   kt_stats stats{};
   mutable std::recursive_mutex mu;  // every entry point, readers included

@@ -137,11 +137,22 @@ extern "C" kt_status kt_kcore_noalloc(const uint64_t* d_off, const uint32_t* d_a
   using namespace kt;
   if (n > kNoAllocMaxVertices) return KT_ERR_LIMIT;
   if (n == 0) return KT_OK;
-  if (!d_off || !d_member) return KT_ERR_INVALID;
+  if (!d_off || !d_adj || !d_member) return KT_ERR_INVALID;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     return KT_ERR_NODEV;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s) {
+    // The array's address is per device: a stream of another device would
+    // get this device's address.  Such a call is refused.
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) {
+      cudaGetLastError();
+      return KT_ERR_INVALID;
+    }
+    if (sdev != dev) return KT_ERR_INVALID;
   }
   DeviceSetup setup;
   {
@@ -165,7 +176,6 @@ extern "C" kt_status kt_kcore_noalloc(const uint64_t* d_off, const uint32_t* d_a
     }
     setup = g_setup[dev];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   // The header (error flag, barrier words, frontier counters) must start at
   // zero; the arrays are written before they are read.
   if (cudaMemsetAsync(setup.base, 0, kHeaderBytes, s) != cudaSuccess) {

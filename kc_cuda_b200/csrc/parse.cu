@@ -1,4 +1,4 @@
-// Stage (a): TSV bytes on the device -> one canonical edge key per line.
+// Stage (a): TSV bytes on the device -> one edge record per line.
 //
 // The grammar is the reference parser's (src/kc_gpu.cpp:243-306): a byte is
 // a digit when, read as a signed char, it is >= '0', and contributes
@@ -14,8 +14,10 @@
 // stages the block's bytes (plus a 1 KB overhang) in shared memory, finds the
 // chunk's newlines a word at a time (__vcmpeq4), lists the block's line
 // starts in shared memory, and deals the lines round-robin to the threads;
-// line i of the block goes to slot block_offset + i.  A slot gets min(x,y) << 32 | max(x,y),
-// or ~0 for a blank line or a self-loop (sorted to the end, then dropped).
+// line i of the block goes to slot block_offset + i.  A slot gets the record
+// y << 32 | x (the grouping column high), or ~0 for a blank line or a
+// self-loop; the CSR build reads the records in line order (grouped input)
+// or canonicalises them to min << 32 | max for its sort.
 #include "kt_device.cuh"
 #include "kt_internal.h"
 #include "stages.h"
@@ -70,7 +72,7 @@ struct Bytes {
   }
 };
 
-// The line at `start`: ~0 for a blank line or a self-loop, min << 32 | max
+// The line at `start`: ~0 for a blank line or a self-loop, y << 32 | x
 // otherwise; *bad when it holds a single number.
 __device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t p, bool* bad, uint32_t* vmax) {
   int b = B.at(p);
@@ -91,8 +93,7 @@ __device__ __forceinline__ uint64_t parse_line(const Bytes& B, uint64_t p, bool*
     b = B.at(++p);
   }
   *vmax = max(*vmax, max(x, y));
-  if (x == y) return ~0ull;
-  return x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x);
+  return x == y ? ~0ull : (((uint64_t)y << 32) | x);
 }
 
 // The same parse from the staged words held in a register window: one
@@ -143,7 +144,7 @@ __device__ __forceinline__ bool parse_line_fast(const uint32_t* stage, uint64_t 
 #undef KT_ADV
 #undef KT_DIGIT
   *vmax = max(*vmax, max(x, y));
-  *key = x == y ? ~0ull : (x < y ? (((uint64_t)x << 32) | y) : (((uint64_t)y << 32) | x));
+  *key = x == y ? ~0ull : (((uint64_t)y << 32) | x);
   return true;
 }
 

@@ -752,13 +752,15 @@ struct Peeler {
 
   // Algorithmic bytes of this peel: 8 per alive-degree unit of every deleted
   // edge (neighbour id + edge id), 8 per support decrement (read-modify-
-  // write), 4 per alive-list entry scanned by a level frontier, and in dense
-  // recount rounds one bitset row (4 W bytes) per recounted edge.
+  // write), 4 per alive-list entry scanned by a level frontier.  The dense
+  // recount rounds' bitset rows (4 W bytes per recounted edge, mostly from
+  // L2) are kept apart in peel_recount_bytes.
   void account() {
     uint64_t h[3];
     copy_d2h(c, h, acct.get(), 24);
     const double wavg = s->W ? (double)s->bit_words / std::max<uint32_t>(s->n, 1) : 0.0;
-    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned + (uint64_t)(4.0 * wavg * (double)h[2]);
+    c->stats.peel_bytes += 8 * h[0] + 8 * h[1] + 4 * scanned;
+    c->stats.peel_recount_bytes += (uint64_t)(4.0 * wavg * (double)h[2]);
     c->stats.peel_decrements += h[1];
   }
 

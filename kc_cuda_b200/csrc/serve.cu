@@ -107,13 +107,13 @@ struct kt_server {
           kt::solve_wave(c, items);
           kt::sync(c);
         } catch (const kt::Error& e) {
-          c->last_error = e.what();
+          c->set_error(e.what());
           status = e.status;
         } catch (const std::bad_alloc&) {
-          c->last_error = "host allocation failed";
+          c->set_error("host allocation failed");
           status = KT_ERR_NOMEM;
         } catch (const std::exception& e) {
-          c->last_error = e.what();
+          c->set_error(e.what());
           status = KT_ERR_CUDA;
         }
         try {

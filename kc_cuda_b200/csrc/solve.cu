@@ -61,6 +61,7 @@ void begin_solve_stats(Ctx* c) {
   st.ms_parse = st.ms_csr = st.ms_kcore = st.ms_subgraph = st.ms_support = st.ms_peel = st.ms_total = 0;
   st.ms_support_kernel = st.ms_peel_kernel = 0;
   st.support_bytes = st.peel_bytes = st.peel_decrements = 0;
+  st.support_kernel_bytes = st.support_row_words = st.peel_recount_bytes = 0;
   st.core_vertices = st.core_edges = st.predict_vertices = st.predict_edges = 0;
   st.cmax = st.kmax_lower_bound = st.levels = st.rounds = 0;
 }
@@ -244,7 +245,20 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   *count = p2.count;
 }
 
+// Resolves the context's kernel timers when a stage-output call ends.
+struct ResolveTimers {
+  Ctx* c;
+  ~ResolveTimers() {
+    try {
+      c->timer.resolve();
+    } catch (...) {
+    }
+  }
+};
+
 void graph_support(Ctx* c, const Graph& g, uint32_t* dout) {
+  begin_solve_stats(c);
+  ResolveTimers resolve{c};
   Sub s;
   build_sub_all(c, g, s);
   build_bits(c, s);
@@ -258,6 +272,8 @@ void graph_support(Ctx* c, const Graph& g, uint32_t* dout) {
 }
 
 void graph_trussness(Ctx* c, const Graph& g, uint32_t* dout) {
+  begin_solve_stats(c);
+  ResolveTimers resolve{c};
   Sub s;
   build_sub_all(c, g, s);
   build_bits(c, s);

@@ -23,9 +23,11 @@ uint64_t parse_count_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, DBuf& bloc
 void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_off, uint64_t* keys, DevWords* words,
                  uint64_t block0 = 0, uint64_t nblocks = ~0ULL, uint64_t ready = ~0ULL, uint64_t line_base = 0);
 
-// csr.cu -- stage (b): canonical keys (any order, ~0 = none) -> Graph.
-// `keys` is consumed (sorted in place).
-void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g);
+// csr.cu -- stage (b): edge records a << 32 | b (either end first, any
+// order, ~0 = none) -> Graph.  `keys` may be consumed (sorted in place).
+// `lines`: the records are a TSV's lines in file order (y << 32 | x), so the
+// grouped-input route is tried first.
+void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines = false);
 
 DevWords* dev_words(Ctx* c);
 void reset_words(Ctx* c);

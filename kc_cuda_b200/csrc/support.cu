@@ -155,20 +155,24 @@ __global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, cons
 template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
-                                                       uint32_t* __restrict__ sup) {
+                                                       uint32_t* __restrict__ sup,
+                                                       unsigned long long* __restrict__ row_words) {
   extern __shared__ __align__(16) uint32_t dense_smem[];
   uint32_t* su = dense_smem + warp_id() * R.W;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t groups = (m + 31) / 32;
+  unsigned long long wr = 0;  // row words this lane accounts for (one or two lanes per warp)
   for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
     uint32_t e, s;
     bool ok;
     if (kCapped)
-      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok);
+      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr);
     else
-      dense_group(order, g * 32, m, ends, R, nullptr, su, e, s, ok);
+      dense_group(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
     if (ok) sup[e] = s;
   }
+  wr = warp_sum(wr);
+  if (lane_id() == 0 && wr) atomicAdd(row_words, wr);
 }
 
 // Tile keys: (u >> tb) << 16 | (v >> tb), stable-sorted with the edge ids.
@@ -182,14 +186,14 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
 }
 
 template <bool kCapped>
-void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, unsigned long long* row_words) {
   const size_t smem = dense_smem_bytes(s.W, 256);
   KT_CUDA(cudaFuncSetAttribute(k_dense_support<kCapped>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
   k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           dense_rows(s), cap, sup);
+                                                           dense_rows(s), cap, sup, row_words);
   KT_LAUNCHED(c);
 }
 
@@ -322,13 +326,16 @@ bool build_bits(Ctx* c, Sub& s) {
 
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   if (s.m == 0) return;
+  // acc[0]: merge-model list entries, acc[1]: dense row words read.
+  DBuf acc(c, 16);
+  zero(c, acc.get(), 16);
   cudaEvent_t e0;
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
     if (cap)
-      launch_dense_support<true>(c, s, sup, cap);
+      launch_dense_support<true>(c, s, sup, cap, acc.as<unsigned long long>() + 1);
     else
-      launch_dense_support<false>(c, s, sup, 0);
+      launch_dense_support<false>(c, s, sup, 0, acc.as<unsigned long long>() + 1);
   } else if ((int64_t)(s.vbase.get() ? s.max_group : s.n) <= c->opt.support_bitmap_max_n) {
     const uint32_t range = s.vbase.get() ? s.max_group : s.n;
     const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);
@@ -355,16 +362,20 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   }
   c->timer.end(c->stream, e0, &c->stats.ms_support_kernel);
   c->stats.support_launches++;
-  // Algorithmic bytes (outside the timed span).
-  DBuf acc(c, 8);
-  zero(c, acc.get(), 8);
+  // Algorithmic bytes (outside the timed span): the merge model, and the
+  // bytes the kernel that ran moved.
   k_support_alg<<<grid_for(s.m, 256, c->num_sms * 8), 256, 0, c->stream>>>(s.m, s.ends.as<uint64_t>(),
                                                                              s.off.as<uint64_t>(),
                                                                              s.up.as<uint64_t>(),
                                                                              acc.as<unsigned long long>());
   KT_LAUNCHED(c);
-  const uint64_t sum = read_word<uint64_t>(c, acc.as<uint64_t>());
-  c->stats.support_bytes += 4 * sum + 4 * s.m + 8 * ((uint64_t)s.n + 1);
+  uint64_t h[2];
+  copy_d2h(c, h, acc.get(), 16);
+  const uint64_t merge = 4 * h[0] + 4 * s.m + 8 * ((uint64_t)s.n + 1);
+  c->stats.support_bytes += merge;
+  c->stats.support_row_words += h[1];
+  // Dense: row words, plus per edge its list entry (4), ends (8) and result (4).
+  c->stats.support_kernel_bytes += s.W ? 4 * h[1] + 16 * s.m : merge;
 }
 
 }  // namespace kt

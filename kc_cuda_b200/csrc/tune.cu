@@ -188,6 +188,10 @@ kt_status kt_options_load(kt_ctx* h, const char* path) {
     bool known = false;
     for (const kt::Param& p : kt::params())
       if (!std::strcmp(p.name, name)) {
+        if (!kt::option_value_ok(name, v)) {
+          std::fclose(f);
+          throw kt::Error(KT_ERR_INVALID, std::string("options file: value out of range for ") + name);
+        }
         o.*p.field = v;
         known = true;
       }

@@ -50,6 +50,9 @@ class Stats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("peel_decrements", ctypes.c_uint64),
         ("batch_waves", ctypes.c_uint32), ("batch_graphs", ctypes.c_uint32),
+        ("support_kernel_bytes", ctypes.c_uint64), ("support_row_words", ctypes.c_uint64),
+        ("peel_recount_bytes", ctypes.c_uint64),
+        ("csr_grouped", ctypes.c_uint32), ("pad0", ctypes.c_uint32),
     ]
 
     def as_dict(self):

@@ -18,6 +18,7 @@ from kc_cuda_b200 import gen
 
 pytestmark = pytest.mark.gpu
 
+KT_ERR_INVALID = 1
 KT_ERR_LIMIT = 7
 MAX_VERTICES = 1 << 20
 
@@ -64,3 +65,17 @@ def test_kcore_noalloc_matches_kt_kcore():
     st = L.kt_kcore_noalloc(ctypes.c_void_p(d_off.data_ptr()), ctypes.c_void_p(d_adj.data_ptr()), MAX_VERTICES + 1,
                             2, ctypes.c_void_p(d_mem.data_ptr()), stream)
     assert st == KT_ERR_LIMIT
+    # A missing adjacency is refused, not read through.
+    st = L.kt_kcore_noalloc(ctypes.c_void_p(d_off.data_ptr()), None, n, 2, ctypes.c_void_p(d_mem.data_ptr()), stream)
+    assert st == KT_ERR_INVALID
+    # The point of the entry point: calls take no device memory.  With the
+    # solver's context closed, only this test's own buffers are held, so the
+    # device's free memory must not move across repeated calls.
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _call in range(3):
+        st = L.kt_kcore_noalloc(ctypes.c_void_p(d_off.data_ptr()), ctypes.c_void_p(d_adj.data_ptr()), n, 2,
+                                ctypes.c_void_p(d_mem.data_ptr()), stream)
+        assert st == 0, st
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
