@@ -341,30 +341,37 @@ def batch_run(ctx, indices=None, first=0, count=0):
     st = ctx.stats()
     k, c = b.results()
     b.free()
-    return st["ms_total"] - st["ms_parse"], st["batch_waves"], [(int(a), int(e)) for a, e in zip(k, c)]
+    return st["ms_total"], st["batch_waves"], [(int(a), int(e)) for a, e in zip(k, c)]
+
+
+def solve_alone(ctx, index: int):
+    """Mix graph `index` through the one-graph-per-launch path: device time of
+    its generation, CSR build and solve (ms), and its answer."""
+    g = ctx.load_mix_graph(index)
+    st = ctx.stats()
+    ms = st["ms_parse"] + st["ms_csr"]
+    ans = g.kmax_truss()
+    ms += ctx.stats()["ms_total"]
+    g.free()
+    return ms, ans
 
 
 def measure_mix(ctx, args, rank, pg, threads):
     """Batched path vs the one-graph-per-launch path over graphs first..first+G-1
     of the mix (n log-uniform over [1e3, 1e6], R-MAT or Erdos-Renyi, edge factor
-    4..64, one clique of 5..60), generated on the device (generation excluded
-    from both).  Every batched answer is compared with the graph solved alone."""
+    4..64, one clique of 5..60), generated on the device (generation included
+    in both: device time from the first generated draw to the last answer).
+    Every batched answer is compared with the graph solved alone."""
     import numpy as np
     G = args.mix_graphs
     first = ranges_for(args, rank)["mix"][0]
     idx = list(range(first, first + G))
-    # One graph per launch sequence: kt_load_mix_graph (CSR build timed) + kt_solve.
+    # One graph per launch sequence: kt_load_mix_graph + kt_solve.
     for i in idx[: min(3, G)]:
-        g = ctx.load_mix_graph(i)
-        g.kmax_truss()
-        g.free()
+        solve_alone(ctx, i)
     lat, alone = {}, {}
     for i in idx:
-        g = ctx.load_mix_graph(i)
-        csr_ms = ctx.stats()["ms_csr"]
-        alone[i] = g.kmax_truss()
-        lat[i] = csr_ms + ctx.stats()["ms_total"]
-        g.free()
+        lat[i], alone[i] = solve_alone(ctx, i)
     per_graph_ms = max_over_ranks(pg, sum(lat.values()))
     # Batched: a warm-up batch, then the whole mix in one kt_batch_run per step.
     batch_run(ctx, first=first, count=min(G, 64))
@@ -394,6 +401,7 @@ def measure_mix(ctx, args, rank, pg, threads):
     lat_np = np.array([lat[i] for i in idx])
     out = {
         "workload": f"mix graphs {first}..{first + G - 1}", "graphs": G, "steps": args.mix_steps,
+        "lanes": args.batch_lanes,
         "graphs_per_s": total / (batched_ms / 1000.0), "ms_per_step": batched_ms, "waves": waves,
         "per_graph": {"graphs_per_s": total / (per_graph_ms / 1000.0), "ms_total": per_graph_ms, "graphs": G,
                       "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
@@ -454,11 +462,8 @@ def measure_serve(ctx, args, rank, pg, batched_gps=None):
     summ = serving.summarize(submitted, results)
     service, mism = [], []
     for j in range(R):
-        g = ctx.load_mix_graph(first + j)
-        csr_ms = ctx.stats()["ms_csr"]
-        ans = g.kmax_truss()
-        service.append(csr_ms + ctx.stats()["ms_total"])
-        g.free()
+        ms, ans = solve_alone(ctx, first + j)
+        service.append(ms)
         if ans != (results[j]["kmax"], results[j]["edges"]):
             mism.append(first + j)
     pg_lat = fifo_latencies(arrivals, service)
@@ -466,6 +471,7 @@ def measure_serve(ctx, args, rank, pg, batched_gps=None):
     total = sum_over_ranks(pg, float(R))
     return {
         "workload": f"{R} Poisson requests, mix graphs {first}..{first + R - 1}", "requests": R,
+        "lanes": args.serve_lanes,
         "arrival_rate_per_s": rate, "arrival_seed": 55 + rank, "rate_basis_graphs_per_s": batched_gps,
         "calibration": calib, "graphs_per_s": total / span, "span_s": span,
         "p50_ms": summ["p50_ms"], "p99_ms": max_over_ranks(pg, summ["p99_ms"]), "mean_ms": summ["mean_ms"],
@@ -480,6 +486,15 @@ def measure_serve(ctx, args, rank, pg, batched_gps=None):
     }
 
 
+def lane_options(ctx, args):
+    """Options of the batched and serving contexts: a memory pool grown once
+    to the budget (graphs of new sizes then map no memory mid-solve), and the
+    waves in flight at once."""
+    ctx.set_option("pool_reserve_mb", 1 << 30)
+    ctx.set_option("batch_lanes", args.batch_lanes)
+    ctx.set_option("serve_lanes", args.serve_lanes)
+
+
 def line_base(metric, value, unit, world, steps, warmup, ms, config):
     return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": steps, "warmup": warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
@@ -490,7 +505,7 @@ def run_mix(args, world, rank, local, pg):
     """--workload mix4096: the batched figures as the line itself."""
     import kc_cuda_b200 as K
     ctx = K.Context(local)
-    ctx.set_option("pool_reserve_mb", 1 << 30)
+    lane_options(ctx, args)
     tune = autotune(ctx, args, rank)
     ctx.reset_stats()
     with ClockSampler(local) as clk:
@@ -511,7 +526,7 @@ def run_serve(args, world, rank, local, pg):
     """--workload serve: the serving figures as the line itself."""
     import kc_cuda_b200 as K
     ctx = K.Context(local)
-    ctx.set_option("pool_reserve_mb", 1 << 30)
+    lane_options(ctx, args)
     tune = autotune(ctx, args, rank)
     ctx.reset_stats()
     with ClockSampler(local) as clk:
@@ -660,7 +675,7 @@ def run_single(args, world, rank, local, pg, threads):
         staged = None
         ctx.close()
         ctx = K.Context(local)
-        ctx.set_option("pool_reserve_mb", 1 << 30)
+        lane_options(ctx, args)
         mix_tune = autotune(ctx, args, rank)
         if not args.no_batched:
             mix = measure_mix(ctx, args, rank, pg, threads)
@@ -730,6 +745,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=0.0, help="requests/s (0: 0.8 x batched graphs/s)")
     ap.add_argument("--calib-graphs", type=int, default=512)
+    ap.add_argument("--batch-lanes", type=int, default=2, help="batched: waves in flight at once (1 or 2)")
+    ap.add_argument("--serve-lanes", type=int, default=2, help="serving: waves in flight at once (1..4)")
     ap.add_argument("--tune-graphs", type=int, default=128,
                     help="autotune the kernel thresholds on this many other mix graphs first (0: off)")
     args = ap.parse_args()

@@ -90,7 +90,9 @@ const char* kt_status_string(kt_status s);
  *                               (0 = never)
  *   peel_split (16)             peel: a round whose frontier edges x 8-word row
  *                               chunks <= this x warps deals (edge, chunk) units
- *                               to warps instead of edges (0 = off) */
+ *                               to warps instead of edges (0 = off)
+ *   serve_lanes (2)             serving: waves in flight at once, 1..4
+ *   batch_lanes (2)             batch: waves in flight at once, 1..2 */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 
@@ -151,9 +153,13 @@ kt_status kt_batch_add_pairs(kt_batch* b, const uint64_t* xy, uint64_t count, ui
  * (generated on the device at run time from their seeds). */
 kt_status kt_batch_add_mix(kt_batch* b, uint64_t first_index, uint64_t count, uint64_t base_seed);
 kt_status kt_batch_size(const kt_batch* b, uint64_t* graphs, uint64_t* edge_records);
-/* Solves every graph of the batch; kt_get_stats: ms_total = the whole run,
- * ms_parse = the part spent generating / uploading the graphs' edges,
- * batch_waves = waves used. */
+/* Solves every graph of the batch.  Waves run on batch_lanes (option, 1 or 2,
+ * default 2) lanes: the second lane is a context of its own on the same
+ * device (own stream), created on first use and kept with this context; each
+ * lane takes the next wave as soon as it is free.  kt_get_stats: ms_total =
+ * the whole run on the device (generation and upload of the graphs' edges
+ * included), ms_parse and the other stage times = time spent in each stage,
+ * summed over the lanes, batch_waves = waves used. */
 kt_status kt_batch_run(kt_batch* b);
 /* kmax and kmax-truss edge count of every graph, in graph-id order. */
 kt_status kt_batch_results(const kt_batch* b, uint32_t* kmax, uint64_t* edges);
@@ -194,12 +200,16 @@ kt_status kt_options_load(kt_ctx* ctx, const char* path);
 
 /* A continuous-batching serving loop (no counterpart in the reference).
  * Requests are submitted from any thread at any time and queue in arrival
- * order; a worker thread, which owns the context while the server lives,
- * admits queued requests oldest first while their estimated device footprint
- * fits half of the context's free budget (and at most max_wave_graphs of
- * them, 0 = 65535) and solves them as one wave of the batch path; requests
- * that arrive meanwhile join the next wave.  A request's answer is the same
- * alone and in any mix.  Other calls on the context block while a wave runs. */
+ * order.  The server runs serve_lanes (option, 1..4, default 2) lanes: lane 0
+ * works on the context given, each other lane on a context the server creates
+ * on the same device with the same options and budget.  Whenever a lane is
+ * free it admits queued requests oldest first while their estimated device
+ * footprint fits its share of half of the context's free budget (and at most
+ * max_wave_graphs of them, 0 = 65535) and solves them as one wave of the
+ * batch path on its own stream; requests that arrive while waves run start in
+ * the next free lane, so waves overlap on the device.  A request's answer is
+ * the same alone and in any mix.  Other calls on the context block while a
+ * wave of lane 0 runs. */
 typedef struct kt_server kt_server;
 typedef struct kt_request_result {
   kt_status status;      /* KT_OK, or the error of the wave that held it */
@@ -207,8 +217,10 @@ typedef struct kt_request_result {
   uint64_t edges;        /* kmax-truss edge count */
   double ms_wait;        /* submission -> admission into a wave (host clock) */
   double ms_latency;     /* submission -> result available */
-  uint32_t wave;         /* the wave that solved it (0, 1, ...) */
+  uint32_t wave;         /* the wave that solved it (0, 1, ... in order of completion) */
   uint32_t wave_graphs;  /* requests solved in that wave */
+  uint32_t lane;         /* the lane that ran the wave */
+  uint32_t pad0;
 } kt_request_result;
 typedef struct kt_server_stats {
   uint64_t submitted, completed, pending, waves, max_wave_graphs;
@@ -217,7 +229,7 @@ typedef struct kt_server_stats {
 } kt_server_stats;
 kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** out);
 /* Queues a graph given as records x << 32 | y (copied).  KT_ERR_LIMIT if its
- * footprint alone exceeds what a wave may hold. */
+ * footprint alone exceeds what a wave of one lane may hold. */
 kt_status kt_server_submit_pairs(kt_server* s, const uint64_t* xy, uint64_t count, uint64_t* request_id);
 /* Queues graph `index` of the batched mix (generated on the device). */
 kt_status kt_server_submit_mix(kt_server* s, uint64_t index, uint64_t base_seed, uint64_t* request_id);

@@ -25,6 +25,8 @@ bool option_value_ok(const char* name, int64_t value) {
   // timeout_ms = 0 is allowed: every bounded device wait then gives up at
   // once (the error path, for tests); above an hour is refused.
   if (!std::strcmp(name, "timeout_ms")) return value <= 3600000;
+  if (!std::strcmp(name, "serve_lanes")) return value >= 1 && value <= 4;
+  if (!std::strcmp(name, "batch_lanes")) return value >= 1 && value <= 2;
   return true;
 }
 
@@ -342,6 +344,10 @@ kt_status kt_init(int device, uint64_t budget, kt_ctx** out) {
 
 void kt_destroy(kt_ctx* h) {
   if (!h) return;
+  if (h->c.aux) {
+    kt_destroy(h->c.aux);
+    h->c.aux = nullptr;
+  }
   {
     std::lock_guard<std::recursive_mutex> lk(h->c.mu);
     cudaSetDevice(h->c.device);
@@ -393,7 +399,9 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"peel_bitset", &o.peel_bitset},
              {"peel_split", &o.peel_split},
              {"kcore_compact", &o.kcore_compact},
-             {"wave_budget_pct", &o.wave_budget_pct}};
+             {"wave_budget_pct", &o.wave_budget_pct},
+             {"serve_lanes", &o.serve_lanes},
+             {"batch_lanes", &o.batch_lanes}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

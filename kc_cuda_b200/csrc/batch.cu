@@ -19,12 +19,17 @@
 // wave's key buffer, with the host generator's integer conventions
 // (ktgen_core.h), so a device-generated graph equals ktg_make's.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <exception>
+#include <mutex>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
 #include "compact.cuh"
+#include "handles.h"
 #include "ktgen.h"
 #include "ktgen_core.h"
 #include "solve.h"
@@ -63,12 +68,22 @@ __global__ void k_gen_draws(const GenSpec* __restrict__ specs, uint32_t ns, uint
   }
 }
 
-// Host records x << 32 | y -> canonical union keys (self-loops -> ~0).
-__global__ void k_canon_offset(uint64_t* __restrict__ keys, uint64_t n, uint64_t vbase) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = keys[i];
-    const uint64_t x = k >> 32, y = (uint32_t)k;
-    keys[i] = x == y ? ~0ULL : (x < y ? ((x + vbase) << 32) | (y + vbase) : ((y + vbase) << 32) | (x + vbase));
+// Extra keys of a wave (clique edges of generated graphs, records of host
+// graphs; already canonical union keys) from one staging buffer into their
+// graphs' key ranges: graph g's run [src[g], src[g+1]) of the staging buffer
+// goes to keys[dst[g]...].
+__global__ void k_place_extra(const uint64_t* __restrict__ stage, uint64_t total, const uint64_t* __restrict__ src,
+                              const uint64_t* __restrict__ dst, uint32_t ng, uint64_t* __restrict__ keys) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ng;  // last graph with src <= i
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (src[mid] <= i)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    keys[dst[lo] + (i - src[lo])] = stage[i];
   }
 }
 
@@ -224,32 +239,39 @@ static uint64_t wave_keys(Ctx* c, const std::vector<BatchItem*>& items, DBuf& ke
       gen_total += it.draws;
     }
   }
+  DBuf dspecs;
   if (!specs.empty() && gen_total) {
-    DBuf dspecs(c, specs.size() * sizeof(GenSpec));
+    dspecs.alloc(c, specs.size() * sizeof(GenSpec));
     copy_h2d(c, dspecs.get(), specs.data(), specs.size() * sizeof(GenSpec));
     const ktg_rmat_t thr = ktg_rmat_thresholds(570000, 190000, 190000);
     k_gen_draws<<<grid_for(gen_total, 256, c->num_sms * 32), 256, 0, c->stream>>>(
         dspecs.as<GenSpec>(), (uint32_t)specs.size(), gen_total, thr, keys.as<uint64_t>());
     KT_LAUNCHED(c);
-    sync(c);
   }
-  // Clique keys of generated graphs and records of host graphs.
+  // Clique keys of generated graphs and records of host graphs (canonical,
+  // self-loops -> ~0), in union ids, through one staging copy.
+  std::vector<uint64_t> stage_h, src, dst;
   for (uint32_t g = 0; g < G; ++g) {
     const BatchItem& it = *items[g];
     if (it.extra.empty()) continue;
-    uint64_t* dst = keys.as<uint64_t>() + key_off[g] + it.draws;
-    if (it.generated) {
-      std::vector<uint64_t> k(it.extra.size());
-      for (size_t i = 0; i < k.size(); ++i)
-        k[i] = (((it.extra[i] >> 32) + vbase[g]) << 32) | ((uint32_t)it.extra[i] + vbase[g]);
-      copy_h2d(c, dst, k.data(), k.size() * sizeof(uint64_t));
-      sync(c);
-    } else {
-      copy_h2d(c, dst, it.extra.data(), it.extra.size() * sizeof(uint64_t));
-      k_canon_offset<<<grid_for(it.extra.size(), 256, c->num_sms * 16), 256, 0, c->stream>>>(dst, it.extra.size(),
-                                                                                             vbase[g]);
-      KT_LAUNCHED(c);
+    src.push_back(stage_h.size());
+    dst.push_back(key_off[g] + it.draws);
+    const uint64_t vb = vbase[g];
+    for (uint64_t k : it.extra) {
+      const uint64_t x = k >> 32, y = (uint32_t)k;
+      stage_h.push_back(x == y ? ~0ULL : (x < y ? ((x + vb) << 32) | (y + vb) : ((y + vb) << 32) | (x + vb)));
     }
+  }
+  if (!stage_h.empty()) {
+    const uint32_t ng = (uint32_t)src.size();
+    DBuf stage(c, stage_h.size() * sizeof(uint64_t)), dsrc(c, ng * sizeof(uint64_t)), ddst(c, ng * sizeof(uint64_t));
+    copy_h2d(c, stage.get(), stage_h.data(), stage_h.size() * sizeof(uint64_t));
+    copy_h2d(c, dsrc.get(), src.data(), ng * sizeof(uint64_t));
+    copy_h2d(c, ddst.get(), dst.data(), ng * sizeof(uint64_t));
+    k_place_extra<<<grid_for(stage_h.size(), 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        stage.as<uint64_t>(), stage_h.size(), dsrc.as<uint64_t>(), ddst.as<uint64_t>(), ng, keys.as<uint64_t>());
+    KT_LAUNCHED(c);
+    sync(c);  // the host staging vectors go out of scope
   }
   return vbase[G];
 }
@@ -560,23 +582,68 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   }
 }
 
+namespace {
+
+// Adds a lane context's per-run figures into the batch's context.
+void merge_lane_stats(kt_stats& a, const kt_stats& b) {
+  a.ms_parse += b.ms_parse;
+  a.ms_csr += b.ms_csr;
+  a.ms_kcore += b.ms_kcore;
+  a.ms_subgraph += b.ms_subgraph;
+  a.ms_support += b.ms_support;
+  a.ms_peel += b.ms_peel;
+  a.ms_support_kernel += b.ms_support_kernel;
+  a.ms_peel_kernel += b.ms_peel_kernel;
+  a.core_vertices += b.core_vertices;
+  a.core_edges += b.core_edges;
+  a.predict_vertices += b.predict_vertices;
+  a.predict_edges += b.predict_edges;
+  a.levels += b.levels;
+  a.rounds += b.rounds;
+  a.support_bytes += b.support_bytes;
+  a.peel_bytes += b.peel_bytes;
+  a.support_kernel_bytes += b.support_kernel_bytes;
+  a.support_row_words += b.support_row_words;
+  a.peel_recount_bytes += b.peel_recount_bytes;
+  a.support_launches += b.support_launches;
+  a.peel_launches += b.peel_launches;
+  a.peel_decrements += b.peel_decrements;
+}
+
+// The batch driver's second lane: a context of its own on the same device
+// (own stream, device words, timers), created on first use.
+Ctx* aux_lane(Ctx* c) {
+  if (!c->aux) {
+    kt_ctx* h = nullptr;
+    const kt_status st = kt_init(c->device, c->budget, &h);
+    if (st != KT_OK) throw Error(st, "batch: cannot create the second lane's context");
+    c->aux = h;
+    KT_CUDA(cudaSetDevice(c->device));
+  }
+  return &c->aux->c;
+}
+
+}  // namespace
+
 void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
   // Waves: consecutive graphs while the estimated footprint fits
-  // wave_budget_pct (50; measured best on the batched mix: 236 graphs/s vs
-  // 228 at 70 % and 232 at 35 %) of the
-  // free budget (keys, sort buffers, CSR, k-core state ~ 48 B per key and
-  // 40 B per vertex), the union stays below 2^28 vertices and 65536 graphs.
-  // Graphs are taken in ascending size, so a wave's graphs are alike and its
-  // per-graph structures (support bitmaps) are sized for graphs like them.
+  // wave_budget_pct (50; measured best on the batched mix with one lane:
+  // 236 graphs/s vs 228 at 70 % and 232 at 35 %) of the free budget, shared
+  // by the lanes in flight (keys, sort buffers, CSR, k-core state ~ 48 B per
+  // key and 40 B per vertex); the union stays below 2^28 vertices and 65536
+  // graphs.  Graphs are taken in ascending size, so a wave's graphs are alike
+  // and its per-graph structures (support bitmaps) are sized for graphs like
+  // them.
+  const int lanes = (int)std::min<int64_t>(std::max<int64_t>(1, c->opt.batch_lanes), 2);
   const uint64_t budget = (c->budget > c->in_use ? c->budget - c->in_use : 0) / 100 *
-                          (uint64_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.wave_budget_pct), 100);
+                          (uint64_t)std::min<int64_t>(std::max<int64_t>(1, c->opt.wave_budget_pct), 100) / lanes;
   std::vector<size_t> order(items.size());
   std::iota(order.begin(), order.end(), size_t(0));
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
     return items[a].n != items[b].n ? items[a].n < items[b].n : items[a].nkeys < items[b].nkeys;
   });
+  std::vector<std::vector<BatchItem*>> waves;
   size_t i = 0;
-  out.waves = 0;
   while (i < items.size()) {
     std::vector<BatchItem*> wave;
     uint64_t bytes = 0, verts = 0;
@@ -590,22 +657,91 @@ void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
       verts += it.n;
       ++i;
     }
-    const kt_stats before = c->stats;
-    solve_wave(c, wave);
-    if (c->opt.verbose) {
-      const kt_stats& a = c->stats;
+    waves.push_back(std::move(wave));
+  }
+  out.waves = (uint32_t)waves.size();
+
+  auto one = [](Ctx* lc, const std::vector<BatchItem*>& wave, uint32_t no) {
+    const kt_stats before = lc->stats;
+    solve_wave(lc, wave);
+    if (lc->opt.verbose) {
+      const kt_stats& a = lc->stats;
       uint64_t keys = 0, verts_w = 0;
       for (const BatchItem* it : wave) keys += it->nkeys, verts_w += it->n;
-      KT_LOG(c,
+      KT_LOG(lc,
              "kt: wave %u: %zu graphs, %llu keys, %llu vertex ids: input %.2f csr %.2f kcore %.2f subgraph %.2f "
              "support %.2f peel %.2f ms, %u levels, %u rounds\n",
-             out.waves, wave.size(), (unsigned long long)keys, (unsigned long long)verts_w,
-             a.ms_parse - before.ms_parse, a.ms_csr - before.ms_csr, a.ms_kcore - before.ms_kcore,
-             a.ms_subgraph - before.ms_subgraph, a.ms_support - before.ms_support, a.ms_peel - before.ms_peel,
-             a.levels - before.levels, a.rounds - before.rounds);
+             no, wave.size(), (unsigned long long)keys, (unsigned long long)verts_w, a.ms_parse - before.ms_parse,
+             a.ms_csr - before.ms_csr, a.ms_kcore - before.ms_kcore, a.ms_subgraph - before.ms_subgraph,
+             a.ms_support - before.ms_support, a.ms_peel - before.ms_peel, a.levels - before.levels,
+             a.rounds - before.rounds);
     }
-    ++out.waves;
+  };
+  if (lanes == 1 || waves.size() < 2) {
+    for (uint32_t w = 0; w < waves.size(); ++w) one(c, waves[w], w);
+    return;
   }
+
+  // Two lanes: each takes the next wave as soon as it is free, on its own
+  // stream; cooperative launches of the two run one at a time.
+  Ctx* a = aux_lane(c);
+  std::lock_guard<std::recursive_mutex> alk(a->mu);
+  a->opt = c->opt;
+  a->opt.batch_lanes = 1;
+  std::mutex coop;
+  struct Unhook {
+    Ctx* c;
+    Ctx* a;
+    ~Unhook() { c->coop_mu = a->coop_mu = nullptr; }
+  } unhook{c, a};
+  c->coop_mu = a->coop_mu = &coop;
+  begin_solve_stats(a);
+  const uint64_t a_launches = a->launches, a_h2d = a->h2d_bytes, a_d2h = a->d2h_bytes;
+  // The second lane's stream starts after the work already on the first's.
+  KT_CUDA(cudaEventRecord(c->ev[7], c->stream));
+  KT_CUDA(cudaStreamWaitEvent(a->stream, c->ev[7], 0));
+  reset_words(a);
+  std::atomic<size_t> next{0};
+  std::atomic<bool> failed{false};
+  std::exception_ptr err[2];
+  auto lane = [&](Ctx* lc, int li) {
+    try {
+      KT_CUDA(cudaSetDevice(lc->device));
+      for (;;) {
+        const size_t w = next.fetch_add(1);
+        if (w >= waves.size() || failed.load()) break;
+        one(lc, waves[w], (uint32_t)w);
+      }
+    } catch (...) {
+      err[li] = std::current_exception();
+      failed = true;
+    }
+  };
+  std::thread t;
+  try {
+    t = std::thread(lane, a, 1);
+  } catch (...) {
+    lane(c, 0);  // no second thread: one lane does every wave
+  }
+  if (t.joinable()) {
+    lane(c, 0);
+    t.join();
+  }
+  // The first lane's stream continues after the second's work.
+  try {
+    KT_CUDA(cudaEventRecord(a->ev[7], a->stream));
+    KT_CUDA(cudaStreamWaitEvent(c->stream, a->ev[7], 0));
+    a->timer.resolve();
+  } catch (...) {
+    if (!err[0] && !err[1]) throw;
+  }
+  merge_lane_stats(c->stats, a->stats);
+  c->launches += a->launches - a_launches;
+  c->h2d_bytes += a->h2d_bytes - a_h2d;
+  c->d2h_bytes += a->d2h_bytes - a_d2h;
+  c->peak = std::max(c->peak, c->in_use + a->peak);
+  if (err[0]) std::rethrow_exception(err[0]);
+  if (err[1]) std::rethrow_exception(err[1]);
 }
 
 void load_mix_graph(Ctx* c, uint64_t index, uint64_t base_seed, Graph& g) {

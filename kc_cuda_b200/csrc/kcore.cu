@@ -871,10 +871,13 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
       coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
     }
     void* p[] = {&A};
-    KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_probe, dim3(coop_grid), dim3(256), p, 0, c->stream));
-    KT_LAUNCHED(c);
     uint64_t h[2];
-    copy_d2h(c, h, cn + 5, 16);
+    {
+      CoopLock coop(c);
+      KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_probe, dim3(coop_grid), dim3(256), p, 0, c->stream));
+      KT_LAUNCHED(c);
+      copy_d2h(c, h, cn + 5, 16);
+    }
     rounds += h[0];
     removed = h[1];
   } else {
@@ -1054,10 +1057,13 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   if (c->opt.kcore_blocks_per_sm > 0) per_sm = (int)std::min<int64_t>(per_sm, c->opt.kcore_blocks_per_sm);
   const unsigned grid = (unsigned)std::max(1, per_sm) * c->num_sms;
   void* p[] = {&A};
-  KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_core_levels, dim3(grid), dim3(256), p, 0, c->stream));
-  KT_LAUNCHED(c);
   uint64_t h[5];
-  copy_d2h(c, h, cn.as<unsigned long long>() + 14, sizeof(h));
+  {
+    CoopLock coop(c);
+    KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_core_levels, dim3(grid), dim3(256), p, 0, c->stream));
+    KT_LAUNCHED(c);
+    copy_d2h(c, h, cn.as<unsigned long long>() + 14, sizeof(h));
+  }
   rounds += h[0];
   probes += h[1];
   check_words(c, "core decomposition");

@@ -63,6 +63,8 @@ struct Options {
   int64_t kcore_compact = 8;      // max-core search: compact once the core is < 1/this of the graph (0 = never)
   int64_t wave_budget_pct = 50;   // batch: a wave's estimated footprint within this % of the free budget
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
+  int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)
+  int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
 };
 
 // Range check of an option value: every option is a count, size, ratio or
@@ -166,6 +168,22 @@ struct Ctx {
   // Device word block: bounded-wait error flag, barrier state, counters.
   DBuf words;
   EventTimer timer;
+  // Set while this context is a lane of a server whose lanes share the
+  // device: cooperative launches of the lanes then run one at a time.
+  std::mutex* coop_mu = nullptr;
+  // A second context on the same device for the batch driver's second lane
+  // (created on first use, destroyed with this one).
+  kt_ctx* aux = nullptr;
+};
+
+// Held from a cooperative launch until the host has read its result: a
+// cooperative grid takes every SM's resident-block slots, so two of them
+// (from two lanes of a server) are never in flight together.
+struct CoopLock {
+  std::unique_lock<std::mutex> l;
+  explicit CoopLock(Ctx* c) {
+    if (c->coop_mu) l = std::unique_lock<std::mutex>(*c->coop_mu);
+  }
 };
 
 // Graph held on the device: cleaned, symmetric CSR (rows unsorted) plus the

@@ -715,10 +715,13 @@ struct Peeler {
     const auto t_start = std::chrono::steady_clock::now();
     if (coop_grid) {
       void* p[] = {&A};
-      KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, smem, c->stream));
-      KT_LAUNCHED(c);
       uint64_t h[3];
-      copy_d2h(c, h, A.cnt + 3, sizeof(h));
+      {
+        CoopLock coop(c);
+        KT_CUDA(cudaLaunchCooperativeKernel(kernel(), dim3(coop_grid), dim3(kPeelThreads), p, smem, c->stream));
+        KT_LAUNCHED(c);
+        copy_d2h(c, h, A.cnt + 3, sizeof(h));
+      }
       rounds = h[0];
       recounts = h[2];
     } else {

@@ -1,15 +1,20 @@
 // Serving: a continuous-batching request loop over the batch path.
 //
 // Requests (graphs) are submitted from any host thread and queue in arrival
-// order.  One worker thread owns the context: whenever the device is free it
+// order.  The server runs `lanes` workers (option serve_lanes, default 2);
+// each owns a context of its own on the device -- lane 0 the server's
+// context, the others contexts the server creates with the same options --
+// with its own stream, device words and budget.  Whenever a lane is free it
 // admits queued requests, oldest first, while their estimated device
-// footprint fits the context's budget (and up to a graph cap), and solves the
-// admitted set as one wave -- one disjoint union through every stage, each
-// graph on its own peel levels (batch.cu).  Requests that arrive while a wave
-// runs are admitted into the next one, so small requests ride along with
-// large ones and the device never waits for a fixed batch to fill.  The
-// result of a request does not depend on which wave it joined or on its
-// wave-mates: triangles never cross graphs in a union.
+// footprint fits the lane's share of the budget (and up to a graph cap), and
+// solves the admitted set as one wave -- one disjoint union through every
+// stage, each graph on its own peel levels (batch.cu).  So while one wave is
+// on the device, requests that arrive meanwhile start in the next free lane
+// instead of waiting for that wave to end, and the two waves' kernels
+// overlap on the device.  Cooperative launches (which take every SM's
+// resident-block slots) of the lanes run one at a time; everything else
+// overlaps.  The result of a request does not depend on which wave or lane
+// it joined or on its wave-mates: triangles never cross graphs in a union.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -41,9 +46,14 @@ struct Request {
 }  // namespace
 
 struct kt_server {
+  struct Lane {
+    kt_ctx* ctx = nullptr;
+    bool owned = false;  // created by the server (lanes after the first)
+    std::thread worker;
+  };
   kt_ctx* ctx = nullptr;
   uint32_t max_wave = 0;
-  uint64_t budget = 0;  // footprint a wave may hold
+  uint64_t budget = 0;  // footprint one wave may hold (a lane's share)
   std::mutex m;
   std::condition_variable work_cv, done_cv;
   std::deque<Request*> queue;
@@ -51,7 +61,8 @@ struct kt_server {
   uint64_t next_id = 0;
   bool stopping = false;
   kt_server_stats st{};
-  std::thread worker;
+  std::vector<Lane> lanes;
+  std::mutex coop;  // cooperative launches of the lanes, one at a time
 
   // Same estimate as the batch driver's waves: keys, sort buffers, CSR and
   // core state ~ 48 B per edge record and 40 B per vertex id.
@@ -72,8 +83,8 @@ struct kt_server {
     return KT_OK;
   }
 
-  void run() {
-    kt::Ctx* c = &ctx->c;
+  void run(kt_ctx* lane_ctx) {
+    kt::Ctx* c = &lane_ctx->c;
     cudaSetDevice(c->device);
     while (true) {
       std::vector<Request*> wave;
@@ -90,6 +101,8 @@ struct kt_server {
           wave.push_back(r);
           queue.pop_front();
         }
+        // Others still queued: wake another free lane for them.
+        if (!queue.empty()) work_cv.notify_one();
       }
       const Clock::time_point t_admit = Clock::now();
       std::vector<kt::BatchItem*> items;
@@ -137,12 +150,43 @@ struct kt_server {
         r->result.ms_latency = ms_between(r->submitted, r->finished);
         r->result.wave = wave_no;
         r->result.wave_graphs = (uint32_t)wave.size();
+        r->result.lane = (uint32_t)lane_of(lane_ctx);
         r->item.extra.clear();
         r->item.extra.shrink_to_fit();
         st.completed++;
       }
-      st.device_bytes_peak = peak;
+      lane_peak[lane_of(lane_ctx)] = peak;
+      uint64_t tot = 0;
+      for (uint64_t p : lane_peak) tot += p;
+      if (tot > st.device_bytes_peak) st.device_bytes_peak = tot;
       done_cv.notify_all();
+    }
+  }
+
+  std::vector<uint64_t> lane_peak;
+  size_t lane_of(kt_ctx* x) const {
+    for (size_t i = 0; i < lanes.size(); ++i)
+      if (lanes[i].ctx == x) return i;
+    return 0;
+  }
+
+  // Stops and joins the workers, then frees the lanes' own contexts.
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> lk(m);
+      stopping = true;
+    }
+    work_cv.notify_all();
+    for (Lane& l : lanes)
+      if (l.worker.joinable()) l.worker.join();
+    for (Lane& l : lanes) {
+      if (l.owned) {
+        kt_destroy(l.ctx);
+      } else if (l.ctx) {
+        std::lock_guard<std::recursive_mutex> lk(l.ctx->c.mu);
+        l.ctx->c.coop_mu = nullptr;
+      }
+      l.ctx = nullptr;
     }
   }
 };
@@ -156,16 +200,49 @@ kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** ou
   if (!s) return KT_ERR_NOMEM;
   s->ctx = ctx;
   s->max_wave = max_wave_graphs ? std::min<uint32_t>(max_wave_graphs, 65535) : 65535;
+  kt::Options opt;
+  int device = 0;
+  uint64_t ctx_budget = 0;
+  uint32_t nlanes = 1;
   {
     std::lock_guard<std::recursive_mutex> lk(ctx->c.mu);
     const kt::Ctx& c = ctx->c;
-    s->budget = (c.budget > c.in_use ? c.budget - c.in_use : 0) / 2;
+    opt = c.opt;
+    device = c.device;
+    ctx_budget = c.budget;
+    nlanes = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c.opt.serve_lanes), 4);
+    // Half of the free budget for the waves in flight, shared by the lanes.
+    s->budget = (c.budget > c.in_use ? c.budget - c.in_use : 0) / 2 / nlanes;
   }
+  s->lanes.resize(nlanes);
+  s->lane_peak.assign(nlanes, 0);
+  s->lanes[0].ctx = ctx;
+  kt_status st = KT_OK;
+  for (uint32_t i = 1; i < nlanes && st == KT_OK; ++i) {
+    st = kt_init(device, ctx_budget, &s->lanes[i].ctx);
+    if (st == KT_OK) {
+      s->lanes[i].owned = true;
+      s->lanes[i].ctx->c.opt = opt;
+    }
+  }
+  if (st == KT_OK && nlanes > 1)
+    for (auto& l : s->lanes) {
+      std::lock_guard<std::recursive_mutex> lk(l.ctx->c.mu);
+      l.ctx->c.coop_mu = &s->coop;
+    }
   try {
-    s->worker = std::thread([s] { s->run(); });
+    if (st == KT_OK)
+      for (auto& l : s->lanes) {
+        kt_ctx* lc = l.ctx;
+        l.worker = std::thread([s, lc] { s->run(lc); });
+      }
   } catch (...) {
+    st = KT_ERR_NOMEM;
+  }
+  if (st != KT_OK) {
+    s->shutdown();
     delete s;
-    return KT_ERR_NOMEM;
+    return st;
   }
   *out = s;
   return KT_OK;
@@ -217,12 +294,7 @@ kt_status kt_server_get_stats(kt_server* s, kt_server_stats* out) {
 
 void kt_server_destroy(kt_server* s) {
   if (!s) return;
-  {
-    std::lock_guard<std::mutex> lk(s->m);
-    s->stopping = true;
-  }
-  s->work_cv.notify_all();
-  if (s->worker.joinable()) s->worker.join();
+  s->shutdown();
   delete s;
 }
 

@@ -64,6 +64,7 @@ class RequestResult(ctypes.Structure):
         ("status", ctypes.c_int), ("kmax", ctypes.c_uint32), ("edges", ctypes.c_uint64),
         ("ms_wait", ctypes.c_double), ("ms_latency", ctypes.c_double),
         ("wave", ctypes.c_uint32), ("wave_graphs", ctypes.c_uint32),
+        ("lane", ctypes.c_uint32), ("pad0", ctypes.c_uint32),
     ]
 
     def as_dict(self):

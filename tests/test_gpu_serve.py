@@ -99,3 +99,51 @@ def test_oversized_request_is_refused_and_server_keeps_serving():
             tri = np.array([(0 << 32) | 1, (1 << 32) | 2, (0 << 32) | 2], dtype=np.uint64)
             r = srv.wait(srv.submit_pairs(tri))
             assert (r["status"], r["kmax"], r["edges"]) == (0, 3, 3)
+
+
+def test_request_submitted_mid_wave_overtakes_it():
+    """With two lanes, requests submitted while a large wave is on the device
+    start in the other lane at once and finish before that wave ends; every
+    answer equals the graph's alone."""
+    big = gen.Graph(gen.rmat(20, 32, 5, [60]))
+    bigxy = big.edges()
+    small = small_mix_indices(4, max_draws=60_000, start=300)
+    with K.Context(0) as ctx:
+        assert ctx.get_option("serve_lanes") == 2
+        g = ctx.load_pairs(bigxy)
+        want_big = g.kmax_truss()
+        g.free()
+        alone = {}
+        for i in small:
+            g = ctx.load_mix_graph(i)
+            alone[i] = g.kmax_truss()
+            g.free()
+        with ctx.server() as srv:
+            tb = time.perf_counter()
+            rb = srv.submit_pairs(bigxy)
+            time.sleep(0.005)  # the large wave has started
+            sub = []
+            for i in small:
+                sub.append((i, time.perf_counter(), srv.submit_mix(i)))
+            res = [(i, ts, srv.wait(rid)) for i, ts, rid in sub]
+            r_big = srv.wait(rb)
+    assert (r_big["kmax"], r_big["edges"]) == want_big
+    big_end = tb + r_big["ms_latency"] / 1e3
+    for i, ts, r in res:
+        assert (r["kmax"], r["edges"]) == alone[i]
+        assert r["lane"] != r_big["lane"]
+        assert ts + r["ms_wait"] / 1e3 < big_end  # its wave started before the large one ended
+        assert ts + r["ms_latency"] / 1e3 < big_end  # and ended first
+
+
+def test_one_lane_keeps_waves_in_order():
+    idx = small_mix_indices(6, max_draws=200_000, start=500)
+    with K.Context(0) as ctx:
+        ctx.set_option("serve_lanes", 1)
+        with ctx.server(max_wave_graphs=2) as srv:
+            rs = [srv.wait(srv.submit_mix(i)) for i in idx]
+        assert {r["lane"] for r in rs} == {0}
+        for i, r in zip(idx, rs):
+            g = ctx.load_mix_graph(i)
+            assert (r["kmax"], r["edges"]) == g.kmax_truss()
+            g.free()
