@@ -295,7 +295,6 @@ static void union_sub(Ctx* c, const Graph& U, const uint32_t* dcore, const uint3
     KT_LAUNCHED(c);
   }
   build_sub_grouped(c, U, list.as<uint32_t>(), na, deg.as<uint32_t>(), rem.as<uint32_t>(), dgid, G, s);
-  build_bits(c, s);
 }
 
 // Edges of graph thr's group with support >= thr[group] (thr 0: none).
@@ -377,7 +376,6 @@ static bool survivors(Ctx* c, const Sub& s, const uint32_t* sup, const std::vect
   if (only_if_few && k * 2 >= s.m) return false;
   build_sub_grouped_from_keys(c, keys.as<uint64_t>(), k, s.n, s.vgid.as<uint32_t>(), G, out);
   keys.release();
-  build_bits(c, out);
   out_sup = DBuf(c, (out.m ? out.m : 1) * sizeof(uint32_t));
   edge_support(c, out, out_sup.as<uint32_t>());
   return true;

@@ -850,7 +850,6 @@ void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub
   Graph g;
   build_graph(c, keys, m, n_ids, g);
   build_sub_all(c, g, out);
-  build_bits(c, out);
 }
 
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,

@@ -149,7 +149,6 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     build_sub(c, g, kc, s);
     st.core_vertices = s.n;
     st.core_edges = s.m;
-    build_bits(c, s);
     st.ms_subgraph += tm.stop();
     tm.start();
     DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
@@ -174,7 +173,6 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     build_sub(c, g, kc, s1);
     st.predict_vertices = s1.n;
     st.predict_edges = s1.m;
-    build_bits(c, s1);
     st.ms_subgraph += tm.stop();
     tm.start();
     DBuf sup1(c, (s1.m ? s1.m : 1) * sizeof(uint32_t));
@@ -203,7 +201,6 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   build_sub(c, g, kc, s2);
   st.core_vertices = s2.n;
   st.core_edges = s2.m;
-  build_bits(c, s2);
   st.ms_subgraph += tm.stop();
   tm.start();
   DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
@@ -261,7 +258,6 @@ void graph_support(Ctx* c, const Graph& g, uint32_t* dout) {
   ResolveTimers resolve{c};
   Sub s;
   build_sub_all(c, g, s);
-  build_bits(c, s);
   DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
   edge_support(c, s, sup.as<uint32_t>());
   if (s.m) {
@@ -276,7 +272,6 @@ void graph_trussness(Ctx* c, const Graph& g, uint32_t* dout) {
   ResolveTimers resolve{c};
   Sub s;
   build_sub_all(c, g, s);
-  build_bits(c, s);
   DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
   DBuf tr(c, (s.m ? s.m : 1) * sizeof(uint32_t));
   edge_support(c, s, sup.as<uint32_t>());

@@ -79,6 +79,7 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap = 0);
 // each of its edges has support >= t-2).  0 when no t >= 3 qualifies.
 uint32_t support_bound(Ctx* c, const uint32_t* sup, uint64_t m, uint32_t cap);
 // Builds s.bits when the subgraph qualifies for dense mode; returns whether.
+// Every build_sub* call runs it (before the lower entries' edge ids).
 bool build_bits(Ctx* c, Sub& s);
 
 // peel.cu

@@ -2,14 +2,19 @@
 reference's own CPU solver (run by hand on the GPU host; too large for the
 test suite):
 
-    python tests/large_parity.py [--configs 2 3] [--dir /dev/shm] [--record] [--ours-only]
+    python tests/large_parity.py [--configs 1 2 3] [--dir /dev/shm] [--record] [--ours-only]
+                                 [--gpu-reference]
 
 For each configuration: the seeded graph is generated and written as the
 reference's TSV; the drop-in CLI (kc_cuda_b200/kt_solve -f) and kc_cpu (all
 host cores; kc_cpu_large, the build with raised input limits, when the input
 is beyond kc_cpu's own) solve the same file; the answers must be equal.
---record writes the answers and wall times to tests/golden/large_configs.json,
-which the bench checks its answer against.
+--gpu-reference also runs the reference's own GPU build (oracle/_ref/kc_gpu,
+built for sm_100a from the reference sources) on the same file, once, and
+records its wall time and answer beside the others.
+--record writes the answers and wall times to tests/golden/large_configs.json;
+bench.py compares its answer on a workload with the kc_cpu answer recorded
+there.
 """
 from __future__ import annotations
 
@@ -48,6 +53,26 @@ def run_cli(path: str):
     return (int(m.group(1)), int(m.group(2))), wall
 
 
+def run_kc_gpu(path: str, timeout: float):
+    """The reference's GPU solver on a TSV file (a stand-in vmtouch first on
+    PATH, as for kc_cpu): (answer or None, wall seconds, status text)."""
+    binary = os.path.join(O.REF, "kc_gpu")
+    if not os.access(binary, os.X_OK):
+        return None, None, "oracle/_ref/kc_gpu missing"
+    env = dict(os.environ)
+    env["PATH"] = O.HERE + os.pathsep + env.get("PATH", "")
+    t = time.perf_counter()
+    try:
+        p = subprocess.run([binary, "-f", path], capture_output=True, text=True, timeout=timeout, env=env)
+    except subprocess.TimeoutExpired:
+        return None, time.perf_counter() - t, f"no answer within {timeout:.0f} s"
+    wall = time.perf_counter() - t
+    m = RESULT_RE.search(p.stdout)
+    if p.returncode != 0 or not m:
+        return None, wall, f"exit {p.returncode}: {(p.stderr or p.stdout)[-300:]}"
+    return (int(m.group(1)), int(m.group(2))), wall, "ok"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--configs", type=int, nargs="+", default=[2, 3])
@@ -57,6 +82,8 @@ def main():
     ap.add_argument("--reference-only", action="store_true", help="no GPU: record kc_cpu's answers only")
     ap.add_argument("--ours-only", action="store_true",
                     help="compare with the recorded kc_cpu answer instead of running kc_cpu again")
+    ap.add_argument("--gpu-reference", action="store_true", help="also run the reference's kc_gpu once")
+    ap.add_argument("--gpu-reference-timeout", type=float, default=1200)
     a = ap.parse_args()
     rec = json.load(open(RECORD)) if os.path.exists(RECORD) else {}
     ok = True
@@ -85,6 +112,11 @@ def main():
             ref = O.run_kc_cpu(path, threads=a.threads, timeout=7200, binary=binary)
             wall_ref = time.perf_counter() - t
             a_threads = a.threads
+        gpu_ref = None
+        if a.gpu_reference:
+            ans, wall_g, status = run_kc_gpu(path, a.gpu_reference_timeout)
+            gpu_ref = {"answer": list(ans) if ans else None, "wall_s": round(wall_g, 2) if wall_g else None,
+                       "status": status, "equal": (tuple(ans) == tuple(ref)) if ans else None}
         os.unlink(path)
         if ours is None and prev.get("ours"):
             ours, wall_ours = tuple(prev["ours"]), prev.get("ours_cli_wall_s")
@@ -96,6 +128,10 @@ def main():
                  "reference_wall_s": round(wall_ref, 2),
                  "ours_cli_wall_s": round(wall_ours, 2) if wall_ours else None,
                  "generate_s": round(t_gen, 1)}
+        if gpu_ref is not None:
+            entry["reference_gpu"] = gpu_ref
+        elif "reference_gpu" in prev:
+            entry["reference_gpu"] = prev["reference_gpu"]
         print(json.dumps(entry), flush=True)
         rec[name] = entry
     if a.record:
