@@ -31,10 +31,12 @@ from kc_cuda_b200 import gen
 from kc_cuda_b200.solver import Context
 
 
-def dense_support(reps: int, n: int = 40000, draws: int = 48_000_000) -> None:
+def dense_support(reps: int, n: int = 40000, draws: int = 48_000_000, options=()) -> None:
     spec = gen.GraphSpec(kind=gen.KTG_ER, n=n, draws=draws, seed=7)
     g = gen.Graph(spec)
     with Context(0) as ctx:
+        for name, v in options:
+            ctx.set_option(name, v)
         dg = ctx.load_pairs(g.edges())
         for _ in range(reps):
             t = time.perf_counter()
@@ -83,11 +85,14 @@ def main() -> None:
     ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve", "mix-batch"])
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="support cases: a solver option to set first (repeatable)")
     a = ap.parse_args()
+    opts = [(o.split("=")[0], int(o.split("=")[1])) for o in a.option]
     if a.case == "dense-support":
-        dense_support(a.reps)
+        dense_support(a.reps, options=opts)
     elif a.case == "core55k-support":
-        dense_support(a.reps, n=55455, draws=95_000_000)
+        dense_support(a.reps, n=55455, draws=95_000_000, options=opts)
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
     elif a.case == "mix-batch":

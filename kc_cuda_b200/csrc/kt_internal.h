@@ -227,6 +227,12 @@ void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits
 // Sorted-unique compaction of keys (drops key == ~0).  Returns new count.
 uint64_t unique_sorted_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n);
 
+// Lets `func` launch with up to the device's opt-in shared memory per block
+// (less its static shared memory), once per device and function.  Setting the
+// largest limit once, instead of each launch's own size, keeps launches from
+// two lanes (threads) of one device from lowering each other's limit.
+void allow_max_dynamic_smem(const void* func);
+
 // Grid sizing.
 inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap) {
   uint64_t g = (work + block - 1) / block;

@@ -661,7 +661,7 @@ struct Peeler {
     smem = dense_smem_bytes(s->W, kPeelThreads);
     coop_grid = 0;
     if (c->opt.persistent || s->W) {
-      KT_CUDA(cudaFuncSetAttribute(k_cascade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_max_dynamic_smem((const void*)k_cascade);
       int per_sm = 0;
       KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade, kPeelThreads, smem));
       coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;

@@ -2,6 +2,9 @@
 // and the CUDA error -> kt::Error conversion.
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "kt_internal.h"
 
@@ -45,6 +48,22 @@ void DBuf::release() {
   ptr_ = nullptr;
   bytes_ = 0;
   ctx_ = nullptr;
+}
+
+void allow_max_dynamic_smem(const void* func) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  KT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, func})) return;
+  int optin = 0;
+  KT_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  KT_CUDA(cudaFuncGetAttributes(&fa, func));
+  KT_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               optin - (int)fa.sharedSizeBytes));
+  done.insert({dev, func});
 }
 
 void sync(Ctx* c) { KT_CUDA(cudaStreamSynchronize(c->stream)); }

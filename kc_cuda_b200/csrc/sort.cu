@@ -146,12 +146,8 @@ void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits
   copy_d2h(c, h.data(), hist.get(), h.size() * sizeof(unsigned long long));
 
   const uint32_t ntiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
-  static bool attr_set = false;
-  if (!attr_set) {
-    KT_CUDA(cudaFuncSetAttribute(k_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortTile * 12));
-    KT_CUDA(cudaFuncSetAttribute(k_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortTile * 8));
-    attr_set = true;
-  }
+  allow_max_dynamic_smem((const void*)k_scatter<true>);
+  allow_max_dynamic_smem((const void*)k_scatter<false>);
   DBuf keys_alt(c, n * sizeof(uint64_t));
   DBuf vals_alt;
   if (vals) vals_alt.alloc(c, n * sizeof(uint32_t));

@@ -325,7 +325,7 @@ void build_from_list(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t na,
     newid.release();
     const size_t smem = (size_t)((max_range + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
-      KT_CUDA(cudaFuncSetAttribute(k_rows_bitmap_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_max_dynamic_smem((const void*)k_rows_bitmap_sort);
     k_rows_bitmap_sort<<<(unsigned)std::min<uint64_t>(na, (uint64_t)c->num_sms * 32), 256, smem, c->stream>>>(
         na, s.off.as<uint64_t>(), s.adj.as<uint32_t>(), group_of ? s.vbase.as<uint32_t>() : nullptr,
         group_of ? s.vgid.as<uint32_t>() : nullptr, group_of ? gsize.as<uint32_t>() : nullptr, (uint32_t)na);

@@ -156,13 +156,20 @@ template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
                                                        uint32_t* __restrict__ sup,
-                                                       unsigned long long* __restrict__ row_words) {
+                                                       unsigned long long* __restrict__ row_words,
+                                                       unsigned long long* __restrict__ cursor) {
   extern __shared__ __align__(16) uint32_t dense_smem[];
   uint32_t* su = dense_smem + warp_id() * R.W;
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t groups = (m + 31) / 32;
   unsigned long long wr = 0;  // row words this lane accounts for (one or two lanes per warp)
-  for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); g < groups; g += warps) {
+  // Warps take the next 32-edge group from a cursor, so the groups in flight
+  // stay a narrow window of the tile-ordered list (a grid-stride loop lets
+  // warps drift apart, and the rows they read then no longer fit in L2).
+  for (;;) {
+    unsigned long long g = 0;
+    if (lane_id() == 0) g = atomicAdd(cursor, 1ULL);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= groups) break;
     uint32_t e, s;
     bool ok;
     if (kCapped)
@@ -186,14 +193,15 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
 }
 
 template <bool kCapped>
-void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, unsigned long long* row_words) {
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, unsigned long long* row_words,
+                          unsigned long long* cursor) {
   const size_t smem = dense_smem_bytes(s.W, 256);
-  KT_CUDA(cudaFuncSetAttribute(k_dense_support<kCapped>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_max_dynamic_smem((const void*)k_dense_support<kCapped>);
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
   k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           dense_rows(s), cap, sup, row_words);
+                                                           dense_rows(s), cap, sup, row_words, cursor);
   KT_LAUNCHED(c);
 }
 
@@ -326,21 +334,23 @@ bool build_bits(Ctx* c, Sub& s) {
 
 void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   if (s.m == 0) return;
-  // acc[0]: merge-model list entries, acc[1]: dense row words read.
-  DBuf acc(c, 16);
-  zero(c, acc.get(), 16);
+  // acc[0]: merge-model list entries, acc[1]: dense row words read, acc[2]:
+  // the dense kernel's group cursor.
+  DBuf acc(c, 24);
+  zero(c, acc.get(), 24);
   cudaEvent_t e0;
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
+    unsigned long long* a = acc.as<unsigned long long>();
     if (cap)
-      launch_dense_support<true>(c, s, sup, cap, acc.as<unsigned long long>() + 1);
+      launch_dense_support<true>(c, s, sup, cap, a + 1, a + 2);
     else
-      launch_dense_support<false>(c, s, sup, 0, acc.as<unsigned long long>() + 1);
+      launch_dense_support<false>(c, s, sup, 0, a + 1, a + 2);
   } else if ((int64_t)(s.vbase.get() ? s.max_group : s.n) <= c->opt.support_bitmap_max_n) {
     const uint32_t range = s.vbase.get() ? s.max_group : s.n;
     const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);
     if (smem > 48 * 1024)
-      KT_CUDA(cudaFuncSetAttribute(k_support_bitmap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      allow_max_dynamic_smem((const void*)k_support_bitmap);
     // Large bitmaps leave room for few blocks per SM: then wider blocks.
     const unsigned threads = smem > 24 * 1024 ? kSupThreadsWide : kSupThreads;
     int per_sm = 0;

@@ -122,8 +122,8 @@ def test_empty_and_trivial_graphs_in_batch(ctx):
 def test_batch_lanes_same_answers_as_one_lane():
     """Waves in flight on two lanes (two contexts' streams) give the answers of
     one lane, wave for wave; a small budget forces many waves."""
-    idx = small_mix_indices(40, max_draws=800_000)
-    with K.Context(0, hbm_budget=1 << 30) as c:
+    idx = small_mix_indices(40, max_draws=400_000)
+    with K.Context(0, hbm_budget=256 << 20) as c:
         got = {}
         for lanes in (1, 2):
             c.set_option("batch_lanes", lanes)
@@ -132,7 +132,7 @@ def test_batch_lanes_same_answers_as_one_lane():
                 b.add_mix(i, 1)
             b.run()
             st = c.stats()
-            assert st["batch_waves"] >= 4
+            assert st["batch_waves"] >= 2
             got[lanes] = b.results()
             b.free()
         assert np.array_equal(got[1][0], got[2][0]) and np.array_equal(got[1][1], got[2][1])
