@@ -18,6 +18,8 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
                   cliques 80/120/200; 15.5 GB of TSV staged on the device).
   mix-batch       graphs 0..255 of the batched mix in one kt_batch_run
                   (k_core_levels on the union, grouped support and peel).
+  mix-largest     the --count largest of mix graphs 0..4095 (by draws) in one
+                  kt_batch_run; --alone also solves them one at a time.
 --verbose prints the solver's stage decisions and per-level cascades.
 """
 from __future__ import annotations
@@ -65,24 +67,58 @@ def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
         t.free()
 
 
-def mix_batch(reps: int, verbose: bool = False) -> None:
+def mix_batch(reps: int, verbose: bool = False, indices=None, options=(), alone: bool = False) -> None:
+    indices = list(range(256)) if indices is None else indices
     with Context(0) as ctx:
+        ctx.set_option("pool_reserve_mb", 1 << 30)
+        for name, v in options:
+            ctx.set_option(name, v)
         if verbose:
             ctx.set_option("verbose", 1)
         for _ in range(reps):
             b = ctx.batch()
-            b.add_mix(0, 256)
+            for i in indices:
+                b.add_mix(i, 1)
             b.run()
             st = ctx.stats()
             k, _ = b.results()
             b.free()
-            print(f"256 mix graphs, kmax sum {int(k.sum())}, {st['ms_total'] - st['ms_parse']:.1f} ms device "
-                  f"({st['batch_waves']} waves)", flush=True)
+            stages = " ".join(f"{x[3:]} {st[x]:.1f}" for x in
+                              ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel"))
+            print(f"{len(indices)} mix graphs, kmax sum {int(k.sum())}, {st['ms_total']:.1f} ms device "
+                  f"({st['batch_waves']} waves; stage sums: {stages}; support kernel {st['ms_support_kernel']:.1f}, "
+                  f"peel kernel {st['ms_peel_kernel']:.1f}, {st['levels']} levels, {st['rounds']} rounds)", flush=True)
+        if alone:
+            if verbose:
+                ctx.set_option("verbose", 0)
+            tot = {x: 0.0 for x in ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel",
+                                    "ms_total", "ms_support_kernel", "ms_peel_kernel")}
+            for i in indices:
+                g = ctx.load_mix_graph(i)
+                st = ctx.stats()
+                tot["ms_parse"] += st["ms_parse"]
+                tot["ms_csr"] += st["ms_csr"]
+                g.kmax_truss()
+                st = ctx.stats()
+                for x in ("ms_kcore", "ms_subgraph", "ms_support", "ms_peel", "ms_total", "ms_support_kernel",
+                          "ms_peel_kernel"):
+                    tot[x] += st[x]
+                g.free()
+            print("one at a time: " + " ".join(f"{x[3:]} {v:.1f}" for x, v in tot.items()), flush=True)
+
+
+def largest_mix(count: int, among: int = 4096):
+    """The `count` mix graphs with the most draws among graphs 0..among-1."""
+    sizes = sorted(((gen.mix_graph(i).draws, i) for i in range(among)), reverse=True)
+    return sorted(i for _, i in sizes[:count])
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve", "mix-batch"])
+    ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve",
+                                     "mix-batch", "mix-largest"])
+    ap.add_argument("--count", type=int, default=64, help="mix-largest: how many of the largest graphs")
+    ap.add_argument("--alone", action="store_true", help="mix cases: also solve the graphs one at a time")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
@@ -96,7 +132,9 @@ def main() -> None:
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
     elif a.case == "mix-batch":
-        mix_batch(a.reps, a.verbose)
+        mix_batch(a.reps, a.verbose, options=opts, alone=a.alone)
+    elif a.case == "mix-largest":
+        mix_batch(a.reps, a.verbose, indices=largest_mix(a.count), options=opts, alone=a.alone)
     elif a.case == "rmat24-solve":
         solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
     else:

@@ -558,12 +558,22 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   st.ms_subgraph += tm.stop();
   tm.start();
   DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
-  edge_support(c, s2, sup2.as<uint32_t>());
   std::vector<uint32_t> thr(G, 0);
   for (uint32_t g = 0; g < G; ++g) thr[g] = need[g] ? t0[g] - 2 : 0;
+  // As in the single-graph search phase: each graph's peel starts at t0[g]
+  // with no jump, so supports below t0[g] - 2 only need to be known as
+  // "below" (the capped dense kernel, per-graph caps).
+  const bool capped = c->opt.capped_support && s2.W;
+  DBuf dthr;
+  if (capped) {
+    dthr.alloc(c, G * sizeof(uint32_t));
+    copy_h2d(c, dthr.get(), thr.data(), G * sizeof(uint32_t));
+  }
+  edge_support(c, s2, sup2.as<uint32_t>(), 0, capped ? dthr.as<uint32_t>() : nullptr);
   Sub s3;
   DBuf sup3;
   const bool rebuilt = survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
+  if (!rebuilt && capped) edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
   st.ms_support += tm.stop();
   tm.start();
   std::vector<uint32_t> km;

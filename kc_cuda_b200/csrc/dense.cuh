@@ -189,14 +189,17 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 }
 
 
-// As dense_group, but an edge whose count can no longer reach `thr` is
-// abandoned: the rows are ANDed in four segments, and after each one the
+// As dense_group, but an edge whose count can no longer reach its threshold
+// is abandoned: the rows are ANDed in four segments, and after each one the
 // count so far plus the set bits left in row u bounds the result.  An
-// abandoned edge reports a count below thr (not its support).
+// abandoned edge reports a count below the threshold (not its support).  The
+// threshold is `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends, const DenseRows& R,
                                                    uint32_t thr, uint32_t* su, uint32_t& my_e, uint32_t& my_s,
-                                                   bool& my_ok, unsigned long long* wr = nullptr) {
+                                                   bool& my_ok, unsigned long long* wr = nullptr,
+                                                   const uint32_t* __restrict__ gthr = nullptr,
+                                                   const uint32_t* __restrict__ vgid = nullptr) {
   const unsigned l = lane_id();
   const uint64_t idx = base + l;
   uint32_t e = 0, u = 0, v = 0;
@@ -208,6 +211,7 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     v = (uint32_t)k;
     ok = true;
   }
+  const uint32_t my_thr = (gthr && ok) ? gthr[vgid[u]] : thr;
   my_e = e;
   my_ok = ok;
   my_s = 0;
@@ -253,19 +257,21 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       }
     }
     const bool upper = l >= 16;
+    const uint32_t tj = __shfl_sync(kFull, my_thr, j), tj2 = __shfl_sync(kFull, my_thr, j2 >= 0 ? j2 : j);
+    const uint32_t t = upper ? tj2 : tj;
     bool go = !upper || j2 >= 0;
     const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
     uint32_t wds = go ? c1 : 0u;  // row-v words this half reads
     uint32_t found = half_and_popc(pv, su, 0, c1, go);
-    go = go && found + s1 + s2 + s3 >= thr;
+    go = go && found + s1 + s2 + s3 >= t;
     if (__any_sync(kFull, go)) {
       wds += go ? c2 - c1 : 0u;
       found += half_and_popc(pv, su, c1, c2, go);
-      go = go && found + s2 + s3 >= thr;
+      go = go && found + s2 + s3 >= t;
       if (__any_sync(kFull, go)) {
         wds += go ? c3 - c2 : 0u;
         found += half_and_popc(pv, su, c2, c3, go);
-        go = go && found + s3 >= thr;
+        go = go && found + s3 >= t;
         if (__any_sync(kFull, go)) {
           wds += go ? W - c3 : 0u;
           found += half_and_popc(pv, su, c3, W, go);
@@ -278,15 +284,16 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     if (wr && (l & 15u) == 0) *wr += wds;
 #else
     const uint32_t* pv = R.bits + R.off(vj);
+    const uint32_t t = __shfl_sync(kFull, my_thr, j);
     uint32_t wds = c1;
     uint32_t found = dense_and_popc(pv, su, 0, c1);
-    if (found + s1 + s2 + s3 >= thr) {
+    if (found + s1 + s2 + s3 >= t) {
       wds = c2;
       found += dense_and_popc(pv, su, c1, c2);
-      if (found + s2 + s3 >= thr) {
+      if (found + s2 + s3 >= t) {
         wds = c3;
         found += dense_and_popc(pv, su, c2, c3);
-        if (found + s3 >= thr) {
+        if (found + s3 >= t) {
           wds = W;
           found += dense_and_popc(pv, su, c3, W);
         }

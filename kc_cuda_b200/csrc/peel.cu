@@ -387,11 +387,18 @@ __device__ __forceinline__ void clear_deleted(const PeelArgs& A, uint32_t lo, ui
 // graph without this round's frontier; those below the threshold form the
 // next frontier.  Replaces per-triangle decrements when the frontier is a
 // large part of the graph.
+// Warps take the next 32-entry group of the alive list from `cursor` (zero
+// at the start of the round), so the groups in flight stay a narrow window
+// of the tile-ordered list and the rows they read stay in L2.
 __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uint32_t* next,
-                                              unsigned long long* ncnt, uint64_t gwarp, uint64_t gwarps,
+                                              unsigned long long* ncnt, unsigned long long* cursor,
                                               uint64_t& trec, uint32_t* su) {
   const uint64_t groups = (A.na + 31) / 32;
-  for (uint64_t g = gwarp; g < groups; g += gwarps) {
+  for (;;) {
+    unsigned long long g = 0;
+    if (lane_id() == 0) g = atomicAdd(cursor, 1ULL);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= groups) break;
     uint32_t e, sc;
     bool ok;
     dense_group(A.alive, g * 32, A.na, A.ends, A.R, A.state, su, e, sc, ok);
@@ -442,6 +449,10 @@ __global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(Pe
     pending += nf;
     if (recount) {
       ++nrec;
+      // Group cursors: this recount uses slot 6 + (nrec & 1); the other slot,
+      // last used by the previous recount (finished before the barrier that
+      // ended its round), is cleared for the next one.
+      if (gtid == 0) A.cnt[6 + ((nrec + 1) & 1)] = 0;
       if (pending > alive - nf) {
         zero_bits(A, gtid, gthreads);
         if (!grid_barrier(A.words, A.timeout_ns)) {
@@ -458,7 +469,7 @@ __global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(Pe
         ok = false;
         break;
       }
-      recount_round(A, r, nx, nc, gwarp, gwarps, trec, su);
+      recount_round(A, r, nx, nc, &A.cnt[6 + (nrec & 1)], trec, su);
     } else {
       // Few frontier edges for the grid: deal (edge, chunk) units instead.
       const uint64_t chunks = A.R.sbits ? (A.R.W + kSplitWords - 1) / kSplitWords : 1;

@@ -71,8 +71,9 @@ struct GraphTrack {
 // support.cu: sup[e] = triangles through edge e (all edges of s).  Uses the
 // bitsets when they are built.  cap > 0 (dense mode only): an edge whose
 // support is below cap may get any value below cap -- enough for a peel whose
-// first level removes everything below cap.
-void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap = 0);
+// first level removes everything below cap.  gcap (device, per graph of a
+// grouped union; dense mode only): the same with graph g's cap gcap[g].
+void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap = 0, const uint32_t* gcap = nullptr);
 // Upper bound on the largest non-empty truss level, from exact supports: the
 // largest t <= cap with at least t(t-1)/2 edges of support >= t-2 (a
 // non-empty t-truss has t or more vertices, each of degree >= t-1 in it, and

@@ -155,6 +155,8 @@ __global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, cons
 template <bool kCapped>
 __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
+                                                       const uint32_t* __restrict__ gcap,
+                                                       const uint32_t* __restrict__ vgid,
                                                        uint32_t* __restrict__ sup,
                                                        unsigned long long* __restrict__ row_words,
                                                        unsigned long long* __restrict__ cursor) {
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_
     uint32_t e, s;
     bool ok;
     if (kCapped)
-      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr);
+      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr, gcap, vgid);
     else
       dense_group(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
     if (ok) sup[e] = s;
@@ -193,15 +195,17 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
 }
 
 template <bool kCapped>
-void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, unsigned long long* row_words,
-                          unsigned long long* cursor) {
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
+                          unsigned long long* row_words, unsigned long long* cursor) {
   const size_t smem = dense_smem_bytes(s.W, 256);
   allow_max_dynamic_smem((const void*)k_dense_support<kCapped>);
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
   k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           dense_rows(s), cap, sup, row_words, cursor);
+                                                           dense_rows(s), cap, gcap,
+                                                           gcap ? s.vgid.as<uint32_t>() : nullptr, sup, row_words,
+                                                           cursor);
   KT_LAUNCHED(c);
 }
 
@@ -332,7 +336,7 @@ bool build_bits(Ctx* c, Sub& s) {
   return true;
 }
 
-void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
+void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap) {
   if (s.m == 0) return;
   // acc[0]: merge-model list entries, acc[1]: dense row words read, acc[2]:
   // the dense kernel's group cursor.
@@ -342,10 +346,10 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap) {
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
     unsigned long long* a = acc.as<unsigned long long>();
-    if (cap)
-      launch_dense_support<true>(c, s, sup, cap, a + 1, a + 2);
+    if (cap || (gcap && s.vgid.get()))
+      launch_dense_support<true>(c, s, sup, cap, s.vgid.get() ? gcap : nullptr, a + 1, a + 2);
     else
-      launch_dense_support<false>(c, s, sup, 0, a + 1, a + 2);
+      launch_dense_support<false>(c, s, sup, 0, nullptr, a + 1, a + 2);
   } else if ((int64_t)(s.vbase.get() ? s.max_group : s.n) <= c->opt.support_bitmap_max_n) {
     const uint32_t range = s.vbase.get() ? s.max_group : s.n;
     const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);
