@@ -714,7 +714,7 @@ def run_single(args, world, rank, local, pg, threads):
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, desc, _ = cpu_baseline_run(1, 0, threads)
+        v, desc, _ = cpu_baseline_run(3, 1, threads)
         if v is not None:
             cpu = {"value": v, "unit": "edges/s", "cores": threads, "kind": "reference", "sample": desc}
     if rank == 0:

@@ -134,6 +134,21 @@ __global__ void k_group_counts(const uint32_t* __restrict__ core, const uint32_t
   }
 }
 
+// Per graph: vertices with core >= need[g] (need 0: none counted).
+__global__ void k_group_at_least(const uint32_t* __restrict__ core, const uint32_t* __restrict__ gid, uint64_t n,
+                                 const uint32_t* __restrict__ need, unsigned long long* __restrict__ cnt) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < ((n + 31) & ~31ULL);
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const bool ok = v < n;
+    const uint32_t g = ok ? gid[v] : 0xffffffffu;
+    const uint32_t k = ok ? need[g] : 0u;
+    const bool in = ok && k && core[v] >= k;
+    const unsigned peers = __match_any_sync(kFull, g);
+    const unsigned a = __popc(__ballot_sync(kFull, in) & peers);
+    if (ok && a && lane_id() == (unsigned)(__ffs(peers) - 1)) atomicAdd(&cnt[g], (unsigned long long)a);
+  }
+}
+
 // Vertices of graph g with core >= need[g] (need 0 = graph not taken).
 struct CoreAtLeast {
   const uint32_t* core;
@@ -472,17 +487,35 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   for (uint32_t g = 0; g < G; ++g) single[g] = in_max[g] * 4 >= with_edge[g];
   st.ms_kcore += tm.stop();
 
+  // The graphs of a wave are split in two classes for each phase: those
+  // whose working core fits the bitset limit (dense_max_n vertices) and the
+  // others.  A union takes the bitset kernels only when every graph in it
+  // fits, so each class gets a union of its own and every graph runs the
+  // kernels it would run alone.
+  const uint64_t dense_lim = (uint64_t)std::max<int64_t>(0, c->opt.dense_max_n);
+
   // Phase 1.
   std::vector<uint32_t> L(G, 0);
   std::vector<uint64_t> C(G, 0);
-  {
-    tm.start();
+  std::vector<uint32_t> need1(G, 0), cap1(G, 0);
+  for (uint32_t g = 0; g < G; ++g)
+    if (cmax[g] >= 2) {
+      need1[g] = single[g] ? 2 : cmax[g];
+      cap1[g] = cmax[g] + 1;
+    }
+  for (int cls = 0; cls < 2; ++cls) {
     std::vector<uint32_t> need(G, 0), cap(G, 0);
-    for (uint32_t g = 0; g < G; ++g)
-      if (cmax[g] >= 2) {
-        need[g] = single[g] ? 2 : cmax[g];
-        cap[g] = cmax[g] + 1;
+    bool any1 = false;
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint64_t nsub = single[g] ? with_edge[g] : in_max[g];
+      if (need1[g] && (nsub <= dense_lim) == (cls == 0)) {
+        need[g] = need1[g];
+        cap[g] = cap1[g];
+        any1 = true;
       }
+    }
+    if (!any1) continue;
+    tm.start();
     Sub s1;
     union_sub(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, s1);
     st.predict_vertices += s1.n;
@@ -497,7 +530,7 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     std::vector<uint32_t> level(G, 0);
     bool pending = false;
     for (uint32_t g = 0; g < G; ++g)
-      if (ub[g] >= 3) {
+      if (need[g] && ub[g] >= 3) {
         level[g] = std::max<uint32_t>(3, std::min<uint32_t>(ub[g], (cmax[g] + 1) / 2));
         pending = true;
       }
@@ -530,7 +563,7 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   }
 
   // Phase 2.
-  std::vector<uint32_t> need(G, 0), t0(G, 3);
+  std::vector<uint32_t> need2(G, 0), t0(G, 3);
   std::vector<uint64_t> stop(G, 0);
   bool any = false;
   for (uint32_t g = 0; g < G; ++g) {
@@ -542,7 +575,7 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
       items[g]->count = C[g];
       continue;
     }
-    need[g] = L[g] >= 3 ? L[g] - 1 : 2;
+    need2[g] = L[g] >= 3 ? L[g] - 1 : 2;
     if (L[g] >= 3) {
       t0[g] = L[g];
       stop[g] = C[g];
@@ -550,43 +583,73 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     any = true;
   }
   if (!any) return;
-  tm.start();
-  Sub s2;
-  union_sub(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, s2);
-  st.core_vertices += s2.n;
-  st.core_edges += s2.m;
-  st.ms_subgraph += tm.stop();
-  tm.start();
-  DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
-  std::vector<uint32_t> thr(G, 0);
-  for (uint32_t g = 0; g < G; ++g) thr[g] = need[g] ? t0[g] - 2 : 0;
-  // As in the single-graph search phase: each graph's peel starts at t0[g]
-  // with no jump, so supports below t0[g] - 2 only need to be known as
-  // "below" (the capped dense kernel, per-graph caps).
-  const bool capped = c->opt.capped_support && s2.W;
-  DBuf dthr;
-  if (capped) {
-    dthr.alloc(c, G * sizeof(uint32_t));
-    copy_h2d(c, dthr.get(), thr.data(), G * sizeof(uint32_t));
+  // Vertices of each graph's (need2[g])-core, for the class split.
+  std::vector<unsigned long long> n2(G, 0);
+  {
+    tm.start();
+    DBuf dneed(c, G * 4ull), dcnt(c, G * 8ull);
+    copy_h2d(c, dneed.get(), need2.data(), G * 4ull);
+    zero(c, dcnt.get(), dcnt.bytes());
+    k_group_at_least<<<grid_for(nv, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+        dcore.as<uint32_t>(), dgid.as<uint32_t>(), nv, dneed.as<uint32_t>(), dcnt.as<unsigned long long>());
+    KT_LAUNCHED(c);
+    copy_d2h(c, n2.data(), dcnt.get(), G * 8ull);
+    st.ms_subgraph += tm.stop();
   }
-  edge_support(c, s2, sup2.as<uint32_t>(), 0, capped ? dthr.as<uint32_t>() : nullptr);
-  Sub s3;
-  DBuf sup3;
-  const bool rebuilt = survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
-  if (!rebuilt && capped) edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
-  st.ms_support += tm.stop();
-  tm.start();
-  std::vector<uint32_t> km;
-  std::vector<uint64_t> cn;
-  if (rebuilt)
-    tracked_peel(c, s3, sup3.as<uint32_t>(), t0, stop, km, cn);
-  else
-    tracked_peel(c, s2, sup2.as<uint32_t>(), t0, stop, km, cn);
-  st.ms_peel += tm.stop();
-  for (uint32_t g = 0; g < G; ++g) {
-    if (!need[g]) continue;
-    items[g]->kmax = km[g] >= 3 ? km[g] : 0;
-    items[g]->count = km[g] >= 3 ? cn[g] : 0;
+  for (int cls = 0; cls < 2; ++cls) {
+    std::vector<uint32_t> need(G, 0);
+    bool any2 = false;
+    for (uint32_t g = 0; g < G; ++g)
+      if (need2[g] && (n2[g] <= dense_lim) == (cls == 0)) {
+        need[g] = need2[g];
+        any2 = true;
+      }
+    if (!any2) continue;
+    tm.start();
+    Sub s2;
+    union_sub(c, U, dcore.as<uint32_t>(), dgid.as<uint32_t>(), G, need, s2);
+    st.core_vertices += s2.n;
+    st.core_edges += s2.m;
+    st.ms_subgraph += tm.stop();
+    tm.start();
+    DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
+    std::vector<uint32_t> thr(G, 0);
+    for (uint32_t g = 0; g < G; ++g) thr[g] = need[g] ? t0[g] - 2 : 0;
+    // As in the single-graph search phase: each graph's peel starts at t0[g]
+    // with no jump, so supports below t0[g] - 2 only need to be known as
+    // "below" (the capped dense kernel, per-graph caps).
+    const bool capped = c->opt.capped_support && s2.W;
+    DBuf dthr;
+    if (capped) {
+      dthr.alloc(c, G * sizeof(uint32_t));
+      copy_h2d(c, dthr.get(), thr.data(), G * sizeof(uint32_t));
+    }
+    edge_support(c, s2, sup2.as<uint32_t>(), 0, capped ? dthr.as<uint32_t>() : nullptr);
+    Sub s3;
+    DBuf sup3;
+    const bool rebuilt = survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
+    if (!rebuilt && capped) edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
+    st.ms_support += tm.stop();
+    tm.start();
+    std::vector<uint32_t> km;
+    std::vector<uint64_t> cn;
+    std::vector<uint32_t> t0c(G, 3);
+    std::vector<uint64_t> stopc(G, 0);
+    for (uint32_t g = 0; g < G; ++g)
+      if (need[g]) {
+        t0c[g] = t0[g];
+        stopc[g] = stop[g];
+      }
+    if (rebuilt)
+      tracked_peel(c, s3, sup3.as<uint32_t>(), t0c, stopc, km, cn);
+    else
+      tracked_peel(c, s2, sup2.as<uint32_t>(), t0c, stopc, km, cn);
+    st.ms_peel += tm.stop();
+    for (uint32_t g = 0; g < G; ++g) {
+      if (!need[g]) continue;
+      items[g]->kmax = km[g] >= 3 ? km[g] : 0;
+      items[g]->count = km[g] >= 3 ? cn[g] : 0;
+    }
   }
 }
 

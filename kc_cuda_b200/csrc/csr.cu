@@ -180,39 +180,35 @@ __global__ void k_grouped_degrees(uint64_t n, const uint64_t* __restrict__ off, 
   if (lane_id() == 0 && m) atomicMax(mx, m);
 }
 
-// First position in sorted a[lo, hi) holding a value >= x.
-__device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t* __restrict__ a, uint64_t lo, uint64_t hi,
-                                                    uint32_t x) {
-  while (lo < hi) {
-    const uint64_t mid = (lo + hi) >> 1;
-    if (a[mid] < x)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
-// Pass 2: every arc (y -> x) with x < y must have its reverse in row x's
-// upper part (else *bad); every arc with x > y is the canonical edge
-// y << 32 | x, written at its row's edge offset (the edges come out sorted).
-// Runs only once the upper arcs are known to be half of the lines, so every
-// edge index is below that half.
-__global__ void k_grouped_edges(const uint64_t* __restrict__ keys, uint64_t nk, const uint64_t* __restrict__ off,
+// Pass 2: the arcs with x > y are the canonical edges y << 32 | x, written
+// at their row's edge offset (they come out sorted); the arcs with x < y are
+// written transposed, x << 32 | y, at their row's offset among those (row y's
+// offset is off[y] - eoff[y]; they come out sorted by y).  Runs only once the
+// x > y arcs are known to be half of the lines, so every index is below that
+// half.
+__global__ void k_grouped_split(const uint64_t* __restrict__ keys, uint64_t nk, const uint64_t* __restrict__ off,
                                 const uint64_t* __restrict__ up, const uint64_t* __restrict__ eoff,
-                                const uint32_t* __restrict__ adj, uint64_t* __restrict__ edges,
-                                uint32_t* __restrict__ bad) {
+                                uint64_t* __restrict__ edges, uint64_t* __restrict__ low) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
     const uint32_t y = (uint32_t)(k >> 32), x = (uint32_t)k;
-    if (x > y) {
+    if (x > y)
       edges[eoff[y] + (i - up[y])] = k;
-    } else {
-      const uint64_t lo = up[x], hi = off[x + 1];
-      const uint64_t p = lower_bound_u32(adj, lo, hi, y);
-      if (p == hi || adj[p] != y) atomicOr(bad, 1u);
-    }
+    else
+      low[(off[y] - eoff[y]) + (i - off[y])] = ((uint64_t)x << 32) | y;
   }
+}
+
+// Pass 3: symmetry.  The transposed x < y arcs, stable-sorted by their x,
+// are sorted canonical keys; the input is symmetric exactly when they equal
+// the edge list entry by entry (every edge then appears once in each
+// direction).
+__global__ void k_equal_u64(const uint64_t* __restrict__ a, const uint64_t* __restrict__ b, uint64_t n,
+                            uint32_t* __restrict__ bad) {
+  bool diff = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    diff |= a[i] != b[i];
+  if (__any_sync(kFull, diff) && lane_id() == 0) atomicOr(bad, 1u);
 }
 
 __global__ void k_unpack(uint64_t* __restrict__ keys, uint64_t n, int vb) {
@@ -241,7 +237,10 @@ bool build_graph_grouped(Ctx* c, const uint64_t* keys, uint64_t nk, uint64_t n, 
   k_grouped_rows<<<grid, 256, 0, c->stream>>>(keys, nk, n, off.as<uint64_t>(), up.as<uint64_t>(), adj.as<uint32_t>(),
                                               flags.as<uint32_t>());
   KT_LAUNCHED(c);
-  if (read_word<uint32_t>(c, flags.as<uint32_t>())) return false;
+  if (read_word<uint32_t>(c, flags.as<uint32_t>())) {
+    KT_LOG(c, "kt: graph build: lines not in grouped form, sorting them\n");
+    return false;
+  }
   DBuf deg(c, n * sizeof(uint32_t)), ucnt(c, (n + 1) * sizeof(uint32_t));
   zero(c, ucnt.as<uint32_t>() + n, sizeof(uint32_t));
   k_grouped_degrees<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(
@@ -252,16 +251,31 @@ bool build_graph_grouped(Ctx* c, const uint64_t* keys, uint64_t nk, uint64_t n, 
   ucnt.release();
   // Arcs with x > y must be exactly half of the lines (the other half being
   // their reverses, checked next).
-  if (2 * read_word<uint64_t>(c, eoff.as<uint64_t>() + n) != nk) return false;
-  DBuf edges(c, nk / 2 * sizeof(uint64_t));
-  k_grouped_edges<<<grid, 256, 0, c->stream>>>(keys, nk, off.as<uint64_t>(), up.as<uint64_t>(), eoff.as<uint64_t>(),
-                                               adj.as<uint32_t>(), edges.as<uint64_t>(), flags.as<uint32_t>());
+  if (2 * read_word<uint64_t>(c, eoff.as<uint64_t>() + n) != nk) {
+    KT_LOG(c, "kt: graph build: grouped lines are not symmetric, sorting them\n");
+    return false;
+  }
+  const uint64_t m = nk / 2;
+  DBuf edges(c, m * sizeof(uint64_t)), low(c, m * sizeof(uint64_t));
+  k_grouped_split<<<grid, 256, 0, c->stream>>>(keys, nk, off.as<uint64_t>(), up.as<uint64_t>(), eoff.as<uint64_t>(),
+                                               edges.as<uint64_t>(), low.as<uint64_t>());
   KT_LAUNCHED(c);
+  up.release();
+  eoff.release();
+  // Sorted by x, the high half (stable: y stays ascending within each x).
+  radix_sort_u64(c, low.as<uint64_t>(), nullptr, m, 32 + bits_for(n), 32);
+  k_equal_u64<<<grid_for(m, 256, c->num_sms * 16), 256, 0, c->stream>>>(low.as<uint64_t>(), edges.as<uint64_t>(),
+                                                                          m, flags.as<uint32_t>());
+  KT_LAUNCHED(c);
+  low.release();
   uint32_t h[2];
   copy_d2h(c, h, flags.get(), 8);
-  if (h[0]) return false;
+  if (h[0]) {
+    KT_LOG(c, "kt: graph build: grouped lines are not symmetric, sorting them\n");
+    return false;
+  }
   g.n = n;
-  g.m = nk / 2;
+  g.m = m;
   g.off = std::move(off);
   g.adj = std::move(adj);
   g.edges = std::move(edges);

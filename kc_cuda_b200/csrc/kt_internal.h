@@ -221,9 +221,11 @@ void scan_u32_to_u64(Ctx* c, const uint32_t* in, uint64_t* out, uint64_t n);
 void scan_u32(Ctx* c, const uint32_t* in, uint32_t* out, uint64_t n);
 // Sum of n uint32 values (device result in *dsum, also returned).
 uint64_t reduce_u32(Ctx* c, const uint32_t* in, uint64_t n);
-// Stable LSD radix sort of keys (and optional uint32 values) over the low
-// `bits` bits.  `keys`/`vals` hold the input and receive the output.
-void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits);
+// Stable LSD radix sort of keys (and optional uint32 values) by their bits
+// [lo_bit, bits) (8-bit digits from lo_bit up; a digit may also read bits at
+// or above `bits`, which must then be equal in every key).  `keys`/`vals`
+// hold the input and receive the output.
+void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits, int lo_bit = 0);
 // Sorted-unique compaction of keys (drops key == ~0).  Returns new count.
 uint64_t unique_sorted_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n);
 

@@ -9,6 +9,8 @@
 // run with consecutive threads on consecutive addresses.  A
 // first pass histograms all eight digit positions at once so passes whose
 // digit is the same for every key are skipped.
+#include <algorithm>
+
 #include "kt_device.cuh"
 #include "kt_internal.h"
 
@@ -22,13 +24,14 @@ constexpr unsigned kWarpKeys = 32 * kSortIpt;           // 512
 constexpr unsigned kSortTile = kSortWarps * kWarpKeys;  // 4096
 
 __global__ void __launch_bounds__(kSortThreads) k_hist_all(const uint64_t* __restrict__ keys, uint64_t n,
-                                                           int passes, unsigned long long* __restrict__ hist) {
+                                                           int lo, int passes,
+                                                           unsigned long long* __restrict__ hist) {
   __shared__ uint32_t h[8][256];
   for (unsigned i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255], 1u);
+    for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(k >> (lo + 8 * p)) & 255], 1u);
   }
   __syncthreads();
   for (unsigned i = threadIdx.x; i < (unsigned)passes * 256; i += blockDim.x) {
@@ -132,15 +135,16 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t* __rest
 
 }  // namespace
 
-void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits) {
-  if (n < 2 || bits <= 0) return;
-  if (n >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "radix sort: more than 2^32-1 keys");
+void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits, int lo_bit) {
   if (bits > 64) bits = 64;
-  const int passes = (bits + 7) / 8;
+  if (lo_bit < 0) lo_bit = 0;
+  if (n < 2 || bits <= lo_bit) return;
+  if (n >= 0xffffffffULL) throw Error(KT_ERR_LIMIT, "radix sort: more than 2^32-1 keys");
+  const int passes = std::min((bits - lo_bit + 7) / 8, (64 - lo_bit + 7) / 8);
   DBuf hist(c, 8 * 256 * sizeof(unsigned long long));
   zero(c, hist.get(), hist.bytes());
   k_hist_all<<<grid_for(n, kSortThreads, c->num_sms * 8), kSortThreads, 0, c->stream>>>(
-      keys, n, passes, hist.as<unsigned long long>());
+      keys, n, lo_bit, passes, hist.as<unsigned long long>());
   KT_LAUNCHED(c);
   std::vector<unsigned long long> h(8 * 256);
   copy_d2h(c, h.data(), hist.get(), h.size() * sizeof(unsigned long long));
@@ -160,7 +164,7 @@ void radix_sort_u64(Ctx* c, uint64_t* keys, uint32_t* vals, uint64_t n, int bits
     int distinct = 0;
     for (int d = 0; d < 256; ++d) distinct += h[p * 256 + d] != 0;
     if (distinct <= 1) continue;
-    const int shift = 8 * p;
+    const int shift = lo_bit + 8 * p;
     k_tile_hist<<<ntiles, kSortThreads, 0, c->stream>>>(ksrc, n, shift, ntiles, th.as<uint32_t>());
     KT_LAUNCHED(c);
     scan_u32(c, th.as<uint32_t>(), th.as<uint32_t>(), (uint64_t)ntiles * 256);

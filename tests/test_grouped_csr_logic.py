@@ -1,6 +1,7 @@
 """CPU transcription of the graph build's grouped-input route
-(k_grouped_rows, k_grouped_degrees, the upper-arc count check and
-k_grouped_edges in kc_cuda_b200/csrc/csr.cu), run line by line.
+(k_grouped_rows, k_grouped_degrees, the upper-arc count check,
+k_grouped_split, the stable sort of the transposed lower arcs by their first
+column, and k_equal_u64 in kc_cuda_b200/csrc/csr.cu), run line by line.
 
 The route must accept exactly the reference's input contract with ascending
 rows (lines grouped by ascending second column, every edge in both
@@ -94,19 +95,21 @@ def grouped_route(keys, n):
     eoff = np.concatenate([[0], np.cumsum(ucnt)]).astype(np.int64)
     if 2 * int(eoff[n]) != nk:
         return None
-    edges = [None] * (nk // 2)
-    for i, k in enumerate(keys):  # k_grouped_edges
+    m = nk // 2
+    edges, low = [None] * m, [None] * m
+    for i, k in enumerate(keys):  # k_grouped_split
         y, x = k >> 32, k & 0xFFFFFFFF
         if x > y:
             j = int(eoff[y]) + (i - up[y])
-            assert 0 <= j < nk // 2 and edges[j] is None
+            assert 0 <= j < m and edges[j] is None
             edges[j] = k
         else:
-            row = adj[up[x]:off[x + 1]]
-            p = int(np.searchsorted(row, y))
-            if p == len(row) or row[p] != y:
-                bad = True
-    if bad:
+            j = (off[y] - int(eoff[y])) + (i - off[y])
+            assert 0 <= j < m and low[j] is None
+            low[j] = (x << 32) | y
+    # Stable sort by the high half, then entry-by-entry equality (k_equal_u64).
+    low.sort(key=lambda t: t >> 32)
+    if low != edges:
         return None
     return off, adj, deg, np.array(edges, dtype=np.uint64)
 
