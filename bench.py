@@ -588,10 +588,11 @@ def run_reference(args, rank, threads):
 # DRAM traffic of the dense support kernel, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of a k_dense_support launch
 # on the core55k-support case of cases.py: G(n=55455, 95M draws), whose core
-# has the bench graph's search-core shape.  The bench graph's launches are
-# too large to capture under the profiling size rule, so their traffic is
-# scaled from this one by the row words each launch reads.  None: no capture.
-SUPPORT_CAPTURE = None  # {"dram_bytes": ..., "row_words": ...}
+# has the bench graph's search-core shape (92.1M edges, rows of 1736 words);
+# the launch read 166.3G row words.  The bench graph's launches are too large
+# to capture under the profiling size rule, so their traffic is scaled from
+# this one by the row words each launch reads.
+SUPPORT_CAPTURE = {"dram_bytes": 6_683_428_000 + 373_861_632, "row_words": 166_313_504_560}
 
 
 def roofline(name, kbytes, kms, klaunch, steps, hbm, peak_kind, **extra):

@@ -92,7 +92,10 @@ const char* kt_status_string(kt_status s);
  *                               chunks <= this x warps deals (edge, chunk) units
  *                               to warps instead of edges (0 = off)
  *   serve_lanes (2)             serving: waves in flight at once, 1..4
- *   batch_lanes (2)             batch: waves in flight at once, 1..2 */
+ *   batch_lanes (2)             batch: waves in flight at once, 1..2
+ *   support_rows (4)            dense support: edges sharing row u counted together
+ *                               per shared-memory read of it (1, 2 or 4; the capped
+ *                               kernel of the search phase at most 2) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 

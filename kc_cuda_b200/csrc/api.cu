@@ -27,6 +27,7 @@ bool option_value_ok(const char* name, int64_t value) {
   if (!std::strcmp(name, "timeout_ms")) return value <= 3600000;
   if (!std::strcmp(name, "serve_lanes")) return value >= 1 && value <= 4;
   if (!std::strcmp(name, "batch_lanes")) return value >= 1 && value <= 2;
+  if (!std::strcmp(name, "support_rows")) return value == 1 || value == 2 || value == 4;
   return true;
 }
 
@@ -401,7 +402,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"kcore_compact", &o.kcore_compact},
              {"wave_budget_pct", &o.wave_budget_pct},
              {"serve_lanes", &o.serve_lanes},
-             {"batch_lanes", &o.batch_lanes}};
+             {"batch_lanes", &o.batch_lanes},
+             {"support_rows", &o.support_rows}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

@@ -9,11 +9,13 @@
 // A warp takes 32 consecutive edges of a list.  Each lane fetches one edge's
 // ends, then the warp walks the 32 edges: row u is copied into the warp's
 // slice of shared memory (W words) and reused while consecutive edges share
-// u (the lists are tile-ordered by (u block, v block, u, v)), row v streams
-// from L2 with every lane on consecutive words.  Keeping row u in shared
-// memory rather than registers leaves the kernels at few registers, so many
-// warps hide the L2 latency.  Lane j keeps the count of the j-th edge, so
-// results are written or pushed once per group.
+// u (the lists are tile-ordered by (u block, v block, u, v)); up to four
+// edges that share row u are counted together, each lane reading a vector
+// of row u from shared memory once and ANDing it with the same vector of the
+// four rows v, which stream from L2 with every lane on consecutive vectors.
+// Keeping row u in shared memory rather than registers leaves the kernels at
+// few registers, so many warps hide the L2 latency.  Lane j keeps the count
+// of the j-th edge, so results are written or pushed once per group.
 #pragma once
 #include "kt_device.cuh"
 #include "subgraph.h"
@@ -48,20 +50,8 @@ inline DenseRows dense_rows(const Sub& s) {
                    grouped ? s.vbase.as<uint32_t>() : nullptr, s.sbits.as<uint32_t>(), s.spre.as<uint32_t>()};
 }
 
-// 16-byte loads of row v in flight per lane.  Rows are whole 16-byte vectors
-// (W a multiple of 4, rows 16-byte aligned; the padding words stay zero).
-#ifndef KT_DENSE_DEPTH
-#define KT_DENSE_DEPTH 4
-#endif
-constexpr int kDenseDepth = KT_DENSE_DEPTH;
-// Capped and exact support: two edges sharing row u per warp, one per half
-// (build constants).
-#ifndef KT_CAPPED_PAIRS
-#define KT_CAPPED_PAIRS 1
-#endif
-#ifndef KT_EXACT_PAIRS
-#define KT_EXACT_PAIRS 1
-#endif
+// Rows are whole 16-byte vectors (W a multiple of 4, rows 16-byte aligned;
+// the padding words stay zero).
 
 // Shared memory a block of `threads` needs for rows of W words.
 inline size_t dense_smem_bytes(uint32_t W, unsigned threads) { return (size_t)(threads / 32) * W * 4; }
@@ -77,56 +67,78 @@ __device__ __forceinline__ uint32_t popc_and4(uint4 a, uint4 b) {
   return __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
 }
 
-// popcount(row u & row v) over words [w0, w1) (multiples of 4); every lane
-// returns the warp total.  Lanes read 16-byte vectors, kDenseDepth strides
-// of the warp at a time (L2-only caching: each row v is used once per edge).
-__device__ __forceinline__ uint32_t dense_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
-                                                   uint32_t w1) {
-  const uint4* p4 = reinterpret_cast<const uint4*>(p);
-  const uint4* s4 = reinterpret_cast<const uint4*>(su);
-  uint32_t s = 0;
-  uint32_t i = w0 / 4 + lane_id();
-  const uint32_t e = w1 / 4;
-  for (; i + (kDenseDepth - 1) * 32 < e; i += kDenseDepth * 32) {
-    uint4 a[kDenseDepth];
+// popcount(row u & row v_q) over the 16-byte vectors [i0, i1) of up to NQ
+// rows v_q at once (row q taking part when act[q]; the loads of the others
+// are predicated off): each lane reads a vector of row u from shared memory
+// once and ANDs it with the same vector of every row v_q (two vectors per row
+// in flight per lane), so edges that share row u share its shared-memory
+// reads.  Every lane of the warp must call it; out[q] gets row q's warp total
+// (0 when it takes no part).
+template <int NQ>
+__device__ __forceinline__ void rows_and_popc(const DenseRows& R, const uint32_t* vq, const bool* act,
+                                              const uint32_t* su, uint32_t i0, uint32_t i1, uint32_t* out) {
+  const uint4* pv[NQ];
+  uint32_t c[NQ];
 #pragma unroll
-    for (int k = 0; k < kDenseDepth; ++k) a[k] = __ldcg(p4 + i + 32 * k);
-#pragma unroll
-    for (int k = 0; k < kDenseDepth; ++k) s += popc_and4(s4[i + 32 * k], a[k]);
+  for (int q = 0; q < NQ; ++q) {
+    pv[q] = reinterpret_cast<const uint4*>(R.bits + R.off(act[q] ? vq[q] : vq[0]));
+    c[q] = 0;
   }
-  for (; i < e; i += 32) s += popc_and4(s4[i], __ldcg(p4 + i));
-  return warp_sum(s);
+  const uint4* s4 = reinterpret_cast<const uint4*>(su);
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  uint32_t i = i0 + lane_id();
+  for (; i + 32 < i1; i += 64) {
+    const uint4 a0 = s4[i], a1 = s4[i + 32];
+    uint4 b0[NQ], b1[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      b0[q] = act[q] ? __ldcg(pv[q] + i) : z;
+      b1[q] = act[q] ? __ldcg(pv[q] + i + 32) : z;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) c[q] += popc_and4(a0, b0[q]) + popc_and4(a1, b1[q]);
+  }
+  if (i < i1) {
+    const uint4 a = s4[i];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) c[q] += popc_and4(a, act[q] ? __ldcg(pv[q] + i) : z);
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = act[q] ? warp_sum(c[q]) : 0u;
 }
 
-// popcount(row u & row v) over words [w0, w1) (multiples of 4) by one half
-// of the warp (16 lanes, 16-byte vectors); `active` false contributes 0.
-// Every lane of the warp must call it; each lane gets its half's total.
-__device__ __forceinline__ uint32_t half_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
-                                                  uint32_t w1, bool active) {
-  uint32_t s = 0;
-  if (active) {
-    const uint4* p4 = reinterpret_cast<const uint4*>(p);
-    const uint4* s4 = reinterpret_cast<const uint4*>(su);
-    uint32_t i = w0 / 4 + (lane_id() & 15);
-    const uint32_t e = w1 / 4;
-    for (; i + 3 * 16 < e; i += 4 * 16) {
-      uint4 a[4];
+// Edge j and up to NQ-1 more edges of the group that share its row u (they
+// follow it in the tile-ordered list): slot q gets the lane jq[q] and column
+// vq[q] of one of them (act[q]), and they leave `todo`.  Warp-uniform.
+template <int NQ>
+__device__ __forceinline__ void take_same_row(unsigned& todo, uint32_t u, uint32_t v, uint32_t uj, int j,
+                                              uint32_t vj, int* jq, uint32_t* vq, bool* act) {
+  jq[0] = j;
+  vq[0] = vj;
+  act[0] = true;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) a[k] = __ldcg(p4 + i + 16 * k);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s += popc_and4(s4[i + 16 * k], a[k]);
+  for (int q = 1; q < NQ; ++q) {
+    jq[q] = -1;
+    vq[q] = vj;
+    act[q] = false;
+    if (todo) {
+      const int cand = __ffs(todo) - 1;
+      const uint32_t uc = __shfl_sync(kFull, u, cand), vc = __shfl_sync(kFull, v, cand);
+      if (uc == uj && act[q - 1]) {
+        jq[q] = cand;
+        vq[q] = vc;
+        act[q] = true;
+        todo &= todo - 1;
+      }
     }
-    for (; i < e; i += 16) s += popc_and4(s4[i], __ldcg(p4 + i));
   }
-#pragma unroll
-  for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-  return s;
 }
 
 // One group of up to 32 list entries [base, min(base+32, cnt)).  Entries
 // whose state is not kAlive (when state != nullptr) are skipped.  On return
 // lane j holds (my_e, my_s) of the group's j-th entry, my_ok = counted.
 // su is this warp's W-word slice of shared memory.
+template <int NQ = 4>
 __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                             const uint64_t* __restrict__ ends, const DenseRows& R,
                                             const uint32_t* __restrict__ state, uint32_t* su, uint32_t& my_e,
@@ -160,30 +172,20 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
       cu = uj;
       if (wr && l == 0) *wr += W;
     }
-#if KT_EXACT_PAIRS
-    // The next edge with the same row u goes to the upper half of the warp.
-    int j2 = -1;
-    uint32_t vj2 = 0;
-    if (todo) {
-      const int cand = __ffs(todo) - 1;
-      const uint32_t uc = __shfl_sync(kFull, u, cand), vc = __shfl_sync(kFull, v, cand);
-      if (uc == uj) {
-        j2 = cand;
-        vj2 = vc;
-        todo &= todo - 1;
-      }
+    // Up to NQ edges sharing row u: one shared-memory read of row u feeds
+    // all of them.
+    int jq[NQ];
+    uint32_t vq[NQ], cq[NQ];
+    bool act[NQ];
+    take_same_row<NQ>(todo, u, v, uj, j, vj, jq, vq, act);
+    rows_and_popc<NQ>(R, vq, act, su, 0, W / 4, cq);
+    uint32_t nq = 0;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      if (act[q] && l == (unsigned)jq[q]) my_s = cq[q];
+      nq += act[q];
     }
-    const bool upper = l >= 16;
-    const uint32_t s = half_and_popc(R.bits + R.off(upper ? vj2 : vj), su, 0, W, !upper || j2 >= 0);
-    const uint32_t f0 = __shfl_sync(kFull, s, 0), f1 = __shfl_sync(kFull, s, 16);
-    if (l == (unsigned)j) my_s = f0;
-    if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
-    if (wr && l == 0) *wr += j2 >= 0 ? 2ull * W : W;
-#else
-    const uint32_t s = dense_and_popc(R.bits + R.off(vj), su, 0, W);
-    if (l == (unsigned)j) my_s = s;
-    if (wr && l == 0) *wr += W;
-#endif
+    if (wr && l == 0) *wr += (unsigned long long)nq * W;
   }
   __syncwarp();
 }
@@ -194,6 +196,7 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 // count so far plus the set bits left in row u bounds the result.  An
 // abandoned edge reports a count below the threshold (not its support).  The
 // threshold is `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
+template <int NQ = 4>
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends, const DenseRows& R,
                                                    uint32_t thr, uint32_t* su, uint32_t& my_e, uint32_t& my_s,
@@ -242,66 +245,41 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       s3 = warp_sum(d);
       if (wr && l == 0) *wr += W;
     }
-#if KT_CAPPED_PAIRS
-    // The next edge with the same row u goes to the upper half of the warp:
-    // two edges' segments are ANDed side by side (two load streams).
-    int j2 = -1;
-    uint32_t vj2 = 0;
-    if (todo) {
-      const int cand = __ffs(todo) - 1;
-      const uint32_t uc = __shfl_sync(kFull, u, cand), vc = __shfl_sync(kFull, v, cand);
-      if (uc == uj) {
-        j2 = cand;
-        vj2 = vc;
-        todo &= todo - 1;
+    // Up to NQ edges sharing row u, segment by segment; an edge leaves once
+    // its count so far plus row u's set bits in the later segments cannot
+    // reach its threshold.
+    int jq[NQ];
+    uint32_t vq[NQ], tq[NQ], found[NQ], cs[NQ];
+    bool go[NQ], in[NQ];
+    take_same_row<NQ>(todo, u, v, uj, j, vj, jq, vq, in);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      tq[q] = __shfl_sync(kFull, my_thr, in[q] ? jq[q] : j);
+      go[q] = in[q];
+      found[q] = 0;
+    }
+    uint32_t wds = 0;
+#pragma unroll 1
+    for (int sg = 0; sg < 4; ++sg) {
+      const uint32_t b0 = sg == 0 ? 0u : sg == 1 ? c1 : sg == 2 ? c2 : c3;
+      const uint32_t b1 = sg == 0 ? c1 : sg == 1 ? c2 : sg == 2 ? c3 : W;
+      const uint32_t rest = sg == 0 ? s1 + s2 + s3 : sg == 1 ? s2 + s3 : sg == 2 ? s3 : 0u;
+      bool any = false;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) any |= go[q];
+      if (!any) break;
+      rows_and_popc<NQ>(R, vq, go, su, b0 / 4, b1 / 4, cs);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        wds += go[q] ? b1 - b0 : 0u;
+        found[q] += cs[q];
+        go[q] = go[q] && found[q] + rest >= tq[q];
       }
     }
-    const bool upper = l >= 16;
-    const uint32_t tj = __shfl_sync(kFull, my_thr, j), tj2 = __shfl_sync(kFull, my_thr, j2 >= 0 ? j2 : j);
-    const uint32_t t = upper ? tj2 : tj;
-    bool go = !upper || j2 >= 0;
-    const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
-    uint32_t wds = go ? c1 : 0u;  // row-v words this half reads
-    uint32_t found = half_and_popc(pv, su, 0, c1, go);
-    go = go && found + s1 + s2 + s3 >= t;
-    if (__any_sync(kFull, go)) {
-      wds += go ? c2 - c1 : 0u;
-      found += half_and_popc(pv, su, c1, c2, go);
-      go = go && found + s2 + s3 >= t;
-      if (__any_sync(kFull, go)) {
-        wds += go ? c3 - c2 : 0u;
-        found += half_and_popc(pv, su, c2, c3, go);
-        go = go && found + s3 >= t;
-        if (__any_sync(kFull, go)) {
-          wds += go ? W - c3 : 0u;
-          found += half_and_popc(pv, su, c3, W, go);
-        }
-      }
-    }
-    const uint32_t f0 = __shfl_sync(kFull, found, 0), f1 = __shfl_sync(kFull, found, 16);
-    if (l == (unsigned)j) my_s = f0;
-    if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
-    if (wr && (l & 15u) == 0) *wr += wds;
-#else
-    const uint32_t* pv = R.bits + R.off(vj);
-    const uint32_t t = __shfl_sync(kFull, my_thr, j);
-    uint32_t wds = c1;
-    uint32_t found = dense_and_popc(pv, su, 0, c1);
-    if (found + s1 + s2 + s3 >= t) {
-      wds = c2;
-      found += dense_and_popc(pv, su, c1, c2);
-      if (found + s2 + s3 >= t) {
-        wds = c3;
-        found += dense_and_popc(pv, su, c2, c3);
-        if (found + s3 >= t) {
-          wds = W;
-          found += dense_and_popc(pv, su, c3, W);
-        }
-      }
-    }
-    if (l == (unsigned)j) my_s = found;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      if (in[q] && l == (unsigned)jq[q]) my_s = found[q];
     if (wr && l == 0) *wr += wds;
-#endif
   }
   __syncwarp();
 }

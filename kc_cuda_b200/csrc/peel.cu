@@ -401,7 +401,7 @@ __device__ __forceinline__ void recount_round(const PeelArgs& A, uint32_t r, uin
     if (g >= groups) break;
     uint32_t e, sc;
     bool ok;
-    dense_group(A.alive, g * 32, A.na, A.ends, A.R, A.state, su, e, sc, ok);
+    dense_group<2>(A.alive, g * 32, A.na, A.ends, A.R, A.state, su, e, sc, ok);
     trec += __popc(__ballot_sync(kFull, ok));
     bool want = false;
     if (ok) {

@@ -152,8 +152,10 @@ __global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, cons
   }
 }
 
-template <bool kCapped>
-__global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
+// Four resident blocks per SM (what the rows' shared memory allows for the
+// bench graph's cores) bound the registers to 64.
+template <bool kCapped, int NQ>
+__global__ void __launch_bounds__(256, 4) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
                                                        const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
                                                        const uint32_t* __restrict__ gcap,
                                                        const uint32_t* __restrict__ vgid,
@@ -175,9 +177,9 @@ __global__ void __launch_bounds__(256) k_dense_support(uint64_t m, const uint32_
     uint32_t e, s;
     bool ok;
     if (kCapped)
-      dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr, gcap, vgid);
+      dense_group_capped<NQ>(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr, gcap, vgid);
     else
-      dense_group(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
+      dense_group<NQ>(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
     if (ok) sup[e] = s;
   }
   wr = warp_sum(wr);
@@ -194,19 +196,37 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
   }
 }
 
-template <bool kCapped>
-void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
-                          unsigned long long* row_words, unsigned long long* cursor) {
+template <bool kCapped, int NQ>
+void launch_dense_support_n(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
+                            unsigned long long* row_words, unsigned long long* cursor) {
   const size_t smem = dense_smem_bytes(s.W, 256);
-  allow_max_dynamic_smem((const void*)k_dense_support<kCapped>);
+  allow_max_dynamic_smem((const void*)k_dense_support<kCapped, NQ>);
   int per_sm = 0;
-  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped>, 256, smem));
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped, NQ>, 256, smem));
   const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-  k_dense_support<kCapped><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+  k_dense_support<kCapped, NQ><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
                                                            dense_rows(s), cap, gcap,
                                                            gcap ? s.vgid.as<uint32_t>() : nullptr, sup, row_words,
                                                            cursor);
   KT_LAUNCHED(c);
+}
+
+// Edges sharing row u counted together: option support_rows (1, 2 or 4);
+// the capped kernel, whose segment state takes more registers, counts at
+// most two together.
+template <bool kCapped>
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
+                          unsigned long long* row_words, unsigned long long* cursor) {
+  if (c->opt.support_rows <= 1) {
+    launch_dense_support_n<kCapped, 1>(c, s, sup, cap, gcap, row_words, cursor);
+  } else if constexpr (kCapped) {
+    launch_dense_support_n<kCapped, 2>(c, s, sup, cap, gcap, row_words, cursor);
+  } else {
+    if (c->opt.support_rows == 2)
+      launch_dense_support_n<kCapped, 2>(c, s, sup, cap, gcap, row_words, cursor);
+    else
+      launch_dense_support_n<kCapped, 4>(c, s, sup, cap, gcap, row_words, cursor);
+  }
 }
 
 // Algorithmic bytes of a merge-based support count over the degree-oriented
