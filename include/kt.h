@@ -92,6 +92,9 @@ const char* kt_status_string(kt_status s);
  *                               chunks <= this x warps deals (edge, chunk) units
  *                               to warps instead of edges (0 = off)
  *   serve_lanes (2)             serving: waves in flight at once, 1..4
+ *   serve_small_mb (128)        serving with two or more lanes: lane 0 admits only
+ *                               requests whose estimated footprint is at most this
+ *                               many MB, the other lanes any (0: every lane any)
  *   batch_lanes (2)             batch: waves in flight at once, 1..2
  *   support_rows (4)            dense support: edges sharing row u counted together
  *                               per shared-memory read of it (1, 2 or 4; the capped
@@ -210,7 +213,9 @@ kt_status kt_options_load(kt_ctx* ctx, const char* path);
  * footprint fits its share of half of the context's free budget (and at most
  * max_wave_graphs of them, 0 = 65535) and solves them as one wave of the
  * batch path on its own stream; requests that arrive while waves run start in
- * the next free lane, so waves overlap on the device.  A request's answer is
+ * the next free lane, so waves overlap on the device.  With two or more lanes,
+ * lane 0 takes only small requests (serve_small_mb), oldest first, so they
+ * never wait behind a wave of large graphs.  A request's answer is
  * the same alone and in any mix.  Other calls on the context block while a
  * wave of lane 0 runs. */
 typedef struct kt_server kt_server;

@@ -403,7 +403,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"wave_budget_pct", &o.wave_budget_pct},
              {"serve_lanes", &o.serve_lanes},
              {"batch_lanes", &o.batch_lanes},
-             {"support_rows", &o.support_rows}};
+             {"support_rows", &o.support_rows},
+             {"serve_small_mb", &o.serve_small_mb}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

@@ -17,6 +17,7 @@
 // snapshot: revive the vertices whose tag is newer than the last probe at or
 // below that level, recount degrees, and probe once more.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 
@@ -922,18 +923,34 @@ uint32_t KCore::find_max_core(Ctx* c) {
   ub = std::min<uint64_t>(ub, base->max_deg);
   uint64_t lo = 1, hi = ub + 1;  // the 1-core (non-isolated vertices) is non-empty
   bool ramp = true;
+  DBuf mn(c, 4);
   while (hi - lo > 1) {
     uint64_t k = ramp ? std::min<uint64_t>(lo * 2, hi - 1) : lo + (hi - lo) / 2;
     if (k <= lo) k = lo + 1;
     const uint32_t tag = (uint32_t)levels.size();
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint64_t before = n_alive;
     const uint64_t left = probe(c, (uint32_t)k);
+    KT_LOG(c, "kt: k-core probe %llu: %llu of %llu alive vertices left, %.3f ms\n", (unsigned long long)k,
+           (unsigned long long)left, (unsigned long long)before,
+           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     if (left) {
       lo = k;
       succ.push_back(tag);
       rebuild_alive(c);
+      // The probe left the k-core; its minimum degree d >= k makes it the
+      // d-core too, so every level up to d is known to be non-empty.
+      KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));
+      k_min_alive_deg<<<grid_for(n_alive, 256, c->num_sms * 8), 256, 0, c->stream>>>(
+          alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), mn.as<uint32_t>());
+      KT_LAUNCHED(c);
+      const uint32_t d = read_word<uint32_t>(c, mn.as<uint32_t>());
+      if (d != 0xffffffffu && d > lo) lo = std::min<uint64_t>(d, hi - 1);
       // Work on a compacted copy once the core is a small part of the graph.
+      // (The copy holds the k-core, which every level from k up can be
+      // restored from.)
       if (c->opt.kcore_compact > 0 && n_alive * (uint64_t)c->opt.kcore_compact < n)
-        compact_to_alive(c, (uint32_t)lo);
+        compact_to_alive(c, (uint32_t)k);
     } else {
       hi = k;
       ramp = false;

@@ -64,6 +64,7 @@ struct Options {
   int64_t wave_budget_pct = 50;   // batch: a wave's estimated footprint within this % of the free budget
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
   int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)
+  int64_t serve_small_mb = 128;   // serving, two or more lanes: lane 0 admits only requests this small (0: any)
   int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
   int64_t support_rows = 4;       // dense support: edges sharing row u counted per read of it (1, 2, 4)
 };

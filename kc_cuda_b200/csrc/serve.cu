@@ -6,7 +6,9 @@
 // context, the others contexts the server creates with the same options --
 // with its own stream, device words and budget.  Whenever a lane is free it
 // admits queued requests, oldest first, while their estimated device
-// footprint fits the lane's share of the budget (and up to a graph cap), and
+// footprint fits the lane's share of the budget (and up to a graph cap) --
+// with two or more lanes, lane 0 admits only small requests (footprint up to
+// serve_small_mb), so they never queue behind a wave of large graphs -- and
 // solves the admitted set as one wave -- one disjoint union through every
 // stage, each graph on its own peel levels (batch.cu).  So while one wave is
 // on the device, requests that arrive meanwhile start in the next free lane
@@ -63,6 +65,12 @@ struct kt_server {
   kt_server_stats st{};
   std::vector<Lane> lanes;
   std::mutex coop;  // cooperative launches of the lanes, one at a time
+  uint64_t small_bytes = 0;  // lane 0 admits only requests of at most this footprint (0: any)
+  bool queue_has_small() const {
+    for (const Request* r : queue)
+      if (r->footprint <= small_bytes) return true;
+    return false;
+  }
 
   // Same estimate as the batch driver's waves: keys, sort buffers, CSR and
   // core state ~ 48 B per edge record and 40 B per vertex id.
@@ -79,7 +87,7 @@ struct kt_server {
     queue.push_back(r.get());
     reqs.emplace(r->id, std::move(r));
     st.submitted++;
-    work_cv.notify_one();
+    work_cv.notify_all();  // every free lane looks: the small lane may not take it
     return KT_OK;
   }
 
@@ -92,17 +100,32 @@ struct kt_server {
         std::unique_lock<std::mutex> lk(m);
         work_cv.wait(lk, [&] { return stopping || !queue.empty(); });
         if (queue.empty()) break;  // stopping and drained
-        // Admission: arrival order, while the footprint fits.
+        // Admission: arrival order, while the footprint fits.  With a small
+        // lane (lane 0 of two or more, small_bytes > 0) that lane admits only
+        // requests of at most small_bytes, skipping larger ones; the other
+        // lanes admit any request.
+        const bool small_only = small_bytes && lanes.size() > 1 && lane_ctx == lanes[0].ctx;
         uint64_t bytes = 0;
-        while (!queue.empty() && wave.size() < max_wave) {
-          Request* r = queue.front();
+        for (auto it = queue.begin(); it != queue.end() && wave.size() < max_wave;) {
+          Request* r = *it;
+          if (small_only && r->footprint > small_bytes) {
+            ++it;
+            continue;
+          }
           if (!wave.empty() && bytes + r->footprint > budget) break;
           bytes += r->footprint;
           wave.push_back(r);
-          queue.pop_front();
+          it = queue.erase(it);
         }
-        // Others still queued: wake another free lane for them.
-        if (!queue.empty()) work_cv.notify_one();
+        if (wave.empty()) {
+          // Only large requests are queued and this is the small lane: the
+          // other lanes take them; wait for a small arrival (or the end).
+          if (stopping) break;
+          work_cv.wait(lk, [&] { return stopping || queue_has_small(); });
+          continue;
+        }
+        // Others still queued: wake the other free lanes for them.
+        if (!queue.empty()) work_cv.notify_all();
       }
       const Clock::time_point t_admit = Clock::now();
       std::vector<kt::BatchItem*> items;
@@ -211,6 +234,7 @@ kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** ou
     device = c.device;
     ctx_budget = c.budget;
     nlanes = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c.opt.serve_lanes), 4);
+    s->small_bytes = nlanes > 1 ? (uint64_t)std::max<int64_t>(0, c.opt.serve_small_mb) << 20 : 0;
     // Half of the free budget for the waves in flight, shared by the lanes.
     s->budget = (c.budget > c.in_use ? c.budget - c.in_use : 0) / 2 / nlanes;
   }
