@@ -340,9 +340,10 @@ def mix_sizes(first: int, count: int):
     return out
 
 
-def batch_run(ctx, indices=None, first=0, count=0):
+def batch_run(ctx, indices=None, first=0, count=0, stages=None):
     """One kt_batch_run over mix graphs (a list of indices, or a range);
-    returns (device ms without the input generation, waves, answers)."""
+    returns (device ms of the whole run, waves, answers); `stages` (a dict)
+    receives the stage times summed over the lanes."""
     b = ctx.batch()
     if indices is None:
         b.add_mix(first, count)
@@ -353,6 +354,10 @@ def batch_run(ctx, indices=None, first=0, count=0):
     st = ctx.stats()
     k, c = b.results()
     b.free()
+    if stages is not None:
+        stages.update({x[3:]: round(st[x], 1) for x in ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph",
+                                                         "ms_support", "ms_peel", "ms_support_kernel",
+                                                         "ms_peel_kernel")})
     return st["ms_total"], st["batch_waves"], [(int(a), int(e)) for a, e in zip(k, c)]
 
 
@@ -389,8 +394,9 @@ def measure_mix(ctx, args, rank, pg, threads):
     batch_run(ctx, first=first, count=min(G, 64))
     barrier(pg)
     times = []
+    stages = {}
     for _ in range(args.mix_steps):
-        ms, waves, got = batch_run(ctx, first=first, count=G)
+        ms, waves, got = batch_run(ctx, first=first, count=G, stages=stages)
         times.append(ms)
     mism = [i for i, a in zip(idx, got) if a != alone[i]]
     batched_ms = max_over_ranks(pg, sum(times) / len(times))
@@ -415,6 +421,7 @@ def measure_mix(ctx, args, rank, pg, threads):
         "workload": f"mix graphs {first}..{first + G - 1}", "graphs": G, "steps": args.mix_steps,
         "lanes": args.batch_lanes,
         "graphs_per_s": total / (batched_ms / 1000.0), "ms_per_step": batched_ms, "waves": waves,
+        "stage_ms_summed_over_lanes": stages,
         "per_graph": {"graphs_per_s": total / (per_graph_ms / 1000.0), "ms_total": per_graph_ms, "graphs": G,
                       "p50_ms": float(np.percentile(lat_np, 50)), "p99_ms": float(np.percentile(lat_np, 99))},
         "ratio": per_graph_ms / batched_ms,
@@ -684,7 +691,11 @@ def run_single(args, world, rank, local, pg, threads):
         recount_bytes_per_step=acc["peel_recount_bytes"] / S)
     dominant = roof_sup if acc["ms_support_kernel"] >= acc["ms_peel_kernel"] else roof_peel
 
+    attributed = sum(stats_last[k] for k in ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support",
+                                              "ms_peel"))
     progress("single_graph", {"value": value, "e2e": e2e_value, "answer": list(answer),
+                              "ms_total": stats_last["ms_total"],
+                              "ms_outside_stages": stats_last["ms_total"] - attributed,
                               "stage_ms": {k: round(stats_last[k], 3) for k in
                                            ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support",
                                             "ms_peel")},
@@ -736,8 +747,9 @@ def run_single(args, world, rank, local, pg, threads):
                 "dense support rows are read mostly from L2 (tile order), so frac near 1 of the HBM copy "
                 "bandwidth is L2-served work; traffic is the DRAM share")),
             "rooflines": {"support": roof_sup, "peel": roof_peel},
-            "stage_ms": {k: round(stats_last[k], 3) for k in
-                         ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel")},
+            "stage_ms": dict({k: round(stats_last[k], 3) for k in
+                              ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel")},
+                             outside_stages=round(stats_last["ms_total"] - attributed, 3)),
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "batched": mix,

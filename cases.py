@@ -16,6 +16,10 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
   rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
   rmat24-solve    the bench graph (R-MAT scale 24, edge factor 32, seed 2,
                   cliques 80/120/200; 15.5 GB of TSV staged on the device).
+  chunglu10m-solve  Chung-Lu, 10M vertices, 200M draws, exponent 2.1, expected
+                  degrees capped at 400K, seed 3, a 150-vertex block of pair
+                  probability 0.95 (config 3's shape at a fifth of its size).
+  chunglu50m-solve  config 3 itself (32 GB of TSV staged on the device).
   mix-batch       graphs 0..255 of the batched mix in one kt_batch_run
                   (k_core_levels on the union, grouped support and peel).
   mix-largest     the --count largest of mix graphs 0..4095 (by draws) in one
@@ -116,7 +120,7 @@ def largest_mix(count: int, among: int = 4096):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve",
-                                     "mix-batch", "mix-largest"])
+                                     "chunglu10m-solve", "chunglu50m-solve", "mix-batch", "mix-largest"])
     ap.add_argument("--count", type=int, default=64, help="mix-largest: how many of the largest graphs")
     ap.add_argument("--alone", action="store_true", help="mix cases: also solve the graphs one at a time")
     ap.add_argument("--reps", type=int, default=1)
@@ -137,6 +141,11 @@ def main() -> None:
         mix_batch(a.reps, a.verbose, indices=largest_mix(a.count), options=opts, alone=a.alone)
     elif a.case == "rmat24-solve":
         solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
+    elif a.case == "chunglu10m-solve":
+        solve(gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=10_000_000, draws=200_000_000, seed=3, cl_gamma=2.1,
+                            cl_w_min=5.0, cl_w_max=400_000.0, block_size=150, block_p=0.95), a.reps, a.verbose)
+    elif a.case == "chunglu50m-solve":
+        solve(gen.chunglu_50m(), a.reps, a.verbose)
     else:
         solve(gen.rmat_s16_k30(), a.reps, a.verbose)
 

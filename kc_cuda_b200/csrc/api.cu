@@ -7,6 +7,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -569,17 +570,23 @@ kt_status kt_solve_staged(kt_ctx* h, const kt_tsv* t, uint32_t* kmax, uint64_t* 
   KT_API_BEGIN(h)
   kt::Ctx* c = &h->c;
   kt::begin_solve_stats(c);
+  const auto t0 = std::chrono::steady_clock::now();
+  auto host_ms = [&] { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
   KT_CUDA(cudaEventRecord(c->ev[0], c->stream));
   {
     kt::Graph g;
     kt::graph_from_device_bytes(c, t->bytes.as<uint8_t>(), t->len, g);
+    KT_LOG(c, "kt: +%.2f ms graph built (parse %.2f, build %.2f ms)\n", host_ms(), c->stats.ms_parse,
+           c->stats.ms_csr);
     const double p = c->stats.ms_parse, q = c->stats.ms_csr;
     kt::solve_graph(c, g, kmax, edges);
     c->stats.ms_parse = p;
     c->stats.ms_csr = q;
+    KT_LOG(c, "kt: +%.2f ms solved\n", host_ms());
   }
   KT_CUDA(cudaEventRecord(c->ev[1], c->stream));
   c->stats.ms_total = kt::event_ms(c->ev[0], c->ev[1]);
+  KT_LOG(c, "kt: +%.2f ms graph freed; device time %.2f ms\n", host_ms(), c->stats.ms_total);
   KT_API_END(h)
 }
 

@@ -128,6 +128,13 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   *kmax = 0;
   *count = 0;
   Timer tm(c);
+  // Verbose: host time of each stage boundary since the solve began.
+  const auto t_solve = std::chrono::steady_clock::now();
+  auto mark = [&](const char* what) {
+    KT_LOG(c, "kt: +%.2f ms %s\n",
+           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_solve).count(), what);
+  };
+  mark("solve start");
   tm.start();
   KCore kc;
   kc.init(c, g);
@@ -135,6 +142,7 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   const uint32_t cmax = kc.find_max_core(c);
   st.cmax = cmax;
   st.ms_kcore += tm.stop();
+  mark("maximum core found");
   if (g.m == 0 || cmax < 2) return;  // a triangle needs three vertices of degree >= 2
 
   // One phase when the maximum core is a large part of the graph (the
@@ -174,13 +182,16 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     st.predict_vertices = s1.n;
     st.predict_edges = s1.m;
     st.ms_subgraph += tm.stop();
+    mark("prediction subgraph built");
     tm.start();
     DBuf sup1(c, (s1.m ? s1.m : 1) * sizeof(uint32_t));
     edge_support(c, s1, sup1.as<uint32_t>());
     st.ms_support += tm.stop();
+    mark("prediction support counted");
     tm.start();
     const PeelResult p1 = predict_peel(c, s1, sup1.as<uint32_t>(), cmax);
     st.ms_peel += tm.stop();
+    mark("prediction peeled");
     st.levels += p1.levels;
     st.rounds += (uint32_t)p1.rounds;
     L = p1.kmax;
@@ -196,12 +207,14 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   tm.start();
   kc.restore_core(c, L >= 3 ? L - 1 : 2);
   st.ms_kcore += tm.stop();
+  mark("search core restored");
   tm.start();
   Sub s2;
   build_sub(c, g, kc, s2);
   st.core_vertices = s2.n;
   st.core_edges = s2.m;
   st.ms_subgraph += tm.stop();
+  mark("search subgraph built");
   tm.start();
   DBuf sup2(c, (s2.m ? s2.m : 1) * sizeof(uint32_t));
   // The search peel starts at level max(L, 3) with no jump, so supports
@@ -233,9 +246,11 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     }
   }
   st.ms_support += tm.stop();
+  mark("search support counted");
   tm.start();
   const PeelResult p2 = truss_peel(c, *sp, supp, t2, L >= 3 ? C : 0, nullptr);
   st.ms_peel += tm.stop();
+  mark("search peeled");
   st.levels += p2.levels;
   st.rounds += (uint32_t)p2.rounds;
   *kmax = p2.kmax;
