@@ -96,9 +96,12 @@ const char* kt_status_string(kt_status s);
  *                               requests whose estimated footprint is at most this
  *                               many MB, the other lanes any (0: every lane any)
  *   batch_lanes (2)             batch: waves in flight at once, 1..2
- *   support_rows (4)            dense support: edges sharing row u counted together
- *                               per shared-memory read of it (1, 2 or 4; the capped
- *                               kernel of the search phase at most 2) */
+ *   support_rows (2)            exact dense support: edges sharing row u counted
+ *                               together per shared-memory read of it (1, 2 or 4)
+ *   peel_bisect_after (8)       peel: truss levels climbed one at a time before the
+ *                               rest is found by bisection (0 = never) ...
+ *   peel_bisect_gap (16)        ... when the support bound of the alive edges is at
+ *                               least this many levels above (>= 1) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 

@@ -9,10 +9,12 @@
 // A warp takes 32 consecutive edges of a list.  Each lane fetches one edge's
 // ends, then the warp walks the 32 edges: row u is copied into the warp's
 // slice of shared memory (W words) and reused while consecutive edges share
-// u (the lists are tile-ordered by (u block, v block, u, v)); up to four
-// edges that share row u are counted together, each lane reading a vector
-// of row u from shared memory once and ANDing it with the same vector of the
-// four rows v, which stream from L2 with every lane on consecutive vectors.
+// u (the lists are tile-ordered by (u block, v block, u, v)); for exact
+// counts up to four edges that share row u are counted together, each lane
+// reading a vector of row u from shared memory once and ANDing it with the
+// same vector of each row v, which stream from L2 with every lane on
+// consecutive vectors; capped counts run two edges that share row u side by
+// side, one per half of the warp.
 // Keeping row u in shared memory rather than registers leaves the kernels at
 // few registers, so many warps hide the L2 latency.  Lane j keeps the count
 // of the j-th edge, so results are written or pushed once per group.
@@ -65,6 +67,31 @@ __device__ __forceinline__ void dense_load_row(const uint32_t* __restrict__ p, u
 
 __device__ __forceinline__ uint32_t popc_and4(uint4 a, uint4 b) {
   return __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+}
+
+// popcount(row u & row v) over words [w0, w1) (multiples of 4) by one half
+// of the warp (16 lanes, 16-byte vectors); `active` false contributes 0.
+// Every lane of the warp must call it; each lane gets its half's total.
+__device__ __forceinline__ uint32_t half_and_popc(const uint32_t* __restrict__ p, const uint32_t* su, uint32_t w0,
+                                                  uint32_t w1, bool active) {
+  uint32_t s = 0;
+  if (active) {
+    const uint4* p4 = reinterpret_cast<const uint4*>(p);
+    const uint4* s4 = reinterpret_cast<const uint4*>(su);
+    uint32_t i = w0 / 4 + (lane_id() & 15);
+    const uint32_t e = w1 / 4;
+    for (; i + 3 * 16 < e; i += 4 * 16) {
+      uint4 a[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = __ldcg(p4 + i + 16 * k);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += popc_and4(s4[i + 16 * k], a[k]);
+    }
+    for (; i < e; i += 16) s += popc_and4(s4[i], __ldcg(p4 + i));
+  }
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+  return s;
 }
 
 // popcount(row u & row v_q) over the 16-byte vectors [i0, i1) of up to NQ
@@ -196,7 +223,8 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 // count so far plus the set bits left in row u bounds the result.  An
 // abandoned edge reports a count below the threshold (not its support).  The
 // threshold is `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
-template <int NQ = 4>
+// Two edges that share row u run side by side, one per half of the warp (two
+// load streams per warp).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
                                                    const uint64_t* __restrict__ ends, const DenseRows& R,
                                                    uint32_t thr, uint32_t* su, uint32_t& my_e, uint32_t& my_s,
@@ -245,41 +273,45 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       s3 = warp_sum(d);
       if (wr && l == 0) *wr += W;
     }
-    // Up to NQ edges sharing row u, segment by segment; an edge leaves once
-    // its count so far plus row u's set bits in the later segments cannot
-    // reach its threshold.
-    int jq[NQ];
-    uint32_t vq[NQ], tq[NQ], found[NQ], cs[NQ];
-    bool go[NQ], in[NQ];
-    take_same_row<NQ>(todo, u, v, uj, j, vj, jq, vq, in);
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      tq[q] = __shfl_sync(kFull, my_thr, in[q] ? jq[q] : j);
-      go[q] = in[q];
-      found[q] = 0;
-    }
-    uint32_t wds = 0;
-#pragma unroll 1
-    for (int sg = 0; sg < 4; ++sg) {
-      const uint32_t b0 = sg == 0 ? 0u : sg == 1 ? c1 : sg == 2 ? c2 : c3;
-      const uint32_t b1 = sg == 0 ? c1 : sg == 1 ? c2 : sg == 2 ? c3 : W;
-      const uint32_t rest = sg == 0 ? s1 + s2 + s3 : sg == 1 ? s2 + s3 : sg == 2 ? s3 : 0u;
-      bool any = false;
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) any |= go[q];
-      if (!any) break;
-      rows_and_popc<NQ>(R, vq, go, su, b0 / 4, b1 / 4, cs);
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        wds += go[q] ? b1 - b0 : 0u;
-        found[q] += cs[q];
-        go[q] = go[q] && found[q] + rest >= tq[q];
+    // The next edge with the same row u goes to the upper half of the warp:
+    // two edges' segments are ANDed side by side (two load streams).
+    int j2 = -1;
+    uint32_t vj2 = 0;
+    if (todo) {
+      const int cand = __ffs(todo) - 1;
+      const uint32_t uc = __shfl_sync(kFull, u, cand), vc = __shfl_sync(kFull, v, cand);
+      if (uc == uj) {
+        j2 = cand;
+        vj2 = vc;
+        todo &= todo - 1;
       }
     }
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-      if (in[q] && l == (unsigned)jq[q]) my_s = found[q];
-    if (wr && l == 0) *wr += wds;
+    const bool upper = l >= 16;
+    const uint32_t tj = __shfl_sync(kFull, my_thr, j), tj2 = __shfl_sync(kFull, my_thr, j2 >= 0 ? j2 : j);
+    const uint32_t t = upper ? tj2 : tj;
+    bool go = !upper || j2 >= 0;
+    const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
+    uint32_t wds = go ? c1 : 0u;  // row-v words this half reads
+    uint32_t found = half_and_popc(pv, su, 0, c1, go);
+    go = go && found + s1 + s2 + s3 >= t;
+    if (__any_sync(kFull, go)) {
+      wds += go ? c2 - c1 : 0u;
+      found += half_and_popc(pv, su, c1, c2, go);
+      go = go && found + s2 + s3 >= t;
+      if (__any_sync(kFull, go)) {
+        wds += go ? c3 - c2 : 0u;
+        found += half_and_popc(pv, su, c2, c3, go);
+        go = go && found + s3 >= t;
+        if (__any_sync(kFull, go)) {
+          wds += go ? W - c3 : 0u;
+          found += half_and_popc(pv, su, c3, W, go);
+        }
+      }
+    }
+    const uint32_t f0 = __shfl_sync(kFull, found, 0), f1 = __shfl_sync(kFull, found, 16);
+    if (l == (unsigned)j) my_s = f0;
+    if (j2 >= 0 && l == (unsigned)j2) my_s = f1;
+    if (wr && (l & 15u) == 0) *wr += wds;
   }
   __syncwarp();
 }

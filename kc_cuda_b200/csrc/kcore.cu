@@ -422,9 +422,10 @@ struct ProbeArgs {
   uint64_t n_alive;
   uint32_t* front[2];
   uint32_t* big;
-  unsigned long long* cnt;  // [0..2] frontier sizes, [3..4] big-row counts, [5] rounds, [6] removed
+  unsigned long long* cnt;  // [0..2] frontier sizes, [3..4] big-row counts, [5] rounds, [6] removed, [7] stopped
   uint64_t cap;
   uint32_t k, tag;
+  bool may_stop;     // stop once fewer than k+1 vertices can remain (the k-core is then empty)
   uint32_t big_row;  // rows longer than this are dealt to all warps in windows
   DevWords* words;
   unsigned long long timeout_ns;
@@ -471,10 +472,16 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
   if (!grid_barrier(A.words, A.timeout_ns)) return;
   uint32_t i = 0;
   uint64_t removed = 0;
+  bool stopped = false;
   while (true) {
     const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
     if (nf == 0) break;
     removed += nf;
+    // Every block reads the same counts, so all of them stop together.
+    if (A.may_stop && A.n_alive - removed < (uint64_t)A.k + 1) {
+      stopped = true;
+      break;
+    }
     const uint32_t* fr = A.front[i & 1];
     uint32_t* nx = A.front[(i + 1) & 1];
     unsigned long long* nc = &A.cnt[(i + 1) % 3];
@@ -511,6 +518,7 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
   if (gtid == 0) {
     A.cnt[5] = i;
     A.cnt[6] = removed;
+    A.cnt[7] = stopped;
   }
 }
 
@@ -838,7 +846,7 @@ void KCore::recount(Ctx* c) {
   KT_LAUNCHED(c);
 }
 
-uint64_t KCore::probe(Ctx* c, uint32_t k) {
+uint64_t KCore::probe(Ctx* c, uint32_t k, bool may_stop) {
   const uint32_t tag = (uint32_t)levels.size();
   if (tag >= 0xfffffff0u) throw Error(KT_ERR_LIMIT, "k-core: too many probes");
   levels.push_back(k);
@@ -863,6 +871,7 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
     A.cap = n;
     A.k = k;
     A.tag = tag;
+    A.may_stop = may_stop;
     A.big_row = big_row(c);
     A.words = dev_words(c);
     A.timeout_ns = (unsigned long long)c->opt.timeout_ms * 1000000ULL;
@@ -872,15 +881,15 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
       coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
     }
     void* p[] = {&A};
-    uint64_t h[2];
+    uint64_t h[3];
     {
       CoopLock coop(c);
       KT_CUDA(cudaLaunchCooperativeKernel((const void*)k_probe, dim3(coop_grid), dim3(256), p, 0, c->stream));
       KT_LAUNCHED(c);
-      copy_d2h(c, h, cn + 5, 16);
+      copy_d2h(c, h, cn + 5, 24);
     }
     rounds += h[0];
-    removed = h[1];
+    removed = h[2] ? n_alive : h[1];  // stopped: the k-core is empty (the state is partial)
   } else {
     k_frontier_init<<<grid_for(n_alive, 256, c->num_sms * 16), 256, 0, c->stream>>>(
         alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), k, tag, front[0].as<uint32_t>(),
@@ -891,6 +900,10 @@ uint64_t KCore::probe(Ctx* c, uint32_t k) {
       const uint64_t nf = read_word<unsigned long long>(c, cn + cur_f);
       if (nf == 0) break;
       removed += nf;
+      if (may_stop && n_alive - removed < (uint64_t)k + 1) {
+        removed = n_alive;  // the k-core is empty (the state is partial)
+        break;
+      }
       ++rounds;
       KT_CUDA(cudaMemsetAsync(cn + (cur_f ^ 1), 0, sizeof(unsigned long long), c->stream));
       KT_CUDA(cudaMemsetAsync(cn + 4, 0, sizeof(unsigned long long), c->stream));
@@ -923,14 +936,18 @@ uint32_t KCore::find_max_core(Ctx* c) {
   ub = std::min<uint64_t>(ub, base->max_deg);
   uint64_t lo = 1, hi = ub + 1;  // the 1-core (non-isolated vertices) is non-empty
   bool ramp = true;
-  DBuf mn(c, 4);
+  DBuf mn(c, 4), snap;
   while (hi - lo > 1) {
     uint64_t k = ramp ? std::min<uint64_t>(lo * 2, hi - 1) : lo + (hi - lo) / 2;
     if (k <= lo) k = lo + 1;
     const uint32_t tag = (uint32_t)levels.size();
     const auto t0 = std::chrono::steady_clock::now();
     const uint64_t before = n_alive;
-    const uint64_t left = probe(c, (uint32_t)k);
+    // Degrees before the probe: a failed probe is undone by reviving its tag
+    // and copying them back (the alive set is then the one they belong to).
+    snap.ensure(c, n * sizeof(uint32_t));
+    KT_CUDA(cudaMemcpyAsync(snap.get(), deg.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+    const uint64_t left = probe(c, (uint32_t)k, true);
     KT_LOG(c, "kt: k-core probe %llu: %llu of %llu alive vertices left, %.3f ms\n", (unsigned long long)k,
            (unsigned long long)left, (unsigned long long)before,
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
@@ -954,11 +971,11 @@ uint32_t KCore::find_max_core(Ctx* c) {
     } else {
       hi = k;
       ramp = false;
-      // Undo: revive this probe's vertices and recount their degrees.
+      // Undo: revive this probe's vertices and restore their degrees.
       k_revive<<<grid_for(n, 256, c->num_sms * 16), 256, 0, c->stream>>>(rem.as<uint32_t>(), n, tag - 1);
       KT_LAUNCHED(c);
       levels.pop_back();
-      recount(c);
+      KT_CUDA(cudaMemcpyAsync(deg.get(), snap.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
     }
   }
   cmax = (uint32_t)lo;

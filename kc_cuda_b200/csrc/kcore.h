@@ -33,8 +33,10 @@ struct KCore {
   void init(Ctx* c, const Graph& gr);
   void rebuild_alive(Ctx* c);
   void recount(Ctx* c);
-  // Peels the alive set to its k-core; returns the vertices left.
-  uint64_t probe(Ctx* c, uint32_t k);
+  // Peels the alive set to its k-core; returns the vertices left.  may_stop:
+  // the peel may stop once fewer than k+1 vertices can remain, returning 0
+  // with the state partial (the caller then undoes the probe).
+  uint64_t probe(Ctx* c, uint32_t k, bool may_stop = false);
   // Leaves the alive set at the maximum core; returns its k.
   uint32_t find_max_core(Ctx* c);
   // Leaves the alive set at the k-core (k <= cmax after find_max_core).

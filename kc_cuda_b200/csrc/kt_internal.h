@@ -66,7 +66,9 @@ struct Options {
   int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)
   int64_t serve_small_mb = 128;   // serving, two or more lanes: lane 0 admits only requests this small (0: any)
   int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
-  int64_t support_rows = 4;       // dense support: edges sharing row u counted per read of it (1, 2, 4)
+  int64_t support_rows = 2;       // exact dense support: edges sharing row u counted per read of it (1, 2, 4)
+  int64_t peel_bisect_after = 8;  // peel: truss levels climbed one at a time before bisecting the rest (0 = never)
+  int64_t peel_bisect_gap = 16;   // peel: ... when the support bound is at least this far above
 };
 
 // Range check of an option value: every option is a count, size, ratio or

@@ -841,6 +841,52 @@ struct Peeler {
     return true;
   }
 
+  // Finds the top level by bisection, between lo (the current state is the
+  // lo-truss, non-empty) and hi (the hi-truss is empty): a level whose truss
+  // is empty is undone from a snapshot of the state (supports, edge states,
+  // alive degrees, bitsets; the alive list of the snapshot stays in the
+  // other buffer), a non-empty one is kept.  A t-truss is non-empty exactly
+  // for t <= kmax, so this ends with res at kmax and its edge count.
+  void bisect(uint32_t lo, uint32_t hi, PeelResult& out) {
+    DBuf ssup(c, s->m * sizeof(uint32_t)), sstate(c, s->m * sizeof(uint32_t)), sdeg(c, adeg.bytes()), sbits;
+    if (s->W) sbits.alloc(c, s->bits.bytes());
+    uint64_t na0 = 0;
+    int ai0 = 0;
+    auto copy = [&](void* dst, const void* src, size_t bytes) {
+      KT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    };
+    auto save = [&] {
+      copy(ssup.get(), sup, s->m * sizeof(uint32_t));
+      copy(sstate.get(), state.get(), s->m * sizeof(uint32_t));
+      copy(sdeg.get(), adeg.get(), adeg.bytes());
+      if (s->W) copy(sbits.get(), s->bits.get(), s->bits.bytes());
+      na0 = na;
+      ai0 = ai;
+    };
+    save();
+    while (hi - lo > 1) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      const uint64_t left = cascade(mid);
+      if (left) {
+        uint32_t mn, mx;
+        minmax(mn, mx);
+        lo = mn + 2;  // >= mid
+        out.kmax = lo;
+        out.count = left;
+        if (hi - lo > 1) save();
+      } else {
+        copy(sup, ssup.get(), s->m * sizeof(uint32_t));
+        copy(state.get(), sstate.get(), s->m * sizeof(uint32_t));
+        copy(adeg.get(), sdeg.get(), adeg.bytes());
+        if (s->W) copy(s->bits.get(), sbits.get(), s->bits.bytes());
+        na = na0;
+        ai = ai0;
+        hi = mid;
+      }
+    }
+    KT_LOG(c, "kt: bisection ends at level %u with %llu edges\n", out.kmax, (unsigned long long)out.count);
+  }
+
   // (min, max) support over alive edges.
   void minmax(uint32_t& mn, uint32_t& mx) {
     const uint32_t init[2] = {0xffffffffu, 0u};
@@ -929,7 +975,13 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
       stop_count = 0;
     }
   }
+  // Levels climbed one at a time before a long climb turns into a bisection
+  // (peel_bisect_after, 0 = never), and the gap to the support bound that
+  // makes it one (peel_bisect_gap).
+  const uint64_t bisect_after = (uint64_t)std::max<int64_t>(0, c->opt.peel_bisect_after);
+  const uint64_t bisect_gap = (uint64_t)std::max<int64_t>(1, c->opt.peel_bisect_gap);
   bool first = true;
+  uint32_t climbed = 0;
   while (true) {
     const uint64_t left = P.cascade(t);
     if (left == 0) break;
@@ -947,6 +999,16 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
     res.count = left;
     t = mn + 3;
     P.compact_graph(own, own_sup);
+    if (!truss && bisect_after && ++climbed == bisect_after) {
+      // No level above the support bound of the alive edges is non-empty
+      // (removed edges keep supports below the current level's threshold).
+      const uint32_t ub = support_bound(c, P.sup, P.s->m, mx + 2);
+      if (ub >= t + bisect_gap) {
+        KT_LOG(c, "kt: level %u, support bound %u: bisecting\n", t, ub);
+        P.bisect(res.kmax, ub + 1, res);
+        break;
+      }
+    }
   }
   if (res.kmax < 3) {
     res.kmax = 0;

@@ -152,23 +152,24 @@ __global__ void k_group_rows(uint32_t n, const uint32_t* __restrict__ vgid, cons
   }
 }
 
-// Four resident blocks per SM (what the rows' shared memory allows for the
+// Warps take 32-edge groups from a cursor, so the groups in flight stay a
+// narrow window of the tile-ordered list (a grid-stride loop lets warps drift
+// apart, and the rows they read then no longer fit in L2).  `row_words`
+// accumulates the row words read.
+//
+// Exact counts, up to NQ edges sharing row u per shared-memory read of it;
+// four resident blocks per SM (what the rows' shared memory allows for the
 // bench graph's cores) bound the registers to 64.
-template <bool kCapped, int NQ>
+template <int NQ>
 __global__ void __launch_bounds__(256, 4) k_dense_support(uint64_t m, const uint32_t* __restrict__ order,
-                                                       const uint64_t* __restrict__ ends, DenseRows R, uint32_t cap,
-                                                       const uint32_t* __restrict__ gcap,
-                                                       const uint32_t* __restrict__ vgid,
-                                                       uint32_t* __restrict__ sup,
-                                                       unsigned long long* __restrict__ row_words,
-                                                       unsigned long long* __restrict__ cursor) {
+                                                          const uint64_t* __restrict__ ends, DenseRows R,
+                                                          uint32_t* __restrict__ sup,
+                                                          unsigned long long* __restrict__ row_words,
+                                                          unsigned long long* __restrict__ cursor) {
   extern __shared__ __align__(16) uint32_t dense_smem[];
   uint32_t* su = dense_smem + warp_id() * R.W;
   const uint64_t groups = (m + 31) / 32;
-  unsigned long long wr = 0;  // row words this lane accounts for (one or two lanes per warp)
-  // Warps take the next 32-edge group from a cursor, so the groups in flight
-  // stay a narrow window of the tile-ordered list (a grid-stride loop lets
-  // warps drift apart, and the rows they read then no longer fit in L2).
+  unsigned long long wr = 0;  // row words this lane accounts for (lane 0)
   for (;;) {
     unsigned long long g = 0;
     if (lane_id() == 0) g = atomicAdd(cursor, 1ULL);
@@ -176,10 +177,34 @@ __global__ void __launch_bounds__(256, 4) k_dense_support(uint64_t m, const uint
     if (g >= groups) break;
     uint32_t e, s;
     bool ok;
-    if (kCapped)
-      dense_group_capped<NQ>(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr, gcap, vgid);
-    else
-      dense_group<NQ>(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
+    dense_group<NQ>(order, g * 32, m, ends, R, nullptr, su, e, s, ok, &wr);
+    if (ok) sup[e] = s;
+  }
+  wr = warp_sum(wr);
+  if (lane_id() == 0 && wr) atomicAdd(row_words, wr);
+}
+
+// Capped counts (search phase): threshold `cap`, or gcap[vgid[u]] per graph
+// of a grouped union.
+__global__ void __launch_bounds__(256) k_dense_support_capped(uint64_t m, const uint32_t* __restrict__ order,
+                                                              const uint64_t* __restrict__ ends, DenseRows R,
+                                                              uint32_t cap, const uint32_t* __restrict__ gcap,
+                                                              const uint32_t* __restrict__ vgid,
+                                                              uint32_t* __restrict__ sup,
+                                                              unsigned long long* __restrict__ row_words,
+                                                              unsigned long long* __restrict__ cursor) {
+  extern __shared__ __align__(16) uint32_t dense_smem[];
+  uint32_t* su = dense_smem + warp_id() * R.W;
+  const uint64_t groups = (m + 31) / 32;
+  unsigned long long wr = 0;  // row words this lane accounts for (lanes 0 and 16)
+  for (;;) {
+    unsigned long long g = 0;
+    if (lane_id() == 0) g = atomicAdd(cursor, 1ULL);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= groups) break;
+    uint32_t e, s;
+    bool ok;
+    dense_group_capped(order, g * 32, m, ends, R, cap, su, e, s, ok, &wr, gcap, vgid);
     if (ok) sup[e] = s;
   }
   wr = warp_sum(wr);
@@ -196,36 +221,42 @@ __global__ void k_tile_keys(uint64_t m, const uint64_t* __restrict__ ends, uint3
   }
 }
 
-template <bool kCapped, int NQ>
-void launch_dense_support_n(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
-                            unsigned long long* row_words, unsigned long long* cursor) {
-  const size_t smem = dense_smem_bytes(s.W, 256);
-  allow_max_dynamic_smem((const void*)k_dense_support<kCapped, NQ>);
+// Grid of the resident blocks of `kernel` with the rows' shared memory.
+unsigned dense_grid(Ctx* c, const void* kernel, const Sub& s, size_t smem) {
+  allow_max_dynamic_smem(kernel);
   int per_sm = 0;
-  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_support<kCapped, NQ>, 256, smem));
-  const unsigned grid = grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
-  k_dense_support<kCapped, NQ><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
-                                                           dense_rows(s), cap, gcap,
-                                                           gcap ? s.vgid.as<uint32_t>() : nullptr, sup, row_words,
-                                                           cursor);
+  KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
+  return grid_for((s.m + 31) / 32 * 32, 256, std::max(1, per_sm) * c->num_sms);
+}
+
+template <int NQ>
+void launch_exact(Ctx* c, const Sub& s, uint32_t* sup, unsigned long long* row_words, unsigned long long* cursor) {
+  const size_t smem = dense_smem_bytes(s.W, 256);
+  const unsigned grid = dense_grid(c, (const void*)k_dense_support<NQ>, s, smem);
+  k_dense_support<NQ><<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+                                                      dense_rows(s), sup, row_words, cursor);
   KT_LAUNCHED(c);
 }
 
-// Edges sharing row u counted together: option support_rows (1, 2 or 4);
-// the capped kernel, whose segment state takes more registers, counts at
-// most two together.
-template <bool kCapped>
-void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint32_t* gcap,
+// Exact counts: option support_rows (1, 2 or 4) edges sharing row u per
+// shared-memory read of it.  Capped counts: two edges sharing row u side by
+// side, one per half of the warp.
+void launch_dense_support(Ctx* c, const Sub& s, uint32_t* sup, bool capped, uint32_t cap, const uint32_t* gcap,
                           unsigned long long* row_words, unsigned long long* cursor) {
-  if (c->opt.support_rows <= 1) {
-    launch_dense_support_n<kCapped, 1>(c, s, sup, cap, gcap, row_words, cursor);
-  } else if constexpr (kCapped) {
-    launch_dense_support_n<kCapped, 2>(c, s, sup, cap, gcap, row_words, cursor);
+  if (capped) {
+    const size_t smem = dense_smem_bytes(s.W, 256);
+    const unsigned grid = dense_grid(c, (const void*)k_dense_support_capped, s, smem);
+    k_dense_support_capped<<<grid, 256, smem, c->stream>>>(s.m, s.order.as<uint32_t>(), s.ends.as<uint64_t>(),
+                                                           dense_rows(s), cap, gcap,
+                                                           gcap ? s.vgid.as<uint32_t>() : nullptr, sup, row_words,
+                                                           cursor);
+    KT_LAUNCHED(c);
+  } else if (c->opt.support_rows <= 1) {
+    launch_exact<1>(c, s, sup, row_words, cursor);
+  } else if (c->opt.support_rows == 2) {
+    launch_exact<2>(c, s, sup, row_words, cursor);
   } else {
-    if (c->opt.support_rows == 2)
-      launch_dense_support_n<kCapped, 2>(c, s, sup, cap, gcap, row_words, cursor);
-    else
-      launch_dense_support_n<kCapped, 4>(c, s, sup, cap, gcap, row_words, cursor);
+    launch_exact<4>(c, s, sup, row_words, cursor);
   }
 }
 
@@ -366,10 +397,8 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint3
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
     unsigned long long* a = acc.as<unsigned long long>();
-    if (cap || (gcap && s.vgid.get()))
-      launch_dense_support<true>(c, s, sup, cap, s.vgid.get() ? gcap : nullptr, a + 1, a + 2);
-    else
-      launch_dense_support<false>(c, s, sup, 0, nullptr, a + 1, a + 2);
+    const bool capped = cap || (gcap && s.vgid.get());
+    launch_dense_support(c, s, sup, capped, cap, s.vgid.get() ? gcap : nullptr, a + 1, a + 2);
   } else if ((int64_t)(s.vbase.get() ? s.max_group : s.n) <= c->opt.support_bitmap_max_n) {
     const uint32_t range = s.vbase.get() ? s.max_group : s.n;
     const size_t smem = ((range + 31) / 32) * sizeof(uint32_t);

@@ -244,17 +244,21 @@ def test_without_prediction_same_answer(ctx, golden):
 
 
 @pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never", "dense_uncapped",
-                                  "dense_merge_only", "dense_split_always"])
+                                  "dense_merge_only", "dense_split_always", "bisect_always_sparse",
+                                  "bisect_always_dense"])
 def test_modes_support_trussness_answer(ctx, golden, mode):
     """Sparse lists vs dense bitsets, dense peels that recount every round vs
-    never, and dense peels that intersect sorted lists instead of bitset
-    rows: all bit-identical to the oracle."""
+    never, dense peels that intersect sorted lists instead of bitset rows, and
+    peels that bisect the truss levels after the first one (undoing empty
+    levels from a snapshot): all bit-identical to the oracle."""
     opts = {"sparse": {"dense_max_n": 0},
             "dense_recount_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1 << 30},
             "dense_recount_never": {"dense_min_fill": 1 << 30, "recount_gamma": 1},
             "dense_uncapped": {"dense_min_fill": 1 << 30, "capped_support": 0},
             "dense_merge_only": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_bitset": 0},
-            "dense_split_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_split": 1 << 20}}[mode]
+            "dense_split_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1, "peel_split": 1 << 20},
+            "bisect_always_sparse": {"dense_max_n": 0, "peel_bisect_after": 1, "peel_bisect_gap": 1},
+            "bisect_always_dense": {"dense_min_fill": 1 << 30, "peel_bisect_after": 1, "peel_bisect_gap": 1}}[mode]
     old = {k: ctx.get_option(k) for k in opts}
     for k, v in opts.items():
         ctx.set_option(k, v)
