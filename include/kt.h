@@ -92,16 +92,18 @@ const char* kt_status_string(kt_status s);
  *                               chunks <= this x warps deals (edge, chunk) units
  *                               to warps instead of edges (0 = off)
  *   serve_lanes (2)             serving: waves in flight at once, 1..4
- *   serve_small_mb (128)        serving with two or more lanes: lane 0 admits only
- *                               requests whose estimated footprint is at most this
- *                               many MB, the other lanes any (0: every lane any)
+ *   serve_small_mb (128)        serving with two or more lanes: the last lane admits
+ *                               only requests whose estimated footprint is at most
+ *                               this many MB, the other lanes any (0: every lane any)
  *   batch_lanes (2)             batch: waves in flight at once, 1..2
  *   support_rows (2)            exact dense support: edges sharing row u counted
  *                               together per shared-memory read of it (1, 2 or 4)
- *   peel_bisect_after (8)       peel: truss levels climbed one at a time before the
+ *   peel_bisect_after (16)      peel: truss levels climbed one at a time before the
  *                               rest is found by bisection (0 = never) ...
  *   peel_bisect_gap (16)        ... when the support bound of the alive edges is at
- *                               least this many levels above (>= 1) */
+ *                               least this many levels above (>= 1)
+ *   coop_occupancy_pct (100)    cooperative launches use this % of the blocks the
+ *                               device can hold at once (1..100) */
 kt_status kt_set_option(kt_ctx* ctx, const char* name, int64_t value);
 kt_status kt_get_option(const kt_ctx* ctx, const char* name, int64_t* value);
 
@@ -217,8 +219,11 @@ kt_status kt_options_load(kt_ctx* ctx, const char* path);
  * max_wave_graphs of them, 0 = 65535) and solves them as one wave of the
  * batch path on its own stream; requests that arrive while waves run start in
  * the next free lane, so waves overlap on the device.  With two or more lanes,
- * lane 0 takes only small requests (serve_small_mb), oldest first, so they
- * never wait behind a wave of large graphs.  A request's answer is
+ * the last lane takes only small requests (serve_small_mb), oldest first, so they
+ * never wait behind a wave of large graphs: that lane launches nothing
+ * cooperative, and the other lanes' cooperative launches take 75% of the
+ * device's resident blocks (coop_occupancy_pct, restored on the context at
+ * kt_server_destroy), so its waves run beside theirs.  A request's answer is
  * the same alone and in any mix.  Other calls on the context block while a
  * wave of lane 0 runs. */
 typedef struct kt_server kt_server;

@@ -30,6 +30,7 @@ bool option_value_ok(const char* name, int64_t value) {
   if (!std::strcmp(name, "batch_lanes")) return value >= 1 && value <= 2;
   if (!std::strcmp(name, "support_rows")) return value == 1 || value == 2 || value == 4;
   if (!std::strcmp(name, "peel_bisect_gap")) return value >= 1;
+  if (!std::strcmp(name, "coop_occupancy_pct")) return value >= 1 && value <= 100;
   return true;
 }
 
@@ -408,7 +409,8 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"support_rows", &o.support_rows},
              {"serve_small_mb", &o.serve_small_mb},
              {"peel_bisect_after", &o.peel_bisect_after},
-             {"peel_bisect_gap", &o.peel_bisect_gap}};
+             {"peel_bisect_gap", &o.peel_bisect_gap},
+             {"coop_occupancy_pct", &o.coop_occupancy_pct}};
   for (auto& t : tab)
     if (!std::strcmp(t.n, name)) return t.p;
   return nullptr;

@@ -20,6 +20,7 @@
 // (ktgen_core.h), so a device-generated graph equals ktg_make's.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstring>
 #include <exception>
 #include <mutex>
@@ -535,15 +536,24 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
         pending = true;
       }
     const std::vector<uint64_t> nostop(G, 0);
+    uint32_t iter = 0;
     while (pending) {
       std::vector<uint32_t> thr(G, 0);
       for (uint32_t g = 0; g < G; ++g) thr[g] = level[g] ? level[g] - 2 : 0;
       Sub s;
       DBuf sup;
+      const auto t_a = std::chrono::steady_clock::now();
       survivors(c, s1, sup1.as<uint32_t>(), thr, false, s, sup);
+      const auto t_b = std::chrono::steady_clock::now();
       std::vector<uint32_t> km;
       std::vector<uint64_t> cn;
+      const uint32_t lv0 = st.levels, rd0 = st.rounds;
       tracked_peel(c, s, sup.as<uint32_t>(), level, nostop, km, cn);
+      KT_LOG(c, "kt: wave phase 1 class %d pass %u: survivors %llu edges in %.2f ms, tracked peel %u levels %u "
+                "rounds in %.2f ms\n",
+             cls, iter++, (unsigned long long)s.m,
+             std::chrono::duration<double, std::milli>(t_b - t_a).count(), st.levels - lv0, st.rounds - rd0,
+             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_b).count());
       pending = false;
       for (uint32_t g = 0; g < G; ++g) {
         if (!level[g]) continue;
@@ -631,6 +641,8 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     if (!rebuilt && capped) edge_support(c, s2, sup2.as<uint32_t>());  // most edges stay: exact supports
     st.ms_support += tm.stop();
     tm.start();
+    const auto t_p = std::chrono::steady_clock::now();
+    const uint32_t lv0 = st.levels, rd0 = st.rounds;
     std::vector<uint32_t> km;
     std::vector<uint64_t> cn;
     std::vector<uint32_t> t0c(G, 3);
@@ -645,6 +657,9 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
     else
       tracked_peel(c, s2, sup2.as<uint32_t>(), t0c, stopc, km, cn);
     st.ms_peel += tm.stop();
+    KT_LOG(c, "kt: wave phase 2 class %d: %llu edges (%s), tracked peel %u levels %u rounds in %.2f ms\n", cls,
+           (unsigned long long)(rebuilt ? s3.m : s2.m), rebuilt ? "survivors" : "whole cores", st.levels - lv0,
+           st.rounds - rd0, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_p).count());
     for (uint32_t g = 0; g < G; ++g) {
       if (!need[g]) continue;
       items[g]->kmax = km[g] >= 3 ? km[g] : 0;

@@ -878,7 +878,7 @@ uint64_t KCore::probe(Ctx* c, uint32_t k, bool may_stop) {
     if (!coop_grid) {
       int per_sm = 0;
       KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe, 256, 0));
-      coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+      coop_grid = coop_blocks(c, per_sm);
     }
     void* p[] = {&A};
     uint64_t h[3];
@@ -1089,7 +1089,7 @@ void KCore::core_numbers_persistent(Ctx* c, uint32_t* dcore) {
   int per_sm = 0;
   KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_core_levels, 256, 0));
   if (c->opt.kcore_blocks_per_sm > 0) per_sm = (int)std::min<int64_t>(per_sm, c->opt.kcore_blocks_per_sm);
-  const unsigned grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+  const unsigned grid = coop_blocks(c, per_sm);
   void* p[] = {&A};
   uint64_t h[5];
   {

@@ -2,6 +2,7 @@
 // device buffers charged to the context's HBM budget, error propagation and
 // launch accounting.
 #pragma once
+#include <algorithm>
 #include <cstdio>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -67,8 +68,9 @@ struct Options {
   int64_t serve_small_mb = 128;   // serving, two or more lanes: lane 0 admits only requests this small (0: any)
   int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
   int64_t support_rows = 2;       // exact dense support: edges sharing row u counted per read of it (1, 2, 4)
-  int64_t peel_bisect_after = 8;  // peel: truss levels climbed one at a time before bisecting the rest (0 = never)
+  int64_t peel_bisect_after = 16; // peel: truss levels climbed one at a time before bisecting the rest (0 = never)
   int64_t peel_bisect_gap = 16;   // peel: ... when the support bound is at least this far above
+  int64_t coop_occupancy_pct = 100;  // cooperative grids: this % of the resident blocks the device holds
 };
 
 // Range check of an option value: every option is a count, size, ratio or
@@ -238,6 +240,15 @@ uint64_t unique_sorted_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n
 // largest limit once, instead of each launch's own size, keeps launches from
 // two lanes (threads) of one device from lowering each other's limit.
 void allow_max_dynamic_smem(const void* func);
+
+// Grid of a cooperative launch: coop_occupancy_pct of the blocks that can be
+// resident at once (per_sm on each SM), at least one.  Below 100, another
+// lane's kernels keep room on every SM while the launch runs.
+inline unsigned coop_blocks(const Ctx* c, int per_sm) {
+  const int64_t pct = std::min<int64_t>(std::max<int64_t>(1, c->opt.coop_occupancy_pct), 100);
+  const int64_t all = (int64_t)std::max(1, per_sm) * c->num_sms;
+  return (unsigned)std::max<int64_t>(1, all * pct / 100);
+}
 
 // Grid sizing.
 inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap) {

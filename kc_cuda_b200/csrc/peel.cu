@@ -675,7 +675,7 @@ struct Peeler {
       allow_max_dynamic_smem((const void*)k_cascade);
       int per_sm = 0;
       KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade, kPeelThreads, smem));
-      coop_grid = (unsigned)std::max(1, per_sm) * c->num_sms;
+      coop_grid = coop_blocks(c, per_sm);
     }
   }
 

@@ -7,8 +7,11 @@
 // with its own stream, device words and budget.  Whenever a lane is free it
 // admits queued requests, oldest first, while their estimated device
 // footprint fits the lane's share of the budget (and up to a graph cap) --
-// with two or more lanes, lane 0 admits only small requests (footprint up to
-// serve_small_mb), so they never queue behind a wave of large graphs -- and
+// with two or more lanes, the last lane admits only small requests
+// (footprint up to serve_small_mb), so they never queue behind a wave of
+// large graphs; it launches nothing cooperative, and the other lanes'
+// cooperative grids take 75% of the resident blocks, so its waves run beside
+// theirs -- and
 // solves the admitted set as one wave -- one disjoint union through every
 // stage, each graph on its own peel levels (batch.cu).  So while one wave is
 // on the device, requests that arrive meanwhile start in the next free lane
@@ -65,7 +68,8 @@ struct kt_server {
   kt_server_stats st{};
   std::vector<Lane> lanes;
   std::mutex coop;  // cooperative launches of the lanes, one at a time
-  uint64_t small_bytes = 0;  // lane 0 admits only requests of at most this footprint (0: any)
+  uint64_t small_bytes = 0;  // the small lane (the last) admits only requests this small (0: any)
+  int64_t lane0_coop_pct = 100;  // the server's context's coop_occupancy_pct, restored at the end
   bool queue_has_small() const {
     for (const Request* r : queue)
       if (r->footprint <= small_bytes) return true;
@@ -101,10 +105,10 @@ struct kt_server {
         work_cv.wait(lk, [&] { return stopping || !queue.empty(); });
         if (queue.empty()) break;  // stopping and drained
         // Admission: arrival order, while the footprint fits.  With a small
-        // lane (lane 0 of two or more, small_bytes > 0) that lane admits only
+        // lane (the last of two or more, small_bytes > 0) that lane admits only
         // requests of at most small_bytes, skipping larger ones; the other
         // lanes admit any request.
-        const bool small_only = small_bytes && lanes.size() > 1 && lane_ctx == lanes[0].ctx;
+        const bool small_only = small_bytes && lanes.size() > 1 && lane_ctx == lanes.back().ctx;
         uint64_t bytes = 0;
         for (auto it = queue.begin(); it != queue.end() && wave.size() < max_wave;) {
           Request* r = *it;
@@ -208,6 +212,7 @@ struct kt_server {
       } else if (l.ctx) {
         std::lock_guard<std::recursive_mutex> lk(l.ctx->c.mu);
         l.ctx->c.coop_mu = nullptr;
+        l.ctx->c.opt.coop_occupancy_pct = lane0_coop_pct;
       }
       l.ctx = nullptr;
     }
@@ -250,9 +255,23 @@ kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** ou
     }
   }
   if (st == KT_OK && nlanes > 1)
-    for (auto& l : s->lanes) {
-      std::lock_guard<std::recursive_mutex> lk(l.ctx->c.mu);
-      l.ctx->c.coop_mu = &s->coop;
+    for (size_t i = 0; i < s->lanes.size(); ++i) {
+      kt::Ctx& lc = s->lanes[i].ctx->c;
+      std::lock_guard<std::recursive_mutex> lk(lc.mu);
+      lc.coop_mu = &s->coop;
+      if (!s->small_bytes) continue;
+      if (i + 1 == s->lanes.size()) {
+        // The small lane launches nothing cooperative (host-stepped rounds,
+        // list-mode support), so it never waits for another lane's
+        // cooperative grid to end ...
+        lc.opt.persistent = 0;
+        lc.opt.dense_max_n = 0;
+      } else {
+        // ... and the other lanes' cooperative grids leave it room on
+        // every SM.
+        if (i == 0) s->lane0_coop_pct = lc.opt.coop_occupancy_pct;
+        lc.opt.coop_occupancy_pct = 75;
+      }
     }
   try {
     if (st == KT_OK)
