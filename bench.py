@@ -502,6 +502,7 @@ def measure_serve(ctx, args, rank, pg, batched_gps=None):
         "max_ms": summ["max_ms"], "wait_p50_ms": summ["wait_p50_ms"],
         "waves": sst["waves"], "mean_wave_graphs": summ["mean_wave_graphs"],
         "max_wave_graphs": sst["max_wave_graphs"], "device_bytes_peak": sst["device_bytes_peak"],
+        "per_lane": summ["per_lane"],
         "per_graph_same_arrivals": {
             "p50_ms": float(np.percentile(pg_lat, 50)), "p99_ms": float(np.percentile(pg_lat, 99)),
             "service_p50_ms": float(np.percentile(service, 50)),
@@ -517,6 +518,9 @@ def lane_options(ctx, args):
     ctx.set_option("pool_reserve_mb", 1 << 30)
     ctx.set_option("batch_lanes", args.batch_lanes)
     ctx.set_option("serve_lanes", args.serve_lanes)
+    for o in args.option:
+        name, value = o.split("=", 1)
+        ctx.set_option(name, int(value))
 
 
 def progress(name: str, obj) -> None:
@@ -657,12 +661,15 @@ def run_single(args, world, rank, local, pg, threads):
     barrier(pg)
     ctx.reset_stats()
     e2e_s = []
+    e2e_copy_parse_ms = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         got = ctx.solve_tsv(tsv)
         e2e_s.append(time.perf_counter() - t0)
         if got != answer:
             raise SystemExit(f"end-to-end answer differs: {got} vs {answer}")
+        # The pipelined load's parse stage spans the host-to-device copy.
+        e2e_copy_parse_ms.append(ctx.stats()["ms_parse"])
     est = ctx.stats()
     barrier(pg)
     e2e_step = max_over_ranks(pg, sum(e2e_s) / len(e2e_s))
@@ -741,7 +748,12 @@ def run_single(args, world, rank, local, pg, threads):
         line.update({
             "parity": parity,
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": est["h2d_bytes"] // args.steps,
-                    "d2h_bytes_per_step": est["d2h_bytes"] // args.steps, "ms_per_step": 1000 * e2e_step},
+                    "d2h_bytes_per_step": est["d2h_bytes"] // args.steps, "ms_per_step": 1000 * e2e_step,
+                    "step_ms": [round(1000 * x, 1) for x in e2e_s],
+                    "copy_parse_ms": [round(x, 1) for x in e2e_copy_parse_ms],
+                    "copy_gbs": [round(tsv.nbytes / (x / 1000.0) / 1e9, 1) for x in e2e_copy_parse_ms if x > 0],
+                    "copy_note": "copy_parse_ms: the host-to-device copy of the TSV bytes in chunks with each "
+                                 "chunk's parse overlapped (copy-bound); copy_gbs: TSV bytes over it"},
             "gpu_launches": launches,
             "roofline": dict(dominant, note=(
                 "dense support rows are read mostly from L2 (tile order), so frac near 1 of the HBM copy "
@@ -789,6 +801,8 @@ def main():
     ap.add_argument("--calib-graphs", type=int, default=512)
     ap.add_argument("--batch-lanes", type=int, default=2, help="batched: waves in flight at once (1 or 2)")
     ap.add_argument("--serve-lanes", type=int, default=2, help="serving: waves in flight at once (1..4)")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="batched and serving contexts: a solver option to set (repeatable)")
     ap.add_argument("--tune-graphs", type=int, default=128,
                     help="autotune the kernel thresholds on this many other mix graphs first (0: off)")
     args = ap.parse_args()

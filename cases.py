@@ -20,11 +20,13 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
                   degrees capped at 400K, seed 3, a 150-vertex block of pair
                   probability 0.95 (config 3's shape at a fifth of its size).
   chunglu50m-solve  config 3 itself (32 GB of TSV staged on the device).
-  mix-batch       graphs 0..255 of the batched mix in one kt_batch_run
+  mix-batch       graphs 0..255 (--graphs; --max-draws keeps the smaller
+                  ones) of the batched mix in one kt_batch_run
                   (k_core_levels on the union, grouped support and peel).
   mix-largest     the --count largest of mix graphs 0..4095 (by draws) in one
                   kt_batch_run; --alone also solves them one at a time.
---verbose prints the solver's stage decisions and per-level cascades.
+--verbose prints the solver's stage decisions and per-level cascades
+(--verbose-alone: also for the graphs solved one at a time).
 """
 from __future__ import annotations
 
@@ -71,7 +73,8 @@ def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
         t.free()
 
 
-def mix_batch(reps: int, verbose: bool = False, indices=None, options=(), alone: bool = False) -> None:
+def mix_batch(reps: int, verbose: bool = False, indices=None, options=(), alone: bool = False,
+              verbose_alone: bool = False) -> None:
     indices = list(range(256)) if indices is None else indices
     with Context(0) as ctx:
         ctx.set_option("pool_reserve_mb", 1 << 30)
@@ -93,8 +96,7 @@ def mix_batch(reps: int, verbose: bool = False, indices=None, options=(), alone:
                   f"({st['batch_waves']} waves; stage sums: {stages}; support kernel {st['ms_support_kernel']:.1f}, "
                   f"peel kernel {st['ms_peel_kernel']:.1f}, {st['levels']} levels, {st['rounds']} rounds)", flush=True)
         if alone:
-            if verbose:
-                ctx.set_option("verbose", 0)
+            ctx.set_option("verbose", 1 if verbose_alone else 0)
             tot = {x: 0.0 for x in ("ms_parse", "ms_csr", "ms_kcore", "ms_subgraph", "ms_support", "ms_peel",
                                     "ms_total", "ms_support_kernel", "ms_peel_kernel")}
             for i in indices:
@@ -122,7 +124,10 @@ def main() -> None:
     ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve",
                                      "chunglu10m-solve", "chunglu50m-solve", "mix-batch", "mix-largest"])
     ap.add_argument("--count", type=int, default=64, help="mix-largest: how many of the largest graphs")
+    ap.add_argument("--graphs", type=int, default=256, help="mix-batch: graphs 0..N-1")
+    ap.add_argument("--max-draws", type=int, default=0, help="mix-batch: only graphs of at most this many draws")
     ap.add_argument("--alone", action="store_true", help="mix cases: also solve the graphs one at a time")
+    ap.add_argument("--verbose-alone", action="store_true")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
@@ -136,9 +141,12 @@ def main() -> None:
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
     elif a.case == "mix-batch":
-        mix_batch(a.reps, a.verbose, options=opts, alone=a.alone)
+        idx = [i for i in range(a.graphs) if not a.max_draws or gen.mix_graph(i).draws <= a.max_draws]
+        mix_batch(a.reps, a.verbose, indices=idx, options=opts, alone=a.alone,
+                  verbose_alone=a.verbose_alone)
     elif a.case == "mix-largest":
-        mix_batch(a.reps, a.verbose, indices=largest_mix(a.count), options=opts, alone=a.alone)
+        mix_batch(a.reps, a.verbose, indices=largest_mix(a.count), options=opts, alone=a.alone,
+                  verbose_alone=a.verbose_alone)
     elif a.case == "rmat24-solve":
         solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
     elif a.case == "chunglu10m-solve":

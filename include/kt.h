@@ -95,6 +95,10 @@ const char* kt_status_string(kt_status s);
  *   serve_small_mb (128)        serving with two or more lanes: the last lane admits
  *                               only requests whose estimated footprint is at most
  *                               this many MB, the other lanes any (0: every lane any)
+ *   serve_small_coop (0)        the small lane's k-core and peel rounds: 0 = host-
+ *                               stepped (no cooperative launch, so it never waits for
+ *                               another lane's), 1 = cooperative launches taking turns
+ *                               with the other lanes'
  *   batch_lanes (2)             batch: waves in flight at once, 1..2
  *   support_rows (2)            exact dense support: edges sharing row u counted
  *                               together per shared-memory read of it (1, 2 or 4)

@@ -30,6 +30,7 @@ bool option_value_ok(const char* name, int64_t value) {
   if (!std::strcmp(name, "batch_lanes")) return value >= 1 && value <= 2;
   if (!std::strcmp(name, "support_rows")) return value == 1 || value == 2 || value == 4;
   if (!std::strcmp(name, "peel_bisect_gap")) return value >= 1;
+  if (!std::strcmp(name, "serve_small_coop")) return value == 0 || value == 1;
   if (!std::strcmp(name, "coop_occupancy_pct")) return value >= 1 && value <= 100;
   return true;
 }
@@ -408,6 +409,7 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"batch_lanes", &o.batch_lanes},
              {"support_rows", &o.support_rows},
              {"serve_small_mb", &o.serve_small_mb},
+             {"serve_small_coop", &o.serve_small_coop},
              {"peel_bisect_after", &o.peel_bisect_after},
              {"peel_bisect_gap", &o.peel_bisect_gap},
              {"coop_occupancy_pct", &o.coop_occupancy_pct}};

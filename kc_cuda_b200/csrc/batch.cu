@@ -449,6 +449,24 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
   build_graph(c, keys.as<uint64_t>(), nkeys, nv, U);
   keys.release();
   st.ms_csr += tm.stop();
+  if (G == 1) {
+    // A wave of one graph takes the single-graph driver: k-core probes
+    // instead of the union's full decomposition, and none of the per-graph
+    // bookkeeping of a union.  Its per-solve figures add to the batch's.
+    const kt_stats before = st;
+    solve_graph_inner(c, U, &items[0]->kmax, &items[0]->count);
+    st.core_vertices += before.core_vertices;
+    st.core_edges += before.core_edges;
+    st.predict_vertices += before.predict_vertices;
+    st.predict_edges += before.predict_edges;
+    st.cmax = before.cmax;
+    st.kmax_lower_bound = before.kmax_lower_bound;
+    if (items[0]->kmax < 3) {
+      items[0]->kmax = 0;
+      items[0]->count = 0;
+    }
+    return;
+  }
   // Core numbers of the union and each graph's maximum core.
   tm.start();
   DBuf dcore(c, (nv ? nv : 1) * sizeof(uint32_t));

@@ -26,7 +26,6 @@ struct BatchRun {
   uint32_t waves = 0;
 };
 
-float event_ms(cudaEvent_t a, cudaEvent_t b);
 void solve_wave(Ctx* c, const std::vector<BatchItem*>& items);
 void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out);
 // Graph `index` of the batched mix, generated on the device.

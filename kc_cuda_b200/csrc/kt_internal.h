@@ -65,7 +65,8 @@ struct Options {
   int64_t wave_budget_pct = 50;   // batch: a wave's estimated footprint within this % of the free budget
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
   int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)
-  int64_t serve_small_mb = 128;   // serving, two or more lanes: lane 0 admits only requests this small (0: any)
+  int64_t serve_small_mb = 128;   // serving, two or more lanes: the last lane admits only requests this small (0: any)
+  int64_t serve_small_coop = 0;   // serving: the small lane's kernels cooperative (1) or host-stepped (0)
   int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
   int64_t support_rows = 2;       // exact dense support: edges sharing row u counted per read of it (1, 2, 4)
   int64_t peel_bisect_after = 16; // peel: truss levels climbed one at a time before bisecting the rest (0 = never)
@@ -240,6 +241,9 @@ uint64_t unique_sorted_u64(Ctx* c, const uint64_t* in, uint64_t* out, uint64_t n
 // largest limit once, instead of each launch's own size, keeps launches from
 // two lanes (threads) of one device from lowering each other's limit.
 void allow_max_dynamic_smem(const void* func);
+
+// Milliseconds between two recorded events (waits for the second).
+float event_ms(cudaEvent_t a, cudaEvent_t b);
 
 // Grid of a cooperative launch: coop_occupancy_pct of the blocks that can be
 // resident at once (per_sm on each SM), at least one.  Below 100, another

@@ -259,7 +259,7 @@ kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** ou
       kt::Ctx& lc = s->lanes[i].ctx->c;
       std::lock_guard<std::recursive_mutex> lk(lc.mu);
       lc.coop_mu = &s->coop;
-      if (!s->small_bytes) continue;
+      if (!s->small_bytes || opt.serve_small_coop) continue;
       if (i + 1 == s->lanes.size()) {
         // The small lane launches nothing cooperative (host-stepped rounds,
         // list-mode support), so it never waits for another lane's

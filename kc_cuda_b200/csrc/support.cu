@@ -394,6 +394,7 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint3
   DBuf acc(c, 24);
   zero(c, acc.get(), 24);
   cudaEvent_t e0;
+  if (c->opt.verbose) KT_CUDA(cudaEventRecord(c->ev[2], c->stream));
   c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
   if (s.W) {
     unsigned long long* a = acc.as<unsigned long long>();
@@ -424,6 +425,7 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint3
     KT_LAUNCHED(c);
   }
   c->timer.end(c->stream, e0, &c->stats.ms_support_kernel);
+  if (c->opt.verbose) KT_CUDA(cudaEventRecord(c->ev[3], c->stream));
   c->stats.support_launches++;
   // Algorithmic bytes (outside the timed span): the merge model, and the
   // bytes the kernel that ran moved.
@@ -439,6 +441,10 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint3
   c->stats.support_row_words += h[1];
   // Dense: row words, plus per edge its list entry (4), ends (8) and result (4).
   c->stats.support_kernel_bytes += s.W ? 4 * h[1] + 16 * s.m : merge;
+  KT_LOG(c, "kt: support (%s) on %u vertices (widest group %u), %llu edges: %llu row words, %.3f ms\n",
+         s.W ? (cap || (gcap && s.vgid.get()) ? "dense capped" : "dense") : "list", s.n,
+         s.vbase.get() ? s.max_group : s.n, (unsigned long long)s.m, (unsigned long long)h[1],
+         c->opt.verbose ? event_ms(c->ev[2], c->ev[3]) : 0.0);
 }
 
 }  // namespace kt

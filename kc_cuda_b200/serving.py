@@ -71,4 +71,22 @@ def summarize(submitted: Sequence[tuple], results: Sequence[dict]) -> Dict[str, 
         "graphs_per_s": len(results) / span,
         "waves": len(waves),
         "mean_wave_graphs": float(np.mean([r["wave_graphs"] for r in results])) if results else 0.0,
+        "per_lane": per_lane(results),
     }
+
+
+def per_lane(results: Sequence[dict]) -> List[Dict[str, float]]:
+    """Per lane: requests, latency p50/p99, wait p50, in-wave time p50
+    (latency - wait) and waves."""
+    out = []
+    for lane in sorted({r.get("lane", 0) for r in results}):
+        rs = [r for r in results if r.get("lane", 0) == lane]
+        out.append({
+            "lane": int(lane), "requests": len(rs),
+            "p50_ms": percentile([r["ms_latency"] for r in rs], 50),
+            "p99_ms": percentile([r["ms_latency"] for r in rs], 99),
+            "wait_p50_ms": percentile([r["ms_wait"] for r in rs], 50),
+            "in_wave_p50_ms": percentile([r["ms_latency"] - r["ms_wait"] for r in rs], 50),
+            "waves": len({r["wave"] for r in rs}),
+        })
+    return out
