@@ -623,6 +623,9 @@ def run_single(args, world, rank, local, pg, threads):
     n_edges, n_vertices = g.num_edges, g.num_vertices
     del g
     ctx = K.Context(local)
+    # The memory pool grown once up front (as a long-running process would
+    # hold it): a step then never maps new device memory mid-solve.
+    ctx.set_option("pool_reserve_mb", 1 << 30)
     staged = ctx.stage_tsv(tsv)
 
     # Warm-up (device-resident and end-to-end paths).
@@ -755,6 +758,7 @@ def run_single(args, world, rank, local, pg, threads):
                     "copy_note": "copy_parse_ms: the host-to-device copy of the TSV bytes in chunks with each "
                                  "chunk's parse overlapped (copy-bound); copy_gbs: TSV bytes over it"},
             "gpu_launches": launches,
+            "device_step_ms": [round(x, 1) for x in dev_ms],
             "roofline": dict(dominant, note=(
                 "dense support rows are read mostly from L2 (tile order), so frac near 1 of the HBM copy "
                 "bandwidth is L2-served work; traffic is the DRAM share")),

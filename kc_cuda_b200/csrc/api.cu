@@ -11,6 +11,8 @@
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 
 #include "handles.h"
@@ -31,6 +33,7 @@ bool option_value_ok(const char* name, int64_t value) {
   if (!std::strcmp(name, "support_rows")) return value == 1 || value == 2 || value == 4;
   if (!std::strcmp(name, "peel_bisect_gap")) return value >= 1;
   if (!std::strcmp(name, "serve_small_coop")) return value == 0 || value == 1;
+  if (!std::strcmp(name, "support_hash_max_deg")) return value >= 0 && value <= 512;
   if (!std::strcmp(name, "coop_occupancy_pct")) return value >= 1 && value <= 100;
   return true;
 }
@@ -308,6 +311,16 @@ const char* kt_status_string(kt_status s) {
   return "unknown status";
 }
 
+namespace {
+// Contexts alive per device (the default memory pool is shared by them).
+int live_contexts(int device, int delta) {
+  static std::mutex mu;
+  static std::map<int, int> live;
+  std::lock_guard<std::mutex> lk(mu);
+  return live[device] += delta;
+}
+}  // namespace
+
 kt_status kt_init(int device, uint64_t budget, kt_ctx** out) {
   if (!out) return KT_ERR_INVALID;
   *out = nullptr;
@@ -328,12 +341,18 @@ kt_status kt_init(int device, uint64_t budget, kt_ctx** out) {
     KT_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
     size_t fr = 0, tot = 0;
     KT_CUDA(cudaMemGetInfo(&fr, &tot));
-    c.budget = budget ? budget : (uint64_t)(fr * 0.9);
-    // Keep freed blocks in the pool for reuse across calls.
+    // Keep freed blocks in the pool for reuse across calls.  Memory the pool
+    // holds but no allocation uses (left by earlier contexts) counts as free.
     cudaMemPool_t pool;
     KT_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t thr = UINT64_MAX;
     KT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    uint64_t reserved = 0, used = 0;
+    KT_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    KT_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    c.budget = budget ? budget : (uint64_t)((fr + (reserved > used ? reserved - used : 0)) * 0.9);
+    live_contexts(device, +1);
+    h->counted = true;
     KT_CUDA(cudaHostAlloc(&c.pinned, 4096, cudaHostAllocDefault));
     for (auto& e : c.ev) KT_CUDA(cudaEventCreate(&e));
     c.words.alloc(&c, sizeof(kt::DevWords));
@@ -363,6 +382,13 @@ void kt_destroy(kt_ctx* h) {
     if (h->c.pinned) cudaFreeHost(h->c.pinned);
     if (h->c.stream) cudaStreamDestroy(h->c.stream);
     if (h->c.copy_stream) cudaStreamDestroy(h->c.copy_stream);
+    // The last context on the device hands the pool's cached memory back,
+    // so the next one (or anything else in the process) can have it.
+    if (h->counted && live_contexts(h->c.device, -1) == 0) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, h->c.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+      cudaGetLastError();
+    }
   }
   delete h;
 }
@@ -410,6 +436,7 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"support_rows", &o.support_rows},
              {"serve_small_mb", &o.serve_small_mb},
              {"serve_small_coop", &o.serve_small_coop},
+             {"support_hash_max_deg", &o.support_hash_max_deg},
              {"peel_bisect_after", &o.peel_bisect_after},
              {"peel_bisect_gap", &o.peel_bisect_gap},
              {"coop_occupancy_pct", &o.coop_occupancy_pct}};

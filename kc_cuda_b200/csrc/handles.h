@@ -10,6 +10,7 @@
 
 struct kt_ctx {
   kt::Ctx c;
+  bool counted = false;  // counted among the device's live contexts
 };
 struct kt_graph {
   kt::Graph g;
