@@ -101,6 +101,8 @@ const char* kt_status_string(kt_status s);
  *                               stepped (no cooperative launch, so it never waits for
  *                               another lane's), 1 = cooperative launches taking turns
  *                               with the other lanes'
+ *   serve_partition (0)         1: the other lanes admit only requests above
+ *                               serve_small_mb (0: any request)
  *   batch_lanes (2)             batch: waves in flight at once, 1..2
  *   support_rows (2)            exact dense support: edges sharing row u counted
  *                               together per shared-memory read of it (1, 2 or 4)

@@ -69,10 +69,18 @@ struct kt_server {
   std::vector<Lane> lanes;
   std::mutex coop;  // cooperative launches of the lanes, one at a time
   uint64_t small_bytes = 0;  // the small lane (the last) admits only requests this small (0: any)
+  bool partition = false;    // ... and the other lanes only larger ones
   int64_t lane0_coop_pct = 100;  // the server's context's coop_occupancy_pct, restored at the end
-  bool queue_has_small() const {
+  // Whether a lane admits a request: the small lane only small ones; with
+  // the partition the other lanes only the others.
+  bool admits(bool small_lane, const Request* r) const {
+    if (!small_bytes || lanes.size() < 2) return true;
+    if (small_lane) return r->footprint <= small_bytes;
+    return !partition || r->footprint > small_bytes;
+  }
+  bool queue_has_for(bool small_lane) const {
     for (const Request* r : queue)
-      if (r->footprint <= small_bytes) return true;
+      if (admits(small_lane, r)) return true;
     return false;
   }
 
@@ -107,12 +115,12 @@ struct kt_server {
         // Admission: arrival order, while the footprint fits.  With a small
         // lane (the last of two or more, small_bytes > 0) that lane admits only
         // requests of at most small_bytes, skipping larger ones; the other
-        // lanes admit any request.
-        const bool small_only = small_bytes && lanes.size() > 1 && lane_ctx == lanes.back().ctx;
+        // lanes admit any request (with the partition, only larger ones).
+        const bool small_lane = lane_ctx == lanes.back().ctx;
         uint64_t bytes = 0;
         for (auto it = queue.begin(); it != queue.end() && wave.size() < max_wave;) {
           Request* r = *it;
-          if (small_only && r->footprint > small_bytes) {
+          if (!admits(small_lane, r)) {
             ++it;
             continue;
           }
@@ -122,10 +130,10 @@ struct kt_server {
           it = queue.erase(it);
         }
         if (wave.empty()) {
-          // Only large requests are queued and this is the small lane: the
-          // other lanes take them; wait for a small arrival (or the end).
+          // Only requests of another lane's class are queued: that lane takes
+          // them; wait for one of this lane's (or the end).
           if (stopping) break;
-          work_cv.wait(lk, [&] { return stopping || queue_has_small(); });
+          work_cv.wait(lk, [&] { return stopping || queue_has_for(small_lane); });
           continue;
         }
         // Others still queued: wake the other free lanes for them.
@@ -240,6 +248,7 @@ kt_status kt_server_create(kt_ctx* ctx, uint32_t max_wave_graphs, kt_server** ou
     ctx_budget = c.budget;
     nlanes = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, c.opt.serve_lanes), 4);
     s->small_bytes = nlanes > 1 ? (uint64_t)std::max<int64_t>(0, c.opt.serve_small_mb) << 20 : 0;
+    s->partition = c.opt.serve_partition != 0;
     // Half of the free budget for the waves in flight, shared by the lanes.
     s->budget = (c.budget > c.in_use ? c.budget - c.in_use : 0) / 2 / nlanes;
   }
