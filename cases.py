@@ -11,6 +11,10 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
                   bitset rows of 1736 words (385 MB of rows, above L2): the
                   shape of the bench graph's search core (55,455 vertices,
                   92.1M edges).
+  er1m-support    Erdos-Renyi G(n=1,000,000, M=64,000,000 draws), seed 7: one
+                  kt_edge_support call in list mode -> k_support_hash on every
+                  vertex (average degree ~128, the shape of the mix's largest
+                  Erdos-Renyi graphs).
   rmat21-solve    R-MAT scale 21, edge factor 32, seed 2, cliques 80/120/200:
                   one kt_solve_staged (every stage; peel kernel k_cascade<8>).
   rmat16-solve    config-1 graph (R-MAT scale 16, edge factor 16, seed 1, K30).
@@ -121,7 +125,7 @@ def largest_mix(count: int, among: int = 4096):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense-support", "core55k-support", "rmat21-solve", "rmat16-solve", "rmat24-solve",
+    ap.add_argument("case", choices=["dense-support", "core55k-support", "er1m-support", "rmat21-solve", "rmat16-solve", "rmat24-solve",
                                      "chunglu10m-solve", "chunglu50m-solve", "mix-batch", "mix-largest"])
     ap.add_argument("--count", type=int, default=64, help="mix-largest: how many of the largest graphs")
     ap.add_argument("--graphs", type=int, default=256, help="mix-batch: graphs 0..N-1")
@@ -138,6 +142,8 @@ def main() -> None:
         dense_support(a.reps, options=opts)
     elif a.case == "core55k-support":
         dense_support(a.reps, n=55455, draws=95_000_000, options=opts)
+    elif a.case == "er1m-support":
+        dense_support(a.reps, n=1_000_000, draws=64_000_000, options=opts)
     elif a.case == "rmat21-solve":
         solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
     elif a.case == "mix-batch":

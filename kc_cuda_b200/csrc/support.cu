@@ -87,13 +87,13 @@ __global__ void __launch_bounds__(kSupThreadsWide) k_support_bitmap(uint32_t n, 
 // shared-memory hash table of the warp's own (open addressing, linear
 // probing, at most half full), so each SM holds dozens of vertices in flight
 // where the bitmap kernel holds one.  The lower neighbours u of v are taken
-// 32 at a time and their lists flattened over the lanes (a lane finds the u
-// of its entry by a search over the 32 list offsets), so short lists keep
-// every lane busy; hits count into per-warp counters, one per u, written to
-// the edges (u, v) at the end.  Vertices are handed out 32 at a time per
-// warp from `cursor`; heavier ones are left to the bitmap kernel.
+// four at a time, one per group of 8 lanes; a group scans N(u) eight entries
+// per step (one 32-byte sector) against the table and sums its hits.
+// Vertices are handed out 32 at a time per warp from `cursor`; heavier ones
+// are left to the bitmap kernel.
 constexpr unsigned kHashSlots = 1024;   // per warp: room for degree <= 512
 constexpr unsigned kHashThreads = 256;
+constexpr unsigned kHashGroup = 8;      // lanes per lower neighbour
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t w, uint32_t shift) { return (w * 2654435761u) >> shift; }
 
@@ -104,12 +104,9 @@ __global__ void __launch_bounds__(kHashThreads) k_support_hash(uint32_t n, const
                                                                uint32_t* __restrict__ sup, uint32_t maxdeg,
                                                                unsigned long long* cursor) {
   __shared__ uint32_t tab_all[(kHashThreads / 32) * kHashSlots];
-  __shared__ uint32_t cnt_all[(kHashThreads / 32) * 32];
   uint32_t* tab = tab_all + warp_id() * kHashSlots;
-  uint32_t* cnt = cnt_all + warp_id() * 32;
-  const unsigned l = lane_id();
+  const unsigned l = lane_id(), grp = l / kHashGroup, gl = l % kHashGroup;
   for (uint32_t i = l; i < kHashSlots; i += 32) tab[i] = 0;
-  cnt[l] = 0;
   __syncwarp();
   while (true) {
     unsigned long long first = 0;
@@ -131,39 +128,19 @@ __global__ void __launch_bounds__(kHashThreads) k_support_hash(uint32_t n, const
         while (atomicCAS(&tab[h], 0u, w + 1) != 0u) h = (h + 1) & mask;
       }
       __syncwarp();
-      for (uint64_t c0 = vb; c0 < vu; c0 += 32) {
-        const uint64_t j = c0 + l;
-        uint64_t ub = 0;
-        uint32_t du = 0;
+      for (uint64_t j0 = vb; j0 < vu; j0 += 32 / kHashGroup) {
+        const uint64_t j = j0 + grp;
+        uint32_t cnt = 0;
         if (j < vu) {
           const uint32_t u = adj[j];
-          ub = off[u];
-          du = (uint32_t)(off[u + 1] - ub);
-        }
-        // Exclusive offsets of the 32 lists in the flattened range.
-        uint32_t pre = du;
-        for (unsigned o = 1; o < 32; o <<= 1) {
-          const uint32_t t = __shfl_up_sync(kFull, pre, o);
-          if (l >= o) pre += t;
-        }
-        const uint32_t total = __shfl_sync(kFull, pre, 31), excl = pre - du;
-        for (uint32_t p0 = 0; p0 < total; p0 += 32) {
-          const uint32_t p = p0 + l;
-          // Owner of entry p: the last lane whose list starts at or before p.
-          uint32_t k = 0;
-          for (unsigned st = 16; st; st >>= 1) {
-            const uint32_t e = __shfl_sync(kFull, excl, k + st);
-            if (e <= p) k += st;
-          }
-          const uint64_t kb = __shfl_sync(kFull, ub, k);
-          const uint32_t ke = __shfl_sync(kFull, excl, k);
-          if (p < total) {
-            const uint32_t w = adj[kb + (p - ke)];
+          const uint64_t ue = off[u + 1];
+          for (uint64_t q = off[u] + gl; q < ue; q += kHashGroup) {
+            const uint32_t w = adj[q];
             uint32_t h = hash_slot(w, shift);
             while (true) {
               const uint32_t t = tab[h];
               if (t == w + 1) {
-                atomicAdd(&cnt[k], 1u);
+                ++cnt;
                 break;
               }
               if (t == 0) break;
@@ -171,11 +148,10 @@ __global__ void __launch_bounds__(kHashThreads) k_support_hash(uint32_t n, const
             }
           }
         }
-        __syncwarp();
-        if (j < vu) sup[eid[j]] = cnt[l];
-        cnt[l] = 0;
-        __syncwarp();
+        for (unsigned o = kHashGroup / 2; o; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o, kHashGroup);
+        if (gl == 0 && j < vu) sup[eid[j]] = cnt;
       }
+      __syncwarp();
       for (uint32_t i = l; i <= mask; i += 32) tab[i] = 0;
       __syncwarp();
     }
