@@ -12,8 +12,8 @@ Cases (each fits in a few GB of device memory, inputs larger than L2):
                   shape of the bench graph's search core (55,455 vertices,
                   92.1M edges).
   er1m-support    Erdos-Renyi G(n=1,000,000, M=64,000,000 draws), seed 7: one
-                  kt_edge_support call in list mode -> k_support_hash on every
-                  vertex (average degree ~128, the shape of the mix's largest
+                  kt_edge_support call in list mode -> k_support_bitmap
+                  (average degree ~128, the shape of the mix's largest
                   Erdos-Renyi graphs).
   rmat21-solve    R-MAT scale 21, edge factor 32, seed 2, cliques 80/120/200:
                   one kt_solve_staged (every stage; peel kernel k_cascade<8>).

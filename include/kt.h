@@ -56,8 +56,6 @@ const char* kt_status_string(kt_status s);
  *   predict (1)                 prediction phase (truss of the maximum core)
  *   persistent (1)              peel / k-core rounds in one cooperative launch
  *   support_bitmap_max_n (2^20) vertex-bitmap support up to this many vertices
- *   support_hash_max_deg (512)  ... of which the vertices up to this degree are
- *                               counted with a warp hash table each (0..512, 0: off)
  *   dense_max_n (65536)         adjacency bitsets up to this many vertices
  *   dense_min_fill (32)         bitsets when avg degree * this >= words per row
  *   recount_gamma (16)          recount round when frontier * thr * gamma > alive * words

@@ -34,7 +34,6 @@ bool option_value_ok(const char* name, int64_t value) {
   if (!std::strcmp(name, "peel_bisect_gap")) return value >= 1;
   if (!std::strcmp(name, "serve_small_coop")) return value == 0 || value == 1;
   if (!std::strcmp(name, "serve_partition")) return value == 0 || value == 1;
-  if (!std::strcmp(name, "support_hash_max_deg")) return value >= 0 && value <= 512;
   if (!std::strcmp(name, "coop_occupancy_pct")) return value >= 1 && value <= 100;
   return true;
 }
@@ -438,7 +437,6 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"serve_small_mb", &o.serve_small_mb},
              {"serve_small_coop", &o.serve_small_coop},
              {"serve_partition", &o.serve_partition},
-             {"support_hash_max_deg", &o.support_hash_max_deg},
              {"peel_bisect_after", &o.peel_bisect_after},
              {"peel_bisect_gap", &o.peel_bisect_gap},
              {"coop_occupancy_pct", &o.coop_occupancy_pct}};

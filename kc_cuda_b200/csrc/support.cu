@@ -18,7 +18,6 @@
 
 #include <vector>
 
-#include "compact.cuh"
 #include "dense.cuh"
 #include "subgraph.h"
 
@@ -31,16 +30,13 @@ constexpr unsigned kSupThreadsWide = 1024;  // bitmap kernel when its bitmap lim
 // Batched unions: the bitmap covers only v's own graph, bits indexed from
 // vbase[v] (graphs are contiguous and no edge crosses graphs); `range` =
 // most vertices of one graph.
-// `list` (when given): the vertices to count from (n of them, taken from
-// the last); otherwise every vertex, from n-1 down.
 __global__ void __launch_bounds__(kSupThreadsWide) k_support_bitmap(uint32_t n, const uint64_t* __restrict__ off,
                                                                 const uint32_t* __restrict__ adj,
                                                                 const uint32_t* __restrict__ eid,
                                                                 const uint64_t* __restrict__ up,
                                                                 uint32_t* __restrict__ sup,
                                                                 unsigned long long* cursor,
-                                                                const uint32_t* __restrict__ vbase, uint32_t range,
-                                                                const uint32_t* __restrict__ list) {
+                                                                const uint32_t* __restrict__ vbase, uint32_t range) {
   extern __shared__ uint32_t bits[];
   __shared__ uint32_t s_v;
   const uint32_t words = (range + 31) / 32;
@@ -49,8 +45,7 @@ __global__ void __launch_bounds__(kSupThreadsWide) k_support_bitmap(uint32_t n, 
   while (true) {
     if (threadIdx.x == 0) {
       const unsigned long long t = atomicAdd(cursor, 1ULL);
-      const uint32_t at = (uint32_t)(n - 1 - t);
-      s_v = t < n ? (list ? list[at] : at) : 0xffffffffu;
+      s_v = t < n ? (uint32_t)(n - 1 - t) : 0xffffffffu;
     }
     __syncthreads();
     const uint32_t v = s_v;
@@ -82,91 +77,6 @@ __global__ void __launch_bounds__(kSupThreadsWide) k_support_bitmap(uint32_t n, 
     __syncthreads();
   }
 }
-
-// Light vertices (degree <= maxdeg): a warp per vertex v, N(v) in a
-// shared-memory hash table of the warp's own (open addressing, linear
-// probing, at most half full), so each SM holds dozens of vertices in flight
-// where the bitmap kernel holds one.  The lower neighbours u of v are taken
-// four at a time, one per group of 8 lanes; a group scans N(u) eight entries
-// per step (one 32-byte sector) against the table and sums its hits.
-// Vertices are handed out 32 at a time per warp from `cursor`; heavier ones
-// are left to the bitmap kernel.
-constexpr unsigned kHashSlots = 1024;   // per warp: room for degree <= 512
-constexpr unsigned kHashThreads = 256;
-constexpr unsigned kHashGroup = 8;      // lanes per lower neighbour
-
-__device__ __forceinline__ uint32_t hash_slot(uint32_t w, uint32_t shift) { return (w * 2654435761u) >> shift; }
-
-__global__ void __launch_bounds__(kHashThreads) k_support_hash(uint32_t n, const uint64_t* __restrict__ off,
-                                                               const uint32_t* __restrict__ adj,
-                                                               const uint32_t* __restrict__ eid,
-                                                               const uint64_t* __restrict__ up,
-                                                               uint32_t* __restrict__ sup, uint32_t maxdeg,
-                                                               unsigned long long* cursor) {
-  __shared__ uint32_t tab_all[(kHashThreads / 32) * kHashSlots];
-  uint32_t* tab = tab_all + warp_id() * kHashSlots;
-  const unsigned l = lane_id(), grp = l / kHashGroup, gl = l % kHashGroup;
-  for (uint32_t i = l; i < kHashSlots; i += 32) tab[i] = 0;
-  __syncwarp();
-  while (true) {
-    unsigned long long first = 0;
-    if (l == 0) first = atomicAdd(cursor, 32ULL);
-    first = __shfl_sync(kFull, first, 0);
-    if (first >= n) break;
-    const uint32_t last = (uint32_t)(first + 32 < n ? first + 32 : n);
-    for (uint32_t v = (uint32_t)first; v < last; ++v) {
-      const uint64_t vb = off[v], ve = off[v + 1], vu = up[v];
-      const uint32_t deg = (uint32_t)(ve - vb);
-      if (vu == vb || deg > maxdeg) continue;  // nothing below v, or a heavy vertex
-      // Table of 2^b >= 2 deg slots (64 at least): keys w + 1, 0 = empty.
-      uint32_t b = 6;
-      while ((1u << b) < 2 * deg) ++b;
-      const uint32_t mask = (1u << b) - 1, shift = 32 - b;
-      for (uint64_t j = vb + l; j < ve; j += 32) {
-        const uint32_t w = adj[j];
-        uint32_t h = hash_slot(w, shift);
-        while (atomicCAS(&tab[h], 0u, w + 1) != 0u) h = (h + 1) & mask;
-      }
-      __syncwarp();
-      for (uint64_t j0 = vb; j0 < vu; j0 += 32 / kHashGroup) {
-        const uint64_t j = j0 + grp;
-        uint32_t cnt = 0;
-        if (j < vu) {
-          const uint32_t u = adj[j];
-          const uint64_t ue = off[u + 1];
-          for (uint64_t q = off[u] + gl; q < ue; q += kHashGroup) {
-            const uint32_t w = adj[q];
-            uint32_t h = hash_slot(w, shift);
-            while (true) {
-              const uint32_t t = tab[h];
-              if (t == w + 1) {
-                ++cnt;
-                break;
-              }
-              if (t == 0) break;
-              h = (h + 1) & mask;
-            }
-          }
-        }
-        for (unsigned o = kHashGroup / 2; o; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o, kHashGroup);
-        if (gl == 0 && j < vu) sup[eid[j]] = cnt;
-      }
-      __syncwarp();
-      for (uint32_t i = l; i <= mask; i += 32) tab[i] = 0;
-      __syncwarp();
-    }
-  }
-}
-
-// Vertices the bitmap kernel takes when light ones go to k_support_hash:
-// degree above the hash limit and at least one lower neighbour.
-struct HeavyVertex {
-  const uint64_t* off;
-  const uint64_t* up;
-  uint32_t maxdeg;
-  __device__ bool keep(uint64_t v) const { return off[v + 1] - off[v] > maxdeg && up[v] > off[v]; }
-  __device__ uint32_t value(uint64_t v) const { return (uint32_t)v; }
-};
 
 // Position of x in sorted a[lo, hi), or hi.
 __device__ __forceinline__ uint64_t find_sorted(const uint32_t* a, uint64_t lo, uint64_t hi, uint32_t x) {
@@ -500,39 +410,15 @@ void edge_support(Ctx* c, const Sub& s, uint32_t* sup, uint32_t cap, const uint3
     int per_sm = 0;
     KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_support_bitmap, threads, smem));
     if (per_sm < 1) throw Error(KT_ERR_LIMIT, "support: bitmap does not fit in shared memory");
-    // Light vertices by the warp hash kernel, the rest by the bitmap kernel.
-    const uint32_t hmax = (uint32_t)std::min<int64_t>(std::max<int64_t>(0, c->opt.support_hash_max_deg),
-                                                      kHashSlots / 2);
-    DBuf heavy;
-    uint64_t nbit = s.n;
-    if (hmax) {
-      c->timer.end(c->stream, e0, &c->stats.ms_support_kernel);
-      heavy.alloc(c, (uint64_t)s.n * sizeof(uint32_t));
-      nbit = compact(c, s.n, HeavyVertex{s.off.as<uint64_t>(), s.up.as<uint64_t>(), hmax}, heavy.as<uint32_t>());
-      c->timer.begin(c->stream, &c->stats.ms_support_kernel, &e0);
-      int hper_sm = 0;
-      KT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hper_sm, k_support_hash, kHashThreads, 0));
-      DBuf hcur(c, 8);
-      zero(c, hcur.get(), 8);
-      const uint64_t warps = (s.n + 31) / 32;  // vertex groups of 32
-      const unsigned hgrid = (unsigned)std::max<uint64_t>(
-          1, std::min<uint64_t>((uint64_t)std::max(hper_sm, 1) * c->num_sms, (warps + 7) / 8));
-      k_support_hash<<<hgrid, kHashThreads, 0, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
-                                                             s.eid.as<uint32_t>(), s.up.as<uint64_t>(), sup, hmax,
-                                                             hcur.as<unsigned long long>());
-      KT_LAUNCHED(c);
-    }
-    if (nbit) {
-      DBuf cur(c, 8);
-      zero(c, cur.get(), 8);
-      const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * c->num_sms, nbit);
-      k_support_bitmap<<<grid, threads, smem, c->stream>>>((uint32_t)nbit, s.off.as<uint64_t>(),
-                                                               s.adj.as<uint32_t>(), s.eid.as<uint32_t>(),
-                                                               s.up.as<uint64_t>(), sup, cur.as<unsigned long long>(),
-                                                               s.vbase.get() ? s.vbase.as<uint32_t>() : nullptr,
-                                                               range, hmax ? heavy.as<uint32_t>() : nullptr);
-      KT_LAUNCHED(c);
-    }
+    DBuf cur(c, 8);
+    zero(c, cur.get(), 8);
+    const unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * c->num_sms, s.n);
+    k_support_bitmap<<<grid, threads, smem, c->stream>>>(s.n, s.off.as<uint64_t>(), s.adj.as<uint32_t>(),
+                                                             s.eid.as<uint32_t>(), s.up.as<uint64_t>(), sup,
+                                                             cur.as<unsigned long long>(),
+                                                             s.vbase.get() ? s.vbase.as<uint32_t>() : nullptr,
+                                                             range);
+    KT_LAUNCHED(c);
   } else {
     k_support_search<<<grid_for(s.m * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
         s.m, s.ends.as<uint64_t>(), s.off.as<uint64_t>(), s.adj.as<uint32_t>(), sup);

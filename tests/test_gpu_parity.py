@@ -243,20 +243,15 @@ def test_without_prediction_same_answer(ctx, golden):
         ctx.set_option("predict", 1)
 
 
-@pytest.mark.parametrize("mode", ["sparse", "sparse_bitmap_only", "sparse_hash_split", "dense_recount_always",
-                                  "dense_recount_never", "dense_uncapped",
+@pytest.mark.parametrize("mode", ["sparse", "dense_recount_always", "dense_recount_never", "dense_uncapped",
                                   "dense_merge_only", "dense_split_always", "bisect_always_sparse",
                                   "bisect_always_dense"])
 def test_modes_support_trussness_answer(ctx, golden, mode):
-    """Sparse lists (warp hash tables for light vertices and the vertex bitmap
-    for the rest, the bitmap alone, or a low degree limit that splits the
-    vertices between the two) vs dense bitsets, dense peels that recount every round vs
+    """Sparse lists vs dense bitsets, dense peels that recount every round vs
     never, dense peels that intersect sorted lists instead of bitset rows, and
     peels that bisect the truss levels after the first one (undoing empty
     levels from a snapshot): all bit-identical to the oracle."""
     opts = {"sparse": {"dense_max_n": 0},
-            "sparse_bitmap_only": {"dense_max_n": 0, "support_hash_max_deg": 0},
-            "sparse_hash_split": {"dense_max_n": 0, "support_hash_max_deg": 6},
             "dense_recount_always": {"dense_min_fill": 1 << 30, "recount_gamma": 1 << 30},
             "dense_recount_never": {"dense_min_fill": 1 << 30, "recount_gamma": 1},
             "dense_uncapped": {"dense_min_fill": 1 << 30, "capped_support": 0},
