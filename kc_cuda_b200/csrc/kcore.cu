@@ -815,7 +815,15 @@ void KCore::compact_to_alive(Ctx* c, uint32_t level) {
   }
   L.max_deg = g.max_deg;  // an upper bound is enough here
   newid.release();
-  // Install (the old local graph, if any, is released by the swap).
+  // Install; the previous compaction, if any, is kept for restores.
+  if (compacted) {
+    Saved sv;
+    sv.local = std::move(local);
+    sv.idmap = std::move(idmap);
+    sv.level = local_level;
+    saved.push_back(std::move(sv));
+    local = Graph();
+  }
   local.off = std::move(L.off);
   local.adj = std::move(L.adj);
   local.deg = std::move(L.deg);
@@ -984,13 +992,25 @@ uint32_t KCore::find_max_core(Ctx* c) {
 
 void KCore::restore_core(Ctx* c, uint32_t k) {
   if (compacted && k < local_level) {
-    // Below the compacted core: start over from the input graph.
-    compacted = false;
-    local = Graph();
-    idmap.release();
-    levels.assign(1, 1);
-    succ.assign(1, 0);
-    reset_state(c, *base);
+    // Below the compacted core: start over from the deepest earlier
+    // compaction at or below level k, else from the input graph.
+    while (!saved.empty() && saved.back().level > k) saved.pop_back();
+    if (!saved.empty()) {
+      local = std::move(saved.back().local);
+      idmap = std::move(saved.back().idmap);
+      local_level = saved.back().level;
+      saved.pop_back();
+      levels.assign(1, local_level);
+      succ.assign(1, 0);
+      reset_state(c, local);
+    } else {
+      compacted = false;
+      local = Graph();
+      idmap.release();
+      levels.assign(1, 1);
+      succ.assign(1, 0);
+      reset_state(c, *base);
+    }
   }
   // Last successful probe at or below level k; everything newer is revived.
   uint32_t keep = 0;

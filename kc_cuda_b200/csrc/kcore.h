@@ -26,6 +26,15 @@ struct KCore {
   unsigned coop_grid = 0;
   std::vector<uint32_t> levels;  // levels[tag] = k of that probe
   std::vector<uint32_t> succ;    // tags of probes that were kept
+  // Earlier compactions (shallowest first), kept so that a restore below
+  // the current compaction's level starts from the deepest one at or below
+  // it instead of from the input graph.
+  struct Saved {
+    Graph local;
+    DBuf idmap;
+    uint32_t level = 0;
+  };
+  std::vector<Saved> saved;
 
   const Graph& cur() const { return compacted ? local : *base; }
   const uint32_t* map() const { return compacted ? idmap.as<uint32_t>() : nullptr; }

@@ -55,7 +55,7 @@ struct PeelArgs {
   const uint32_t* alive;
   uint64_t na;
   uint32_t* front[2];
-  unsigned long long* cnt;  // 3 rotating frontier counters, [3] rounds done, [5] recount rounds
+  unsigned long long* cnt;  // 3 rotating frontier counters, [3] rounds done, [4] gave up, [5] recount rounds
   uint64_t cap;
   uint32_t thr;    // remove support < thr
   uint32_t tval;   // trussness recorded for removed edges
@@ -75,6 +75,10 @@ struct PeelArgs {
   const uint32_t* gthr;
   const uint32_t* egr;
   const uint32_t* gthr_max;  // batched: the largest running threshold (recount cost model)
+  // A level tried from a snapshot: give up (the level's truss is empty) as
+  // soon as fewer than this many edges can remain, t(t-1)/2 for level t
+  // (0: peel to the end).  The state is then partial; the caller undoes it.
+  uint64_t fail_below = 0;
 };
 
 __device__ __forceinline__ uint32_t edge_thr(const PeelArgs& A, uint32_t e) {
@@ -436,9 +440,15 @@ __global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(Pe
   uint64_t pending = 0;          // edges deleted since then
   uint32_t i = 0, nrec = 0;
   bool ok = true;
+  bool gave_up = false;
   while (true) {
     const uint64_t nf = ld_acquire_u64(&A.cnt[i % 3]);
     if (nf == 0) break;
+    // Every block reads the same counts, so all of them give up together.
+    if (alive - nf < A.fail_below) {
+      gave_up = true;
+      break;
+    }
     const uint32_t r = A.r0 + i;
     uint32_t* fr = A.front[i & 1];
     uint32_t* nx = A.front[(i + 1) & 1];
@@ -487,7 +497,7 @@ __global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(Pe
     ++i;
   }
   // Bring the bitsets up to date with this cascade's remaining deletions.
-  if (ok && A.R.bits && pending) {
+  if (ok && !gave_up && A.R.bits && pending) {
     if (pending > alive) {
       zero_bits(A, gtid, gthreads);
       if (grid_barrier(A.words, A.timeout_ns)) set_alive_bits(A, gtid, gthreads);
@@ -499,6 +509,7 @@ __global__ void __launch_bounds__(kPeelThreads, KT_PEEL_MIN_BLOCKS) k_cascade(Pe
   if (lane_id() == 0 && trec) atomicAdd(&A.acct[2], (unsigned long long)trec);
   if (gtid == 0) {
     A.cnt[3] = i;
+    A.cnt[4] = gave_up;
     A.cnt[5] = nrec;
   }
 }
@@ -640,6 +651,7 @@ struct Peeler {
   int ai = 0;
   uint64_t na = 0;
   uint32_t r = 1;  // next round number
+  uint64_t fail_below = 0;  // set while a level is tried from a snapshot (PeelArgs::fail_below)
   unsigned coop_grid = 0;
   size_t smem = 0;
   PeelResult* res;
@@ -711,7 +723,17 @@ struct Peeler {
     A.gthr = track ? gthr.as<uint32_t>() : nullptr;
     A.egr = track ? egr.as<uint32_t>() : nullptr;
     A.gthr_max = track ? tmax.as<uint32_t>() : nullptr;
+    A.fail_below = fail_below;
     return A;
+  }
+
+  // A level tried from a snapshot: the cascade gives up once its truss can
+  // no longer hold t(t-1)/2 edges.
+  uint64_t try_level(uint32_t t) {
+    fail_below = (uint64_t)t * (t - 1) / 2;
+    const uint64_t left = cascade(t);
+    fail_below = 0;
+    return left;
   }
 
   // Removes every alive edge with support < t-2, to the fixpoint; returns
@@ -722,6 +744,7 @@ struct Peeler {
     cudaEvent_t e0;
     c->timer.begin(c->stream, &c->stats.ms_peel_kernel, &e0);
     uint64_t rounds = 0, recounts = 0;
+    bool gave_up = false;
     scanned += na;
     const auto t_start = std::chrono::steady_clock::now();
     if (coop_grid) {
@@ -734,13 +757,20 @@ struct Peeler {
         copy_d2h(c, h, A.cnt + 3, sizeof(h));
       }
       rounds = h[0];
+      gave_up = h[1] != 0;
       recounts = h[2];
     } else {
       k_level_frontier<<<grid_for(na, kPeelThreads, c->num_sms * 16), kPeelThreads, 0, c->stream>>>(A);
       KT_LAUNCHED(c);
+      uint64_t left = na;
       for (uint32_t i = 0;; ++i) {
         const uint64_t nf = read_word<unsigned long long>(c, A.cnt + (i % 3));
         if (nf == 0) break;
+        if (left - nf < A.fail_below) {
+          gave_up = true;
+          break;
+        }
+        left -= nf;
         ++rounds;
         KT_CUDA(cudaMemsetAsync(A.cnt + ((i + 1) % 3), 0, sizeof(unsigned long long), c->stream));
         k_round<<<grid_for(nf * 32, kPeelThreads, c->num_sms * 16), kPeelThreads, 0, c->stream>>>(A, i, nf);
@@ -750,13 +780,14 @@ struct Peeler {
     c->timer.end(c->stream, e0, &c->stats.ms_peel_kernel);
     c->stats.peel_launches++;
     check_words(c, "truss peel");
-    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds (%llu recount), %.3f ms\n", t,
-           (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds,
-           (unsigned long long)recounts,
+    KT_LOG(c, "kt: cascade level %u on %llu alive of %llu edges (n %u, W %u): %llu rounds (%llu recount)%s, %.3f ms\n",
+           t, (unsigned long long)na, (unsigned long long)s->m, s->n, s->W, (unsigned long long)rounds,
+           (unsigned long long)recounts, gave_up ? ", gave up" : "",
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     r += (uint32_t)rounds + 1;
     res->rounds += rounds;
     res->levels++;
+    if (gave_up) return 0;  // the level is empty; the state is partial and the caller undoes it
     na = compact(c, na,
                  StillAlive{alive[ai].as<uint32_t>(), state.as<uint32_t>(), A.gthr, A.egr},
                  alive[ai ^ 1].as<uint32_t>());
@@ -866,7 +897,7 @@ struct Peeler {
     save();
     while (hi - lo > 1) {
       const uint32_t mid = lo + (hi - lo) / 2;
-      const uint64_t left = cascade(mid);
+      const uint64_t left = try_level(mid);
       if (left) {
         uint32_t mn, mx;
         minmax(mn, mx);
@@ -950,7 +981,7 @@ PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t
     const int ai0 = P.ai;
     uint32_t g = guess;
     while (g > t0) {
-      if (P.cascade(g)) {
+      if (P.try_level(g)) {
         t = g;
         break;
       }

@@ -226,6 +226,32 @@ def test_core_numbers_generated(ctx, persistent):
         ctx.set_option("persistent", 1)
 
 
+def test_kcore_restore_from_nested_compactions(ctx, golden):
+    """With a compacted copy made at almost every successful probe
+    (kcore_compact 2), a restore below the last copy's level starts from the
+    deepest earlier copy at or below it: k-core membership for levels spread
+    over 1..cmax equals the oracle's, and the solver's answers (whose search
+    phase restores the (L-1)-core) equal the golden ones."""
+    ctx.set_option("kcore_compact", 2)
+    try:
+        specs = [gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=200_000, draws=1_500_000, seed=9, cl_w_max=20_000.0),
+                 gen.rmat(15, 24, 5, [40])]
+        for spec in specs:
+            g = gen.Graph(spec)
+            d = ctx.load_pairs(g.edges())
+            want = O.core_numbers(d.edges(), d.num_vertices)
+            cmax = int(want.max())
+            for k in sorted(set(np.linspace(1, cmax, 12).astype(int).tolist()) | {max(1, cmax - 1)}):
+                mem, cm = d.kmax_core(k)
+                assert cm == cmax, (spec, k)
+                assert np.array_equal(mem, want >= k), (spec, k)
+            d.free()
+        for name, e, gg in spec_graphs(golden):
+            assert ctx.solve_tsv(gg.tsv_bytes()) == (e["kmax"], e["edges"]), name
+    finally:
+        ctx.set_option("kcore_compact", 8)
+
+
 def test_config1_rmat_s16(ctx, golden):
     e = golden["rmat_s16_ef16_k30"]
     g = gen.Graph(gen.GraphSpec(**e["spec"]))
