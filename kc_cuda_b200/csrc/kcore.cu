@@ -974,8 +974,15 @@ uint32_t KCore::find_max_core(Ctx* c) {
       // Work on a compacted copy once the core is a small part of the graph.
       // (The copy holds the k-core, which every level from k up can be
       // restored from.)
-      if (c->opt.kcore_compact > 0 && n_alive * (uint64_t)c->opt.kcore_compact < n)
+      if (c->opt.kcore_compact > 0 && n_alive * (uint64_t)c->opt.kcore_compact < n) {
+        const auto tc = std::chrono::steady_clock::now();
+        const uint64_t from = n;
         compact_to_alive(c, (uint32_t)k);
+        KT_LOG(c, "kt: k-core compacted copy of the %llu-core: %llu of %llu vertices, %llu edges, %.3f ms\n",
+               (unsigned long long)k, (unsigned long long)n, (unsigned long long)from,
+               (unsigned long long)local.m,
+               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc).count());
+      }
     } else {
       hi = k;
       ramp = false;
