@@ -65,6 +65,7 @@ def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
     data = g.tsv_bytes()
     del g
     with Context(0) as ctx:
+        ctx.set_option("pool_reserve_mb", 1 << 30)  # no memory mapped mid-solve
         if verbose:
             ctx.set_option("verbose", 1)
         t = ctx.stage_tsv(data)
