@@ -64,14 +64,14 @@ __device__ __forceinline__ void push_warp(bool want, uint32_t item, uint32_t* li
 
 constexpr unsigned kBigBatch = 1024;  // big rows per batch of dealt windows
 
-// Deals the 32-entry windows of the big rows big[0..nbig) to every warp of
+// Deals the kWin-entry windows of the big rows big[0..nbig) to every warp of
 // the grid, so one long row is spread over the whole GPU instead of one
 // block: each block lists the rows' first window numbers (the same block scan
 // in every block, kBigBatch rows at a time) and warp w takes windows w,
-// w + warps, ...; `drop(b, e)` handles entries [b, e) (at most 32) of a row.
-// Every thread of the block must call it (it synchronises the block); blocks
-// have 256 threads.
-template <class Drop>
+// w + warps, ...; `drop(b, e)` handles entries [b, e) (at most kWin) of a
+// row.  Every thread of the block must call it (it synchronises the block);
+// blocks have 256 threads.
+template <unsigned kWin, class Drop>
 __device__ __forceinline__ void deal_big_windows(const uint32_t* __restrict__ big, uint64_t nbig,
                                                  const uint64_t* __restrict__ off, uint64_t* woff, uint64_t* tmp,
                                                  Drop drop) {
@@ -89,7 +89,7 @@ __device__ __forceinline__ void deal_big_windows(const uint32_t* __restrict__ bi
       w[j] = 0;
       if (r < cnt) {
         const uint32_t v = big[base + r];
-        w[j] = (off[v + 1] - off[v] + 31) / 32;
+        w[j] = (off[v + 1] - off[v] + kWin - 1) / kWin;
       }
       sum += w[j];
     }
@@ -113,7 +113,7 @@ __device__ __forceinline__ void deal_big_windows(const uint32_t* __restrict__ bi
           hi = mid;
       }
       const uint32_t v = big[base + lo];
-      const uint64_t b = off[v] + (x - woff[lo]) * 32, e = min(off[v + 1], b + 32);
+      const uint64_t b = off[v] + (x - woff[lo]) * kWin, e = min(off[v + 1], b + kWin);
       drop(b, e);
     }
     __syncthreads();
@@ -320,12 +320,16 @@ struct BigAliveRow {
   __device__ uint32_t value(uint64_t i) const { return (uint32_t)i; }
 };
 
-// Rows longer than kBigRow in the compaction: their 32-entry windows are
-// dealt to every warp of the grid (each block lists the rows' first window
-// numbers with the same block scan, kBigBatch rows at a time); a window's
-// kept entries go to the row's next free positions (a per-row cursor), so a
-// hub row is spread over the whole GPU.  Entry order within these rows is not
-// kept; nothing downstream needs it.
+// Rows longer than kBigRow in the compaction: their 256-entry chunks are
+// dealt to every warp of the grid (each block lists the rows' first chunk
+// numbers with the same block scan, kBigBatch rows at a time); a warp loads
+// its chunk's 8 entries per lane, their alive flags and new ids before it
+// uses any of them (so 8 loads of each kind are in flight per lane), and
+// the chunk's kept entries go to the row's next free positions (a per-row
+// cursor, one atomic per chunk), so a hub row is spread over the whole GPU.
+// Entry order within these rows is not kept; nothing downstream needs it.
+constexpr unsigned kCompactChunk = 256;  // entries per warp step (8 per lane)
+
 __global__ void __launch_bounds__(256) k_compact_big_rows(const uint32_t* __restrict__ rows, uint64_t nrows,
                                                           const uint32_t* __restrict__ alive,
                                                           const uint64_t* __restrict__ off,
@@ -336,8 +340,10 @@ __global__ void __launch_bounds__(256) k_compact_big_rows(const uint32_t* __rest
                                                           uint32_t* __restrict__ cursor, uint32_t* __restrict__ nadj) {
   __shared__ uint64_t woff[kBigBatch + 1];
   __shared__ uint64_t tmp[33];
+  constexpr unsigned kPer = kCompactChunk / 32;
   const uint64_t gwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp_id();
+  const unsigned l = lane_id();
   constexpr unsigned per = kBigBatch / 256;  // rows per thread
   for (uint64_t base = 0; base < nrows; base += kBigBatch) {
     const uint64_t left = nrows - base;
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(256) k_compact_big_rows(const uint32_t* __rest
       w[j] = 0;
       if (r < cnt) {
         const uint32_t v = alive[rows[base + r]];
-        w[j] = (off[v + 1] - off[v] + 31) / 32;
+        w[j] = (off[v + 1] - off[v] + kCompactChunk - 1) / kCompactChunk;
       }
       sum += w[j];
     }
@@ -375,21 +381,35 @@ __global__ void __launch_bounds__(256) k_compact_big_rows(const uint32_t* __rest
       }
       const uint32_t i = rows[base + lo];
       const uint32_t v = alive[i];
-      const uint64_t j = off[v] + (x - woff[lo]) * 32 + lane_id();
-      bool keep = false;
-      uint32_t nb = 0;
-      if (j < off[v + 1]) {
-        const uint32_t u = adj[j];
-        keep = rem[u] == kAlive;
-        if (keep) nb = newid[u];
+      const uint64_t e = off[v + 1];
+      const uint64_t j0 = off[v] + (x - woff[lo]) * kCompactChunk + l;
+      uint32_t u[kPer];
+#pragma unroll
+      for (unsigned k = 0; k < kPer; ++k) u[k] = j0 + 32 * k < e ? adj[j0 + 32 * k] : 0u;
+      bool keep[kPer];
+#pragma unroll
+      for (unsigned k = 0; k < kPer; ++k) keep[k] = j0 + 32 * k < e && rem[u[k]] == kAlive;
+#pragma unroll
+      for (unsigned k = 0; k < kPer; ++k) u[k] = keep[k] ? newid[u[k]] : 0u;
+      unsigned bal[kPer];
+      uint32_t kept = 0;
+#pragma unroll
+      for (unsigned k = 0; k < kPer; ++k) {
+        bal[k] = __ballot_sync(kFull, keep[k]);
+        kept += __popc(bal[k]);
       }
-      const unsigned bal = __ballot_sync(kFull, keep);
-      if (!bal) continue;
+      if (!kept) continue;
       uint32_t at = 0;
-      if (lane_id() == 0) at = atomicAdd(&cursor[base + lo], (uint32_t)__popc(bal));
+      if (l == 0) at = atomicAdd(&cursor[base + lo], kept);
       at = __shfl_sync(kFull, at, 0);
-      const uint64_t p = noff[i] + at + __popc(bal & lanemask_lt());
-      if (keep && p < noff[i + 1]) nadj[p] = nb;
+      const uint64_t row0 = noff[i], row1 = noff[i + 1];
+      uint64_t p0 = row0 + at;
+#pragma unroll
+      for (unsigned k = 0; k < kPer; ++k) {
+        const uint64_t p = p0 + __popc(bal[k] & lanemask_lt());
+        if (keep[k] && p < row1) nadj[p] = u[k];
+        p0 += __popc(bal[k]);
+      }
     }
     __syncthreads();
   }
@@ -450,8 +470,33 @@ __device__ __forceinline__ void drop_neighbours(const ProbeArgs& A, uint64_t b, 
   }
 }
 
+// drop_neighbours for up to 256 entries [b, e): each lane loads its 8
+// entries, their alive flags, then decrements their degrees, before it uses
+// any result, so 8 loads and 8 atomics of each lane are in flight at once
+// (the big rows' windows in a probe).
+__device__ __forceinline__ void drop_neighbours_wide(const ProbeArgs& A, uint64_t b, uint64_t e, uint32_t* next,
+                                                     unsigned long long* ncnt) {
+  constexpr unsigned kPer = 8;
+  const uint64_t j0 = b + lane_id();
+  uint32_t w[kPer];
+#pragma unroll
+  for (unsigned k = 0; k < kPer; ++k) w[k] = j0 + 32 * k < e ? A.adj[j0 + 32 * k] : 0u;
+  bool live[kPer];
+#pragma unroll
+  for (unsigned k = 0; k < kPer; ++k) live[k] = j0 + 32 * k < e && A.rem[w[k]] == kAlive;
+  uint32_t old[kPer];
+#pragma unroll
+  for (unsigned k = 0; k < kPer; ++k) old[k] = live[k] ? atomicSub(&A.deg[w[k]], 1u) : 0u;
+#pragma unroll
+  for (unsigned k = 0; k < kPer; ++k) {
+    const bool want = live[k] && old[k] == A.k;
+    if (want) A.rem[w[k]] = A.tag;
+    push_warp(want, w[k], next, ncnt, A.cap, &A.words->err);
+  }
+}
+
 // A whole probe (frontier init and every round) in one cooperative launch.
-__global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
+__global__ void __launch_bounds__(256, 4) k_probe(ProbeArgs A) {
   __shared__ uint64_t woff[kBigBatch + 1];
   __shared__ uint64_t wtmp[33];
   const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
@@ -508,9 +553,9 @@ __global__ void __launch_bounds__(256) k_probe(ProbeArgs A) {
     if (!grid_barrier(A.words, A.timeout_ns)) return;
     const uint64_t nbig = ld_acquire_u64(bc);
     if (nbig) {
-      // Rows longer than big_row: their 32-entry windows dealt to every warp.
-      deal_big_windows(A.big, nbig, A.off, woff, wtmp,
-                       [&](uint64_t b, uint64_t e) { drop_neighbours(A, b, e, nx, nc); });
+      // Rows longer than big_row: their 256-entry windows dealt to every warp.
+      deal_big_windows<256>(A.big, nbig, A.off, woff, wtmp,
+                            [&](uint64_t b, uint64_t e) { drop_neighbours_wide(A, b, e, nx, nc); });
       if (!grid_barrier(A.words, A.timeout_ns)) return;
     }
     ++i;
@@ -720,8 +765,8 @@ __global__ void __launch_bounds__(256, 4) k_core_levels(DecompArgs A) {
       if (!grid_barrier(A.words, A.timeout_ns)) return;
       const uint64_t nbig = block_read(bc, &sh);
       if (nbig) {
-        deal_big_windows(A.big, nbig, A.off, woff, wtmp,
-                         [&](uint64_t b, uint64_t e) { drop_neighbours_core(A, b, e, R); });
+        deal_big_windows<32>(A.big, nbig, A.off, woff, wtmp,
+                             [&](uint64_t b, uint64_t e) { drop_neighbours_core(A, b, e, R); });
         if (!grid_barrier(A.words, A.timeout_ns)) return;
       }
       ++i;
