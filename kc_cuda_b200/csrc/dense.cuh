@@ -220,7 +220,11 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 
 // As dense_group, but an edge whose count can no longer reach its threshold
 // is abandoned: the rows are ANDed in four segments, and after each one the
-// count so far plus the set bits left in row u bounds the result.  An
+// count so far plus the set bits left in row u bounds the result.  The
+// segments go from the last to the first: vertex ids ascend with degree, so
+// the last words of a row hold the high-degree vertices and most of the set
+// bits, and after them the bits left in row u are few enough to abandon most
+// edges below the threshold after one or two segments.  An
 // abandoned edge reports a count below the threshold (not its support).  The
 // threshold is `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
 // Two edges that share row u run side by side, one per half of the warp (two
@@ -247,7 +251,7 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_ok = ok;
   my_s = 0;
   unsigned todo = __ballot_sync(kFull, ok);
-  uint32_t s1 = 0, s2 = 0, s3 = 0;  // set bits of row u in segments 2..4
+  uint32_t s1 = 0, s2 = 0, s3 = 0;  // set bits of row u in segments 1..3
   uint32_t cu = 0xffffffffu, W = 0, c1 = 0, c2 = 0, c3 = 0;
   while (todo) {
     const int j = __ffs(todo) - 1;
@@ -263,14 +267,14 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       c1 = min(W, (strides / 4) * 32);
       c2 = min(W, (strides / 2) * 32);
       c3 = min(W, ((3 * strides) / 4) * 32);
-      uint32_t b = 0, c = 0, d = 0;
-      for (uint32_t i = c1 + l; i < W; i += 32) {
+      uint32_t a = 0, b = 0, c = 0;
+      for (uint32_t i = l; i < c3; i += 32) {
         const uint32_t pc = __popc(su[i]);
-        if (i < c2) b += pc; else if (i < c3) c += pc; else d += pc;
+        if (i < c1) a += pc; else if (i < c2) b += pc; else c += pc;
       }
-      s1 = warp_sum(b);
-      s2 = warp_sum(c);
-      s3 = warp_sum(d);
+      s1 = warp_sum(a);
+      s2 = warp_sum(b);
+      s3 = warp_sum(c);
       if (wr && l == 0) *wr += W;
     }
     // The next edge with the same row u goes to the upper half of the warp:
@@ -291,20 +295,20 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     const uint32_t t = upper ? tj2 : tj;
     bool go = !upper || j2 >= 0;
     const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
-    uint32_t wds = go ? c1 : 0u;  // row-v words this half reads
-    uint32_t found = half_and_popc(pv, su, 0, c1, go);
+    uint32_t wds = go ? W - c3 : 0u;  // row-v words this half reads
+    uint32_t found = half_and_popc(pv, su, c3, W, go);
     go = go && found + s1 + s2 + s3 >= t;
     if (__any_sync(kFull, go)) {
-      wds += go ? c2 - c1 : 0u;
-      found += half_and_popc(pv, su, c1, c2, go);
-      go = go && found + s2 + s3 >= t;
+      wds += go ? c3 - c2 : 0u;
+      found += half_and_popc(pv, su, c2, c3, go);
+      go = go && found + s1 + s2 >= t;
       if (__any_sync(kFull, go)) {
-        wds += go ? c3 - c2 : 0u;
-        found += half_and_popc(pv, su, c2, c3, go);
-        go = go && found + s3 >= t;
+        wds += go ? c2 - c1 : 0u;
+        found += half_and_popc(pv, su, c1, c2, go);
+        go = go && found + s1 >= t;
         if (__any_sync(kFull, go)) {
-          wds += go ? W - c3 : 0u;
-          found += half_and_popc(pv, su, c3, W, go);
+          wds += go ? c1 : 0u;
+          found += half_and_popc(pv, su, 0, c1, go);
         }
       }
     }
