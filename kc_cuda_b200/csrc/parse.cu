@@ -21,7 +21,6 @@
 #include "kt_device.cuh"
 #include "kt_internal.h"
 #include "stages.h"
-#include "swar_line.h"
 
 namespace kt {
 namespace {
@@ -149,33 +148,6 @@ __device__ __forceinline__ bool parse_line_fast(const uint32_t* stage, uint64_t 
   return true;
 }
 
-// The line at p decoded eight bytes at a time (swar_line.h) from a 24-byte
-// window of the staged words; false when the window would pass lim - 4 or
-// the line is not of the common form (the byte decoders then take it).
-__device__ __forceinline__ bool parse_line_swar(const uint32_t* stage, uint64_t blo, uint64_t lim, uint64_t p,
-                                                uint64_t* key, uint32_t* vmax) {
-  if (p + 28 > lim) return false;
-  const uint32_t off = (uint32_t)(p - blo), q = off >> 2, sh = (off & 3) * 8;
-  uint32_t a[7];
-#pragma unroll
-  for (int i = 0; i < 7; ++i) a[i] = stage[q + i];
-  uint64_t w[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-    w[i] = (uint64_t)__funnelshift_r(a[2 * i], a[2 * i + 1], sh) |
-           ((uint64_t)__funnelshift_r(a[2 * i + 1], a[2 * i + 2], sh) << 32);
-  uint32_t x = 0, y = 0;
-  bool blank = false;
-  if (!swar::decode_line(w, &x, &y, &blank)) return false;
-  if (blank) {
-    *key = ~0ull;
-    return true;
-  }
-  *vmax = max(*vmax, max(x, y));
-  *key = x == y ? ~0ull : (((uint64_t)y << 32) | x);
-  return true;
-}
-
 // Phase 1 finds the block's line starts (newlines a word at a time, a block
 // scan, offsets into shared memory); phase 2 deals the lines round-robin to
 // the threads, so the per-line work is balanced and the keys are written
@@ -237,8 +209,7 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
   for (uint32_t i = threadIdx.x; i < total; i += kParseThreads) {
     bool bad = false;
     uint64_t key;
-    if (!parse_line_swar(stage, blo, lim, blo + starts[i], &key, &vmax) &&
-        !parse_line_fast(stage, blo, lim, blo + starts[i], &key, &bad, &vmax)) {
+    if (!parse_line_fast(stage, blo, lim, blo + starts[i], &key, &bad, &vmax)) {
       bad = false;
       key = parse_line(B, blo + starts[i], &bad, &vmax);
     }
