@@ -218,17 +218,15 @@ __device__ __forceinline__ void dense_group(const uint32_t* __restrict__ list, u
 }
 
 
-constexpr int kCapSegments = 8;  // capped support: segments a row pair is ANDed in
-
 // As dense_group, but an edge whose count can no longer reach its threshold
-// is abandoned: the rows are ANDed in kCapSegments segments, and after each
-// one the count so far plus the set bits left in row u bounds the result.
-// The segments go from the last to the first: vertex ids ascend with degree,
-// so the last words of a row hold the high-degree vertices and most of the
-// set bits, and after them the bits left in row u are few enough to abandon
-// most edges below the threshold after a few segments.  An abandoned edge
-// reports a count below the threshold (not its support).  The threshold is
-// `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
+// is abandoned: the rows are ANDed in four segments, and after each one the
+// count so far plus the set bits left in row u bounds the result.  The
+// segments go from the last to the first: vertex ids ascend with degree, so
+// the last words of a row hold the high-degree vertices and most of the set
+// bits, and after them the bits left in row u are few enough to abandon most
+// edges below the threshold after one or two segments.  An
+// abandoned edge reports a count below the threshold (not its support).  The
+// threshold is `thr`, or for a grouped union gthr[vgid[u]] (its graph's).
 // Two edges that share row u run side by side, one per half of the warp (two
 // load streams per warp).
 __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ list, uint64_t base, uint64_t cnt,
@@ -253,10 +251,8 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
   my_ok = ok;
   my_s = 0;
   unsigned todo = __ballot_sync(kFull, ok);
-  constexpr int S = kCapSegments;
-  uint32_t cb[S + 1];  // segment bounds (whole 32-word strides; the last ends at W)
-  uint32_t below[S];   // set bits of row u in the segments before segment k
-  uint32_t cu = 0xffffffffu, W = 0;
+  uint32_t s1 = 0, s2 = 0, s3 = 0;  // set bits of row u in segments 1..3
+  uint32_t cu = 0xffffffffu, W = 0, c1 = 0, c2 = 0, c3 = 0;
   while (todo) {
     const int j = __ffs(todo) - 1;
     todo &= todo - 1;
@@ -266,17 +262,19 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
       W = R.words(uj);
       dense_load_row(R.bits + R.off(uj), W, su);
       cu = uj;
+      // Segment bounds: four runs of whole 32-word strides.
       const uint32_t strides = (W + 31) / 32;
-#pragma unroll
-      for (int k = 0; k < S; ++k) cb[k] = min(W, (strides * k / S) * 32);
-      cb[S] = W;
-      below[0] = 0;
-#pragma unroll
-      for (int k = 1; k < S; ++k) {
-        uint32_t pc = 0;
-        for (uint32_t i = cb[k - 1] + l; i < cb[k]; i += 32) pc += __popc(su[i]);
-        below[k] = below[k - 1] + warp_sum(pc);
+      c1 = min(W, (strides / 4) * 32);
+      c2 = min(W, (strides / 2) * 32);
+      c3 = min(W, ((3 * strides) / 4) * 32);
+      uint32_t a = 0, b = 0, c = 0;
+      for (uint32_t i = l; i < c3; i += 32) {
+        const uint32_t pc = __popc(su[i]);
+        if (i < c1) a += pc; else if (i < c2) b += pc; else c += pc;
       }
+      s1 = warp_sum(a);
+      s2 = warp_sum(b);
+      s3 = warp_sum(c);
       if (wr && l == 0) *wr += W;
     }
     // The next edge with the same row u goes to the upper half of the warp:
@@ -297,14 +295,22 @@ __device__ __forceinline__ void dense_group_capped(const uint32_t* __restrict__ 
     const uint32_t t = upper ? tj2 : tj;
     bool go = !upper || j2 >= 0;
     const uint32_t* pv = R.bits + R.off(upper ? vj2 : vj);
-    uint32_t wds = 0;  // row-v words this half reads
-    uint32_t found = 0;
-#pragma unroll
-    for (int k = S - 1; k >= 0; --k) {
-      if (k < S - 1 && !__any_sync(kFull, go)) break;
-      wds += go ? cb[k + 1] - cb[k] : 0u;
-      found += half_and_popc(pv, su, cb[k], cb[k + 1], go);
-      go = go && found + below[k] >= t;
+    uint32_t wds = go ? W - c3 : 0u;  // row-v words this half reads
+    uint32_t found = half_and_popc(pv, su, c3, W, go);
+    go = go && found + s1 + s2 + s3 >= t;
+    if (__any_sync(kFull, go)) {
+      wds += go ? c3 - c2 : 0u;
+      found += half_and_popc(pv, su, c2, c3, go);
+      go = go && found + s1 + s2 >= t;
+      if (__any_sync(kFull, go)) {
+        wds += go ? c2 - c1 : 0u;
+        found += half_and_popc(pv, su, c1, c2, go);
+        go = go && found + s1 >= t;
+        if (__any_sync(kFull, go)) {
+          wds += go ? c1 : 0u;
+          found += half_and_popc(pv, su, 0, c1, go);
+        }
+      }
     }
     const uint32_t f0 = __shfl_sync(kFull, found, 0), f1 = __shfl_sync(kFull, found, 16);
     if (l == (unsigned)j) my_s = f0;

@@ -44,6 +44,31 @@ __global__ void k_map_back(const uint64_t* __restrict__ ends, uint64_t m, const 
   }
 }
 
+// Vertices with at least `need` edges of support >= thr (warp per row).
+__global__ void k_rows_at_least(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ eid,
+                                const uint32_t* __restrict__ sup, uint32_t thr, uint32_t need,
+                                unsigned long long* __restrict__ out) {
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t x = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; x < n; x += warps) {
+    uint32_t c = 0;
+    for (uint64_t j = off[x] + lane_id(); j < off[x + 1]; j += 32) c += sup[eid[j]] >= thr;
+    c = warp_sum(c);
+    if (lane_id() == 0 && c >= need) atomicAdd(out, 1ULL);
+  }
+}
+
+// Whether a g-truss can exist in s: each of its (at least g) vertices has at
+// least g-1 edges of support >= g-2 within it, hence within s.
+bool truss_possible(Ctx* c, const Sub& s, const uint32_t* sup, uint32_t g) {
+  if (s.n == 0 || s.m == 0) return false;
+  DBuf cnt(c, 8);
+  zero(c, cnt.get(), 8);
+  k_rows_at_least<<<grid_for((uint64_t)s.n * 32, 256, c->num_sms * 16), 256, 0, c->stream>>>(
+      s.n, s.off.as<uint64_t>(), s.eid.as<uint32_t>(), sup, g - 2, g - 1, cnt.as<unsigned long long>());
+  KT_LAUNCHED(c);
+  return read_word<unsigned long long>(c, cnt.as<unsigned long long>()) >= g;
+}
+
 // Ends of the edges whose (capped) support reaches a threshold.
 struct AtLeast {
   const uint32_t* sup;
@@ -101,6 +126,10 @@ PeelResult predict_peel(Ctx* c, const Sub& s1, uint32_t* sup1, uint32_t cmax) {
     if (k * 2 > s1.m) {
       if (!tried) g = std::min(g, half);
       break;
+    }
+    if (!truss_possible(c, s1, sup1, g)) {
+      KT_LOG(c, "kt: predict level %u: fewer than %u vertices with %u such edges\n", g, g, g - 1);
+      continue;
     }
     Sub s;
     build_sub_from_keys(c, keys.as<uint64_t>(), k, s1.n, s);
