@@ -60,12 +60,14 @@ def dense_support(reps: int, n: int = 40000, draws: int = 48_000_000, options=()
         dg.free()
 
 
-def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False) -> None:
+def solve(spec: gen.GraphSpec, reps: int, verbose: bool = False, options=()) -> None:
     g = gen.Graph(spec)
     data = g.tsv_bytes()
     del g
     with Context(0) as ctx:
         ctx.set_option("pool_reserve_mb", 1 << 30)  # no memory mapped mid-solve
+        for name, v in options:
+            ctx.set_option(name, v)
         if verbose:
             ctx.set_option("verbose", 1)
         t = ctx.stage_tsv(data)
@@ -136,7 +138,7 @@ def main() -> None:
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
-                    help="support cases: a solver option to set first (repeatable)")
+                    help="a solver option to set first (repeatable)")
     a = ap.parse_args()
     opts = [(o.split("=")[0], int(o.split("=")[1])) for o in a.option]
     if a.case == "dense-support":
@@ -146,7 +148,7 @@ def main() -> None:
     elif a.case == "er1m-support":
         dense_support(a.reps, n=1_000_000, draws=64_000_000, options=opts)
     elif a.case == "rmat21-solve":
-        solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose)
+        solve(gen.rmat(21, 32, 2, [80, 120, 200]), a.reps, a.verbose, opts)
     elif a.case == "mix-batch":
         idx = [i for i in range(a.graphs) if not a.max_draws or gen.mix_graph(i).draws <= a.max_draws]
         mix_batch(a.reps, a.verbose, indices=idx, options=opts, alone=a.alone,
@@ -155,14 +157,15 @@ def main() -> None:
         mix_batch(a.reps, a.verbose, indices=largest_mix(a.count), options=opts, alone=a.alone,
                   verbose_alone=a.verbose_alone)
     elif a.case == "rmat24-solve":
-        solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose)
+        solve(gen.rmat_s24_ef32_k80_120_200(), a.reps, a.verbose, opts)
     elif a.case == "chunglu10m-solve":
         solve(gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=10_000_000, draws=200_000_000, seed=3, cl_gamma=2.1,
-                            cl_w_min=5.0, cl_w_max=400_000.0, block_size=150, block_p=0.95), a.reps, a.verbose)
+                            cl_w_min=5.0, cl_w_max=400_000.0, block_size=150, block_p=0.95), a.reps, a.verbose,
+              opts)
     elif a.case == "chunglu50m-solve":
-        solve(gen.chunglu_50m(), a.reps, a.verbose)
+        solve(gen.chunglu_50m(), a.reps, a.verbose, opts)
     else:
-        solve(gen.rmat_s16_k30(), a.reps, a.verbose)
+        solve(gen.rmat_s16_k30(), a.reps, a.verbose, opts)
 
 
 if __name__ == "__main__":

@@ -390,7 +390,7 @@ static bool survivors(Ctx* c, const Sub& s, const uint32_t* sup, const std::vect
                              keys.as<uint64_t>());
   KT_LOG(c, "kt: batch survivors: %llu of %llu edges\n", (unsigned long long)k, (unsigned long long)s.m);
   if (only_if_few && k * 2 >= s.m) return false;
-  build_sub_grouped_from_keys(c, keys.as<uint64_t>(), k, s.n, s.vgid.as<uint32_t>(), G, out);
+  build_sub_grouped_from_keys(c, keys.as<uint64_t>(), k, s.n, s.vgid.as<uint32_t>(), G, out, true);
   keys.release();
   out_sup = DBuf(c, (out.m ? out.m : 1) * sizeof(uint32_t));
   edge_support(c, out, out_sup.as<uint32_t>());

@@ -284,11 +284,17 @@ bool build_graph_grouped(Ctx* c, const uint64_t* keys, uint64_t nk, uint64_t n, 
   return true;
 }
 
-void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g);
+void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool presorted);
+
+// Sets *bad when keys[i] >= keys[i+1] for some i (not strictly ascending).
+__global__ void k_not_ascending(const uint64_t* __restrict__ keys, uint64_t n, unsigned int* bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (keys[i] >= keys[i + 1]) *bad = 1u;
+}
 
 }  // namespace
 
-void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines) {
+void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines, bool sorted) {
   // Vertex counts travel as u32 through the later stages: the all-ones id
   // (which would make n = 2^32) is refused.
   if (n > 0xffffffffULL) throw Error(KT_ERR_LIMIT, "vertex id 4294967295: ids must be below 2^32 - 1");
@@ -297,41 +303,58 @@ void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, b
     c->stats.csr_grouped = 1;
     return;
   }
-  build_graph_sorted(c, keys, nkeys, n, g);
+  bool presorted = false;
+  if (sorted && nkeys > 1) {
+    DBuf bad(c, 4);
+    zero(c, bad.get(), 4);
+    k_not_ascending<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys,
+                                                                                  bad.as<unsigned int>());
+    KT_LAUNCHED(c);
+    presorted = read_word<unsigned int>(c, bad.as<unsigned int>()) == 0;
+  }
+  build_graph_sorted(c, keys, nkeys, n, g, presorted);
 }
 
 namespace {
 
-void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g) {
+void build_graph_sorted(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool presorted) {
   g.n = n;
-  // Keys are min << 32 | max with both halves below 2^vb - 1; the radix sort
-  // skips digits shared by every key, so it runs 2 ceil(vb / 8) passes once
-  // the "no edge" key ~0 is rewritten to ((2^vb - 1) << 32) | (2^vb - 1)
-  // (still last).  When packing to min << vb | max saves a pass (2 vb bits,
-  // ceil(2 vb / 8) passes), the keys are packed instead.
-  const int vb = bits_for(n + 1);
-  const bool small = vb < 32 && nkeys;
-  const bool pack = small && (2 * vb + 7) / 8 < 2 * ((vb + 7) / 8);
-  const uint64_t sentinel = ((((uint64_t)1 << (vb & 31)) - 1) << 32) | (((uint64_t)1 << (vb & 31)) - 1);
-  // Records may hold either end first: every route makes them canonical.
-  if (pack) {
-    k_pack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
-    KT_LAUNCHED(c);
-  } else if (nkeys) {
-    k_canon_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL,
-                                                                                 small ? sentinel : ~0ULL);
-    KT_LAUNCHED(c);
+  if (presorted) {
+    // Canonical, ascending and distinct already (survivors taken from a
+    // working graph's edge list): no sort, no dedup.
+    g.edges.alloc(c, nkeys * sizeof(uint64_t));
+    KT_CUDA(cudaMemcpyAsync(g.edges.get(), keys, nkeys * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+    g.m = nkeys;
+  } else {
+    // Keys are min << 32 | max with both halves below 2^vb - 1; the radix sort
+    // skips digits shared by every key, so it runs 2 ceil(vb / 8) passes once
+    // the "no edge" key ~0 is rewritten to ((2^vb - 1) << 32) | (2^vb - 1)
+    // (still last).  When packing to min << vb | max saves a pass (2 vb bits,
+    // ceil(2 vb / 8) passes), the keys are packed instead.
+    const int vb = bits_for(n + 1);
+    const bool small = vb < 32 && nkeys;
+    const bool pack = small && (2 * vb + 7) / 8 < 2 * ((vb + 7) / 8);
+    const uint64_t sentinel = ((((uint64_t)1 << (vb & 31)) - 1) << 32) | (((uint64_t)1 << (vb & 31)) - 1);
+    // Records may hold either end first: every route makes them canonical.
+    if (pack) {
+      k_pack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
+      KT_LAUNCHED(c);
+    } else if (nkeys) {
+      k_canon_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, ~0ULL,
+                                                                                   small ? sentinel : ~0ULL);
+      KT_LAUNCHED(c);
+    }
+    if (nkeys > 1) radix_sort_u64(c, keys, nullptr, nkeys, 64);
+    if (pack) {
+      k_unpack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
+      KT_LAUNCHED(c);
+    } else if (small) {
+      k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, sentinel, ~0ULL);
+      KT_LAUNCHED(c);
+    }
+    g.edges.alloc(c, (nkeys ? nkeys : 1) * sizeof(uint64_t));
+    g.m = unique_sorted_u64(c, keys, g.edges.as<uint64_t>(), nkeys);
   }
-  if (nkeys > 1) radix_sort_u64(c, keys, nullptr, nkeys, 64);
-  if (pack) {
-    k_unpack<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, vb);
-    KT_LAUNCHED(c);
-  } else if (small) {
-    k_remap<<<grid_for(nkeys, 256, c->num_sms * 16), 256, 0, c->stream>>>(keys, nkeys, sentinel, ~0ULL);
-    KT_LAUNCHED(c);
-  }
-  g.edges.alloc(c, (nkeys ? nkeys : 1) * sizeof(uint64_t));
-  g.m = unique_sorted_u64(c, keys, g.edges.as<uint64_t>(), nkeys);
   if ((uint64_t)2 * g.m >= 0xffffffffULL * 4ULL) throw Error(KT_ERR_LIMIT, "graph too large");
   g.deg.alloc(c, (n ? n : 1) * sizeof(uint32_t));
   zero(c, g.deg.get(), (n ? n : 1) * sizeof(uint32_t));

@@ -861,7 +861,9 @@ struct Peeler {
                                                     s->ends.as<uint64_t>()},
                                    keys.as<uint64_t>());
     std::unique_ptr<Sub> ns(new Sub);
-    build_sub_from_keys(c, keys.as<uint64_t>(), k, s->n, *ns);
+    // The alive list is in edge-id order unless the graph has bitsets (tile
+    // order), so its ends are already sorted then.
+    build_sub_from_keys(c, keys.as<uint64_t>(), k, s->n, *ns, s->W == 0);
     DBuf nsup(c, (ns->m ? ns->m : 1) * sizeof(uint32_t));
     edge_support(c, *ns, nsup.as<uint32_t>());
     own.swap(ns);
@@ -934,9 +936,9 @@ struct Peeler {
 
 }  // namespace
 
-void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out) {
+void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out, bool sorted) {
   Graph g;
-  build_graph(c, keys, m, n_ids, g);
+  build_graph(c, keys, m, n_ids, g, false, sorted);
   build_sub_all(c, g, out);
 }
 

@@ -132,7 +132,7 @@ PeelResult predict_peel(Ctx* c, const Sub& s1, uint32_t* sup1, uint32_t cmax) {
       continue;
     }
     Sub s;
-    build_sub_from_keys(c, keys.as<uint64_t>(), k, s1.n, s);
+    build_sub_from_keys(c, keys.as<uint64_t>(), k, s1.n, s, true);
     keys.release();
     DBuf sup(c, (s.m ? s.m : 1) * sizeof(uint32_t));
     edge_support(c, s, sup.as<uint32_t>());
@@ -265,7 +265,7 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
     KT_LOG(c, "kt: search level %u: %llu of %llu edges have support >= %u\n", t2, (unsigned long long)k,
            (unsigned long long)s2.m, t2 - 2);
     if (k * 2 < s2.m) {
-      build_sub_from_keys(c, keys.as<uint64_t>(), k, s2.n, s3);
+      build_sub_from_keys(c, keys.as<uint64_t>(), k, s2.n, s3, true);
       sup3 = DBuf(c, (s3.m ? s3.m : 1) * sizeof(uint32_t));
       edge_support(c, s3, sup3.as<uint32_t>());
       sp = &s3;

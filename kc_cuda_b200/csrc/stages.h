@@ -27,7 +27,11 @@ void parse_lines(Ctx* c, const uint8_t* dbuf, uint64_t len, const DBuf& block_of
 // order, ~0 = none) -> Graph.  `keys` may be consumed (sorted in place).
 // `lines`: the records are a TSV's lines in file order (y << 32 | x), so the
 // grouped-input route is tried first.
-void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines = false);
+// lines: the keys are parsed lines (tried in the grouped form first);
+// sorted: the keys are canonical, ascending and distinct (checked on the
+// device; the sort is skipped when they are).
+void build_graph(Ctx* c, uint64_t* keys, uint64_t nkeys, uint64_t n, Graph& g, bool lines = false,
+                 bool sorted = false);
 
 DevWords* dev_words(Ctx* c);
 void reset_words(Ctx* c);

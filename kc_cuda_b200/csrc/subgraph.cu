@@ -396,9 +396,9 @@ void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t n
 }
 
 void build_sub_grouped_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, const uint32_t* group_of,
-                                 uint32_t ngroups, Sub& s) {
+                                 uint32_t ngroups, Sub& s, bool sorted) {
   Graph g;
-  build_graph(c, keys, m, n_ids, g);
+  build_graph(c, keys, m, n_ids, g, false, sorted);
   DBuf list(c, (g.n ? g.n : 1) * sizeof(uint32_t));
   const uint64_t na = compact(c, g.n, DegPositive{g.deg.as<uint32_t>()}, list.as<uint32_t>());
   build_sub_grouped(c, g, list.as<uint32_t>(), na, g.deg.as<uint32_t>(), nullptr, group_of, ngroups, s);

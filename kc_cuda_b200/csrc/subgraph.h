@@ -54,7 +54,7 @@ void build_sub_grouped(Ctx* c, const Graph& g, const uint32_t* alive, uint64_t n
 // The same from edge keys u << 32 | v (ids below n_ids, group_of indexed by
 // them; keys consumed).
 void build_sub_grouped_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, const uint32_t* group_of,
-                                 uint32_t ngroups, Sub& s);
+                                 uint32_t ngroups, Sub& s, bool sorted = false);
 
 // Per-graph bookkeeping of a batched peel: every graph climbs its own
 // levels; after each of its levels a graph with alive edges records (its
@@ -96,7 +96,9 @@ struct PeelResult {
 // truss (optional, device uint32[m]) receives each edge's trussness.
 // The subgraph of edge keys (u << 32 | v, ids below n_ids; consumed), with
 // bitsets when it qualifies.
-void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out);
+// sorted: the keys are canonical, ascending and distinct (a working graph's
+// edges taken in edge-id order), so the graph build skips its sort.
+void build_sub_from_keys(Ctx* c, uint64_t* keys, uint64_t m, uint32_t n_ids, Sub& out, bool sorted = false);
 // guess (> t0, 0 = none): first level to try, undone and halved toward t0 if
 // it empties the graph (only without truss output).
 PeelResult truss_peel(Ctx* c, const Sub& s, uint32_t* sup, uint32_t t0, uint64_t stop_count, uint32_t* truss,
