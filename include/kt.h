@@ -85,9 +85,9 @@ const char* kt_status_string(kt_status s);
  *                               rows) when the rows are shorter than the lists
  *   wave_budget_pct (50)        batch: a wave's estimated device footprint stays
  *                               within this % of the free budget
- *   kcore_compact (8)           maximum-core search: copy the core into a compact
- *                               graph once it holds < 1/this of the vertices
- *                               (0 = never)
+ *   kcore_compact (4)           maximum-core search: copy the core into a compact
+ *                               graph once it holds < 1/this of the current
+ *                               graph's edges (0 = never)
  *   peel_split (16)             peel: a round whose frontier edges x 8-word row
  *                               chunks <= this x warps deals (edge, chunk) units
  *                               to warps instead of edges (0 = off)

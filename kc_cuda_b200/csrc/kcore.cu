@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "compact.cuh"
 #include "kcore.h"
@@ -256,15 +257,26 @@ __global__ void k_revive(uint32_t* __restrict__ rem, uint64_t n, uint32_t newer_
   }
 }
 
+// Minimum alive degree into *out; with `sum`, also the sum of the alive
+// degrees (twice the alive edges).
 __global__ void k_min_alive_deg(const uint32_t* __restrict__ alive, uint64_t n_alive, const uint32_t* __restrict__ deg,
-                                const uint32_t* __restrict__ rem, uint32_t* out) {
+                                const uint32_t* __restrict__ rem, uint32_t* out,
+                                unsigned long long* sum = nullptr) {
   uint32_t mn = 0xffffffffu;
+  uint64_t s = 0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_alive; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t v = alive[i];
-    if (rem[v] == kAlive) mn = min(mn, deg[v]);
+    if (rem[v] == kAlive) {
+      mn = min(mn, deg[v]);
+      s += deg[v];
+    }
   }
   mn = warp_min(mn);
   if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(out, mn);
+  if (sum) {
+    s = warp_sum(s);
+    if (lane_id() == 0 && s) atomicAdd(sum, (unsigned long long)s);
+  }
 }
 
 __global__ void k_members(const uint32_t* __restrict__ rem, uint64_t n, uint8_t* __restrict__ out) {
@@ -989,7 +1001,7 @@ uint32_t KCore::find_max_core(Ctx* c) {
   ub = std::min<uint64_t>(ub, base->max_deg);
   uint64_t lo = 1, hi = ub + 1;  // the 1-core (non-isolated vertices) is non-empty
   bool ramp = true;
-  DBuf mn(c, 4), snap;
+  DBuf mn(c, 16), snap;
   while (hi - lo > 1) {
     uint64_t k = ramp ? std::min<uint64_t>(lo * 2, hi - 1) : lo + (hi - lo) / 2;
     if (k <= lo) k = lo + 1;
@@ -1010,16 +1022,24 @@ uint32_t KCore::find_max_core(Ctx* c) {
       rebuild_alive(c);
       // The probe left the k-core; its minimum degree d >= k makes it the
       // d-core too, so every level up to d is known to be non-empty.
+      // mn: [0] the minimum alive degree, [2..3] the sum of alive degrees.
       KT_CUDA(cudaMemsetAsync(mn.get(), 0xff, 4, c->stream));
+      KT_CUDA(cudaMemsetAsync(mn.as<uint32_t>() + 2, 0, 8, c->stream));
       k_min_alive_deg<<<grid_for(n_alive, 256, c->num_sms * 8), 256, 0, c->stream>>>(
-          alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), mn.as<uint32_t>());
+          alive.as<uint32_t>(), n_alive, deg.as<uint32_t>(), rem.as<uint32_t>(), mn.as<uint32_t>(),
+          reinterpret_cast<unsigned long long*>(mn.as<uint32_t>() + 2));
       KT_LAUNCHED(c);
-      const uint32_t d = read_word<uint32_t>(c, mn.as<uint32_t>());
+      uint32_t h[4];
+      copy_d2h(c, h, mn.get(), sizeof(h));
+      const uint32_t d = h[0];
+      uint64_t deg_sum = 0;
+      std::memcpy(&deg_sum, h + 2, 8);
       if (d != 0xffffffffu && d > lo) lo = std::min<uint64_t>(d, hi - 1);
-      // Work on a compacted copy once the core is a small part of the graph.
-      // (The copy holds the k-core, which every level from k up can be
-      // restored from.)
-      if (c->opt.kcore_compact > 0 && n_alive * (uint64_t)c->opt.kcore_compact < n) {
+      // Work on a compacted copy once the core's edges are a small part of
+      // the current graph's: a copy that keeps most of them costs more than
+      // the probes it would speed up.  (The copy holds the k-core, which
+      // every level from k up can be restored from.)
+      if (c->opt.kcore_compact > 0 && (deg_sum / 2) * (uint64_t)c->opt.kcore_compact < cur().m) {
         const auto tc = std::chrono::steady_clock::now();
         const uint64_t from = n;
         compact_to_alive(c, (uint32_t)k);

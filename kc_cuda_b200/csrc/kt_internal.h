@@ -61,7 +61,7 @@ struct Options {
   int64_t kcore_blocks_per_sm = 0;  // core decomposition: resident blocks per SM (0 = as many as fit)
   int64_t kcore_window = 32;      // core decomposition: levels per pass over the whole alive list
   int64_t peel_bitset = 1;        // peel: dense rows intersected as bitsets when shorter than the lists
-  int64_t kcore_compact = 8;      // max-core search: compact once the core is < 1/this of the graph (0 = never)
+  int64_t kcore_compact = 4;      // max-core search: compact once the core's edges are < 1/this of the graph's (0 = never)
   int64_t wave_budget_pct = 50;   // batch: a wave's estimated footprint within this % of the free budget
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
   int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)

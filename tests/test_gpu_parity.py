@@ -228,11 +228,12 @@ def test_core_numbers_generated(ctx, persistent):
 
 def test_kcore_restore_from_nested_compactions(ctx, golden):
     """With a compacted copy made at almost every successful probe
-    (kcore_compact 2), a restore below the last copy's level starts from the
-    deepest earlier copy at or below it: k-core membership for levels spread
-    over 1..cmax equals the oracle's, and the solver's answers (whose search
-    phase restores the (L-1)-core) equal the golden ones."""
-    ctx.set_option("kcore_compact", 2)
+    (kcore_compact 1: whenever the core has lost edges), a restore below the
+    last copy's level starts from the deepest earlier copy at or below it:
+    k-core membership for levels spread over 1..cmax equals the oracle's, and
+    the solver's answers (whose search phase restores the (L-1)-core) equal
+    the golden ones."""
+    ctx.set_option("kcore_compact", 1)
     try:
         specs = [gen.GraphSpec(kind=gen.KTG_CHUNGLU, n=200_000, draws=1_500_000, seed=9, cl_w_max=20_000.0),
                  gen.rmat(15, 24, 5, [40])]
@@ -249,7 +250,7 @@ def test_kcore_restore_from_nested_compactions(ctx, golden):
         for name, e, gg in spec_graphs(golden):
             assert ctx.solve_tsv(gg.tsv_bytes()) == (e["kmax"], e["edges"]), name
     finally:
-        ctx.set_option("kcore_compact", 8)
+        ctx.set_option("kcore_compact", 4)
 
 
 def test_config1_rmat_s16(ctx, golden):
