@@ -56,3 +56,16 @@ def test_no_cpu_fallback_without_device():
     h = ctypes.c_void_p()
     s = K.lib().kt_init(0, 0, ctypes.byref(h))
     assert s != 0
+
+
+def test_every_option_is_documented():
+    """Each name in the library's option table (kt_set_option) is described in
+    the header's option list."""
+    src = open(os.path.join(ROOT, "kc_cuda_b200", "csrc", "api.cu")).read()
+    table = src[src.index("option_slot(kt::Options& o"):]
+    table = table[: table.index("};")]
+    names = re.findall(r'\{"([a-z_0-9]+)", &o\.', table)
+    assert len(names) > 20
+    header = open(os.path.join(ROOT, "include", "kt.h")).read()
+    missing = [n for n in names if not re.search(r"\*\s+" + n + r" \(", header)]
+    assert not missing, missing
