@@ -99,9 +99,6 @@ const char* kt_status_string(kt_status s);
  *                               stepped (no cooperative launch, so it never waits for
  *                               another lane's), 1 = cooperative launches taking turns
  *                               with the other lanes'
- *   batch_alone_keys (0)        batch: graphs with at least this many edge records
- *                               get a wave of their own (the single-graph driver;
- *                               0: none)
  *   serve_partition (0)         1: the other lanes admit only requests above
  *                               serve_small_mb (0: any request)
  *   batch_lanes (2)             batch: waves in flight at once, 1..2

@@ -437,7 +437,6 @@ static int64_t* option_slot(kt::Options& o, const char* name) {
              {"serve_small_mb", &o.serve_small_mb},
              {"serve_small_coop", &o.serve_small_coop},
              {"serve_partition", &o.serve_partition},
-             {"batch_alone_keys", &o.batch_alone_keys},
              {"peel_bisect_after", &o.peel_bisect_after},
              {"peel_bisect_gap", &o.peel_bisect_gap},
              {"coop_occupancy_pct", &o.coop_occupancy_pct}};

@@ -746,9 +746,6 @@ void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
     return items[a].n != items[b].n ? items[a].n < items[b].n : items[a].nkeys < items[b].nkeys;
   });
-  // Graphs of at least batch_alone_keys edge records (0: none) get a wave of
-  // their own, which takes the single-graph driver.
-  const uint64_t alone_keys = (uint64_t)std::max<int64_t>(0, c->opt.batch_alone_keys);
   std::vector<std::vector<BatchItem*>> waves;
   size_t i = 0;
   while (i < items.size()) {
@@ -757,15 +754,12 @@ void run_batch(Ctx* c, std::vector<BatchItem>& items, BatchRun& out) {
     while (i < items.size()) {
       const BatchItem& it = items[order[i]];
       const uint64_t b = 48 * it.nkeys + 40 * it.n;
-      const bool alone = alone_keys && it.nkeys >= alone_keys;
-      if (!wave.empty() && (alone || bytes + b > budget || verts + it.n >= (1ull << 28) || wave.size() >= 65535))
-        break;
+      if (!wave.empty() && (bytes + b > budget || verts + it.n >= (1ull << 28) || wave.size() >= 65535)) break;
       if (it.n >= (1ull << 28)) throw Error(KT_ERR_LIMIT, "batch: a graph with 2^28 or more vertex ids");
       wave.push_back(&items[order[i]]);
       bytes += b;
       verts += it.n;
       ++i;
-      if (alone) break;
     }
     waves.push_back(std::move(wave));
   }

@@ -66,9 +66,8 @@ struct Options {
   int64_t peel_split = 16;        // peel: (edge, 8-word chunk) units when frontier x chunks <= this x warps (0 = off)
   int64_t serve_lanes = 2;        // serving: waves in flight at once (each on a stream of its own)
   int64_t serve_small_mb = 128;   // serving, two or more lanes: the last lane admits only requests this small (0: any)
-  int64_t serve_small_coop = 0;
-  int64_t serve_partition = 0;
-  int64_t batch_alone_keys = 0;   // batch: graphs with this many edge records or more solved one per wave (0: none)    // serving: the other lanes admit only requests above serve_small_mb   // serving: the small lane's kernels cooperative (1) or host-stepped (0)
+  int64_t serve_small_coop = 0;   // serving: the small lane's kernels cooperative (1) or host-stepped (0)
+  int64_t serve_partition = 0;    // serving: the other lanes admit only requests above serve_small_mb
   int64_t batch_lanes = 2;        // batch: waves in flight at once (each on a stream of its own)
   int64_t support_rows = 2;       // exact dense support: edges sharing row u counted per read of it (1, 2, 4)
   int64_t peel_bisect_after = 16; // peel: truss levels climbed one at a time before bisecting the rest (0 = never)
