@@ -166,4 +166,38 @@ __device__ __forceinline__ bool grid_barrier(DevWords* w, unsigned long long tim
   return ld_volatile_u32(&w->err) == 0;
 }
 
+// One bulk copy by the TMA engine (cp.async.bulk, no multicast) of `bytes`
+// from global memory into this block's shared memory; both addresses 16-byte
+// aligned and `bytes` a multiple of 16.  Completion is tracked by the
+// mbarrier `mbar` (shared memory, 8-byte aligned, used once).  Every thread
+// of the block calls it: thread 0 initialises the barrier, announces the
+// bytes and issues the copy; then every thread polls the barrier's first
+// phase at most `polls` times.  Returns false (with kDevErrWait in *err) in
+// any thread that gave up; the staged bytes must then not be used.
+__device__ __forceinline__ bool bulk_load_to_shared(void* dst, const void* src, uint32_t bytes, uint64_t* mbar,
+                                                    uint32_t* err, uint32_t polls = 1u << 20) {
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
+  const uint32_t sdst = (uint32_t)__cvta_generic_to_shared(dst);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(sdst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+  }
+  uint32_t done = 0;
+  for (uint32_t i = 0; i < polls && !done; ++i)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+  if (!done) atomicOr(err, kDevErrWait);
+  return done != 0;
+}
+
 }  // namespace kt

@@ -159,13 +159,14 @@ __global__ void __launch_bounds__(kParseThreads) k_parse_lines(const uint8_t* __
   __shared__ __align__(16) uint32_t stage[(kBlockBytes + kOverhang) / 4];
   __shared__ uint16_t starts[kBlockBytes + 1];
   __shared__ uint32_t tmp[33];
+  __shared__ __align__(8) uint64_t stage_bar;
   const uint64_t blo = (block0 + blockIdx.x) * kBlockBytes;
   const uint64_t bhi = min(len, blo + kBlockBytes + kOverhang);
-  // The device buffer is padded (zeros) to whole 16-byte words past len.
+  // The device buffer is padded (zeros) to whole 16-byte words past len; the
+  // block's bytes come in as one bulk copy (blo is a multiple of 16).
   const uint64_t nvec = (bhi - blo + 15) / 16;
-  for (uint64_t i = threadIdx.x; i < nvec; i += kParseThreads)
-    reinterpret_cast<uint4*>(stage)[i] = reinterpret_cast<const uint4*>(buf + blo)[i];
-  __syncthreads();
+  const bool staged = bulk_load_to_shared(stage, buf + blo, (uint32_t)(nvec * 16), &stage_bar, &words->err);
+  if (__syncthreads_or(!staged)) return;
 
   const uint64_t s = blo + (uint64_t)threadIdx.x * kChunk;
   const uint64_t e = min(len, s + kChunk);
