@@ -653,12 +653,12 @@ void solve_wave(Ctx* c, const std::vector<BatchItem*>& items) {
       copy_h2d(c, dthr.get(), thr.data(), G * sizeof(uint32_t));
     }
     edge_support(c, s2, sup2.as<uint32_t>(), 0, capped ? dthr.as<uint32_t>() : nullptr);
-    // With capped counts the union is peeled in place (as the single-graph
-    // search phase does); with lists, a union rebuilt from the survivors when
-    // they are fewer than half.
+    // A union rebuilt from the survivors when they are fewer than half; else
+    // the union is peeled in place, capped counts and all (those of the
+    // survivors are exact, the others leave in the first round).
     Sub s3;
     DBuf sup3;
-    const bool rebuilt = !capped && survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
+    const bool rebuilt = survivors(c, s2, sup2.as<uint32_t>(), thr, true, s3, sup3);
     st.ms_support += tm.stop();
     tm.start();
     const auto t_p = std::chrono::steady_clock::now();

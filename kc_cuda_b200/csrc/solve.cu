@@ -69,16 +69,6 @@ bool truss_possible(Ctx* c, const Sub& s, const uint32_t* sup, uint32_t g) {
   return read_word<unsigned long long>(c, cnt.as<unsigned long long>()) >= g;
 }
 
-// Edges whose (capped) support reaches thr, counted into *out.
-__global__ void k_count_at_least(const uint32_t* __restrict__ sup, uint64_t m, uint32_t thr,
-                                 unsigned long long* out) {
-  uint64_t n = 0;
-  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x)
-    n += sup[e] >= thr;
-  n = warp_sum(n);
-  if (lane_id() == 0 && n) atomicAdd(out, (unsigned long long)n);
-}
-
 // Ends of the edges whose (capped) support reaches a threshold.
 struct AtLeast {
   const uint32_t* sup;
@@ -261,29 +251,17 @@ void solve_graph_inner(Ctx* c, const Graph& g, uint32_t* kmax, uint64_t* count) 
   const uint32_t t2 = std::max<uint32_t>(L, 3);
   const bool capped = c->opt.capped_support && s2.W;
   edge_support(c, s2, sup2.as<uint32_t>(), capped ? t2 - 2 : 0);
-  // Edges below the first threshold leave in the first round.  With bitsets
-  // (capped counts) the core is peeled in place: the first round's recount
-  // clears their bits and counts the rest exactly, and the capped counts of
-  // the rest are exact already (a rebuild of the survivors keeps the core's
-  // vertices, so its rows are no narrower).  With lists, when they are most
-  // of the graph, the peel continues on a graph rebuilt from the rest (the
-  // L-truss of the survivors is the L-truss of the core).
+  // Edges below the first threshold leave in the first round: when they are
+  // most of the graph, continue on the rest (the L-truss of the survivors is
+  // the L-truss of the core) instead of clearing them one by one.  When they
+  // are not, the core is peeled in place even with capped counts: those of
+  // the edges at or above the threshold are exact, and the others leave in
+  // the first round.
   Sub s3;
   DBuf sup3;
   const Sub* sp = &s2;
   uint32_t* supp = sup2.as<uint32_t>();
-  if (t2 > 3 && s2.m && capped) {
-    if (c->opt.verbose) {
-      DBuf n(c, 8);
-      zero(c, n.get(), 8);
-      k_count_at_least<<<grid_for(s2.m, 256, c->num_sms * 8), 256, 0, c->stream>>>(
-          sup2.as<uint32_t>(), s2.m, t2 - 2, n.as<unsigned long long>());
-      KT_LAUNCHED(c);
-      KT_LOG(c, "kt: search level %u: %llu of %llu edges have support >= %u (core peeled in place)\n", t2,
-             (unsigned long long)read_word<unsigned long long>(c, n.as<unsigned long long>()),
-             (unsigned long long)s2.m, t2 - 2);
-    }
-  } else if (t2 > 3 && s2.m) {
+  if (t2 > 3 && s2.m) {
     DBuf keys(c, s2.m * sizeof(uint64_t));
     const uint64_t k = compact(c, s2.m, AtLeast{sup2.as<uint32_t>(), s2.ends.as<uint64_t>(), t2 - 2},
                                keys.as<uint64_t>());
