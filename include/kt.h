@@ -72,7 +72,8 @@ const char* kt_status_string(kt_status s);
  *   pool_reserve_mb (0)         setting it grows the device memory pool by that
  *                               much at once (allocations mid-solve then reuse it)
  *   kcore_big_row (512)         k-core rounds deal longer rows to all warps in
- *                               32-entry windows
+ *                               windows (256 entries in the maximum-core probes,
+ *                               32 in the full decomposition)
  *   peel_search_ratio (16)      peel: per-lane binary search when one row is this
  *                               many times longer than the other
  *   dense_tile_mb (48)          dense support: bitset rows of two tile blocks fit
