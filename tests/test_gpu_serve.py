@@ -147,3 +147,34 @@ def test_one_lane_keeps_waves_in_order():
             g = ctx.load_mix_graph(i)
             assert (r["kmax"], r["edges"]) == g.kmax_truss()
             g.free()
+
+
+@pytest.mark.parametrize("partition,coop", [(1, 0), (0, 1), (1, 1)])
+def test_small_lane_modes(partition, coop):
+    """The small-request lane's variants: cooperative launches taking turns
+    (serve_small_coop 1) and the other lanes kept to large requests
+    (serve_partition 1).  Every answer equals the graph's alone; with the
+    partition, small requests (estimated footprint well under serve_small_mb)
+    run on the last lane and large ones (well over it) on the other."""
+    small = [5, 7, 10, 17, 23]
+    large = [9, 16, 18, 19]
+    with K.Context(0) as ctx:
+        ctx.set_option("serve_small_mb", 16)
+        ctx.set_option("serve_partition", partition)
+        ctx.set_option("serve_small_coop", coop)
+        alone = {}
+        for i in small + large:
+            g = ctx.load_mix_graph(i)
+            alone[i] = g.kmax_truss()
+            g.free()
+        with ctx.server() as srv:
+            rids = [(i, srv.submit_mix(i)) for pair in zip(large + [None], small) for i in pair if i is not None]
+            rs = {i: srv.wait(rid) for i, rid in rids}
+        ctx.set_option("serve_partition", 0)
+        ctx.set_option("serve_small_coop", 0)
+        ctx.set_option("serve_small_mb", 128)
+    for i, r in rs.items():
+        assert r["status"] == 0 and (r["kmax"], r["edges"]) == alone[i], i
+    if partition:
+        assert {rs[i]["lane"] for i in small} == {1}
+        assert {rs[i]["lane"] for i in large} == {0}
